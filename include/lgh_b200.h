@@ -1,0 +1,335 @@
+/* lgh_b200.h -- C ABI of the B200 (sm_100a) GLR library.
+ *
+ * A drop-in for the GLR + prior path of NickAlger/lgpsf-hessian: the same
+ * lgh_prior_* / lgh_glr_* names, argument order, option/report structs
+ * (field for field) and error codes as the reference headers
+ *   include/lgpsf_hessian/prior.h:38-110
+ *   include/lgpsf_hessian/glr.h:50-169
+ *   include/lgpsf_hessian/lgpsf_hessian.h:19-43 (conventions),
+ * with PETSc replaced by three opaque handle types:
+ *
+ *   Mat  a device-resident operator: a CSR matrix (lgh_mat_create_csr /
+ *        lgh_mat_create_dense) or a dense column block handed to blocked
+ *        prior callbacks.  The engine only ever multiplies by B and Z
+ *        (glr.h:104-108).
+ *   Vec  a device vector of doubles (lgh_vec_create / _with_array).
+ *   KSP  accepted by lgh_prior_create_ksp only to return LGH_ERR_SUP.
+ *
+ * Conventions (lgpsf_hessian.h:19-35): functions return 0 on success and a
+ * nonzero PETSc-numbered code on failure; in/out Vec arguments must not
+ * alias; calls on one lgh_glr_t are serialised by the caller (the object
+ * owns scratch).  Every call is synchronous with respect to the host
+ * unless its name ends in _async.  There is one device (the current CUDA
+ * device at the first call); no MPI: the communicator is one process.
+ *
+ * Extensions live under new names and never change a reference signature:
+ * lgh_glr_compute_ex (precision), lgh_glr_*_batch (many right-hand sides
+ * and shifts), lgh_glr_get_stats, the lgh_server_* request loop, and the
+ * Mat / Vec constructors.
+ */
+
+#ifndef LGH_B200_H
+#define LGH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#define LGPSF_HESSIAN_VERSION_MAJOR 0
+#define LGPSF_HESSIAN_VERSION_MINOR 1
+#define LGPSF_HESSIAN_VERSION_PATCH 0
+
+/* error codes: the PETSc numbers the reference returns (lgpsf_hessian.h:
+ * 27-28 and its PetscCheck sites) */
+#define LGH_SUCCESS               0
+#define LGH_ERR_MEM              55  /* PETSC_ERR_MEM: device allocation    */
+#define LGH_ERR_SUP              56  /* PETSC_ERR_SUP                        */
+#define LGH_ERR_ORDER            58  /* PETSC_ERR_ORDER: extend after correct*/
+#define LGH_ERR_ARG_SIZ          60  /* PETSC_ERR_ARG_SIZ                    */
+#define LGH_ERR_ARG_WRONG        62  /* PETSC_ERR_ARG_WRONG                  */
+#define LGH_ERR_ARG_OUTOFRANGE   63  /* PETSC_ERR_ARG_OUTOFRANGE             */
+#define LGH_ERR_ARG_WRONGSTATE   73  /* PETSC_ERR_ARG_WRONGSTATE             */
+#define LGH_ERR_LIB              76  /* PETSC_ERR_LIB: factorisation failed  */
+#define LGH_ERR_ARG_NULL         85  /* PETSC_ERR_ARG_NULL                   */
+#define LGH_ERR_NOT_CONVERGED    91  /* PETSC_ERR_NOT_CONVERGED              */
+#define LGH_ERR_GPU              97  /* PETSC_ERR_GPU: CUDA runtime error    */
+
+#ifdef __cplusplus
+extern "C"
+{
+#endif
+
+/* ---- PETSc-free handle types ------------------------------------------ */
+
+typedef struct lgh_mat_s *lgh_Mat;
+typedef struct lgh_vec_s *lgh_Vec;
+typedef struct lgh_ksp_s *lgh_KSP;
+
+#ifndef LGH_NO_PETSC_NAMES
+typedef lgh_Mat Mat;
+typedef lgh_Vec Vec;
+typedef lgh_KSP KSP;
+#endif
+
+/* where a constructor's input arrays live */
+#define LGH_MEM_HOST   0
+#define LGH_MEM_DEVICE 1
+
+/* Sparse symmetric operator from CSR (0-based, int64 row pointers, int32
+ * column indices, sorted or not).  Arrays are copied to the device
+ * (where = LGH_MEM_HOST) or device-to-device (LGH_MEM_DEVICE).  A float
+ * copy of the values is kept too, for the mixed-precision path.  The
+ * handle is reference counted; lgh_mat_destroy drops one reference.       */
+int lgh_mat_create_csr (int64_t n, const int64_t *rowptr,
+                        const int32_t *colidx, const double *vals, int where,
+                        lgh_Mat *A);
+/* Dense n x n operator (column-major, leading dimension lda), e.g. the
+ * MPIDENSE B of the reference's tests; stored as a full CSR.             */
+int lgh_mat_create_dense (int64_t n, const double *a, int64_t lda, int where,
+                          lgh_Mat *A);
+int lgh_mat_get_info (lgh_Mat A, int64_t *n, int64_t *nnz);
+/* y = A x (MatMult). */
+int lgh_mat_mult (lgh_Mat A, lgh_Vec x, lgh_Vec y);
+/* Dense column block views given to blocked prior callbacks:
+ * data[i + j * ld] is row i of column j (MATDENSE layout), device memory. */
+int lgh_mat_dense_get_array (lgh_Mat X, double **data, int64_t *nrows,
+                             int *ncols, int64_t *ld);
+int lgh_mat_destroy (lgh_Mat *A);
+
+/* Device vectors of length n.  _with_array borrows a device array.       */
+int lgh_vec_create (int64_t n, lgh_Vec *v);
+int lgh_vec_create_with_array (int64_t n, double *device_array, lgh_Vec *v);
+int lgh_vec_get_array (lgh_Vec v, double **device_array, int64_t *n);
+int lgh_vec_set_host (lgh_Vec v, const double *host);  /* H2D copy        */
+int lgh_vec_get_host (lgh_Vec v, double *host);        /* D2H copy        */
+int lgh_vec_destroy (lgh_Vec *v);
+
+/* ---- prior.h ------------------------------------------------------------ */
+
+typedef struct lgh_prior lgh_prior_t; /* opaque */
+
+/* y = Op x on device vectors. */
+typedef void (*lgh_vec_fn) (lgh_Vec x, lgh_Vec y, void *ctx);
+/* Y = Op X on dense device column blocks (lgh_mat_dense_get_array). */
+typedef void (*lgh_mat_fn) (lgh_Mat X, lgh_Mat Y, void *ctx);
+
+/* prior.h:47-57 */
+typedef struct lgh_prior_callbacks
+{
+  lgh_vec_fn applyZ;           /* required                                 */
+  lgh_vec_fn applyZt;          /* NULL => Z treated as symmetric           */
+  lgh_vec_fn solveZ;           /* required                                 */
+  lgh_vec_fn solveZt;          /* NULL => symmetric                        */
+  lgh_mat_fn solveZ_blocked;   /* optional, performance                    */
+  lgh_mat_fn solveZt_blocked;  /* optional                                 */
+  void      *ctx;
+}
+lgh_prior_callbacks_t;
+
+int lgh_prior_create_callbacks (lgh_Vec mass_lumps,
+                                const lgh_prior_callbacks_t *callbacks,
+                                lgh_prior_t **prior);
+
+/* prior.h:76-89.  On this device the Mat path solves Z with blocked,
+ * per-column preconditioned CG (blocked_mode 0/1, rtol ksp_rtol, the
+ * reference's per-column KSP semantics) or blocked fixed-count Chebyshev
+ * (mode 2, cheb_rtol, bounds from a CG-Lanczos probe widened 0.9/1.1), both
+ * Jacobi-preconditioned; mode 3 runs Chebyshev around a block V-cycle on an
+ * aggregation hierarchy built from Z.  tile caps the block width of one
+ * blocked solve pass.                                                     */
+typedef struct lgh_prior_mat_opts
+{
+  double ksp_rtol;     /* per-column solve tolerance (default 1e-12)     */
+  int    blocked_mode; /* 0 (default) | 1 | 2 | 3                         */
+  int    tile;         /* block width cap (default 64; 0 = no cap)       */
+  double cheb_rtol;    /* Chebyshev accuracy target (default 1e-10)      */
+  int    smax_krylov;  /* 1 (default): level bounds via CG-Lanczos       */
+  double smoother_top; /* smoothing-interval top factor (default 1.1)    */
+  int    nu_force;     /* force smoother degree (0 = default 2)          */
+  int    verbose;
+}
+lgh_prior_mat_opts_t;
+
+lgh_prior_mat_opts_t lgh_prior_mat_opts_default (void);
+
+int lgh_prior_create_mat (lgh_Mat Z, lgh_Vec mass_lumps,
+                          const lgh_prior_mat_opts_t *opts,
+                          lgh_prior_t **prior);
+/* Always LGH_ERR_SUP: there is no PETSc KSP on this device.              */
+int lgh_prior_create_ksp (lgh_KSP ksp, lgh_Vec mass_lumps,
+                          const lgh_prior_mat_opts_t *opts,
+                          lgh_prior_t **prior);
+void lgh_prior_destroy (lgh_prior_t *prior);
+/* y = R x = Z M^{-1} Z x */
+int lgh_prior_apply (lgh_prior_t *prior, lgh_Vec x, lgh_Vec y);
+/* y = Z^{-1} x through the prior's single-vector solve (testing).       */
+int lgh_prior_solve (lgh_prior_t *prior, lgh_Vec x, lgh_Vec y);
+/* Y = Z^{-1} X on a device column block (column-major, leading dim ld),
+ * through the prior's blocked solve (testing and batched callers).      */
+int lgh_prior_solve_block (lgh_prior_t *prior, int m, const double *X,
+                           int64_t ldx, double *Y, int64_t ldy);
+
+/* Diagnostics of a Mat-path prior's Z-solver: out[0..7] = Lanczos emin,
+ * emax, margined lmin, lmax, Chebyshev nit, probe iterations, mean
+ * per-column CG iterations so far, number of solve calls.               */
+int lgh_prior_get_info (const lgh_prior_t *prior, double *out);
+
+/* ---- glr.h --------------------------------------------------------------- */
+
+typedef struct lgh_glr lgh_glr_t; /* opaque */
+
+typedef enum
+{
+  LGH_GLR_DEFAULT    = 0,  /* the device backend, incremental extend      */
+  LGH_GLR_REPLICATED = 1,  /* the device backend, extend = full rebuild   */
+  LGH_GLR_SCALAPACK  = 2   /* accepted: same as DEFAULT                   */
+}
+lgh_glr_backend_t;
+
+typedef enum
+{
+  LGH_TREAT_FLIP = 0,      /* lam <- |lam|  (default)                      */
+  LGH_TREAT_RELU = 1,      /* lam <- max(lam, 0)                           */
+  LGH_TREAT_NONE = 2
+}
+lgh_treat_t;
+
+/* glr.h:68-86, field for field */
+typedef struct lgh_glr_opts
+{
+  int               ell;       /* sketch width (target rank <= ell)        */
+  int               q_power;   /* power-iteration passes                   */
+  double            trunc_abs; /* keep treated |lam| > trunc_abs           */
+  double            trunc_rel; /* ... or > trunc_rel * max|lam| (0 = off)  */
+  lgh_treat_t       treat;
+  unsigned long     seed;      /* hashed-sketch seed                       */
+  lgh_glr_backend_t backend;
+  int               nb;        /* accepted, unused (no block-cyclic T)     */
+  int               panel;     /* BCGS2 panel width of the extension       */
+  int               grid2d;    /* accepted, unused                         */
+  int               check;     /* eigen-residual check on build            */
+}
+lgh_glr_opts_t;
+
+lgh_glr_opts_t lgh_glr_opts_default (void);
+
+/* glr.h:90-102 */
+typedef struct lgh_glr_report
+{
+  int    kept;
+  double lam_abs_max;
+  double lam_raw_min, lam_raw_max;
+  double next_abs;
+  int    n_negative_raw;
+  double resid_max;
+  double t_operator, t_dense;
+}
+lgh_glr_report_t;
+
+/* glr.h:104-113 */
+int lgh_glr_compute (lgh_Mat B, lgh_prior_t *prior,
+                     const lgh_glr_opts_t *opts, lgh_glr_t **glr,
+                     lgh_glr_report_t *report);
+/* glr.h:115-124 */
+int lgh_glr_extend (lgh_glr_t *glr, int k_new, lgh_glr_report_t *report);
+void lgh_glr_destroy (lgh_glr_t *glr);
+
+/* full space: H(c) = B + c R (glr.h:128-158) */
+int lgh_glr_solve (lgh_glr_t *glr, double c, lgh_Vec rhs, lgh_Vec x);
+int lgh_glr_apply (lgh_glr_t *glr, double c, lgh_Vec v, lgh_Vec y);
+int lgh_glr_sample (lgh_glr_t *glr, double c, lgh_Vec xi, lgh_Vec x);
+
+typedef enum
+{
+  LGH_FACTOR_G     = 0,
+  LGH_FACTOR_GT    = 1,
+  LGH_FACTOR_GINV  = 2,
+  LGH_FACTOR_GINVT = 3   /* == lgh_glr_sample */
+}
+lgh_factor_t;
+
+int lgh_glr_factor (lgh_glr_t *glr, double c, lgh_factor_t which,
+                    lgh_Vec in, lgh_Vec out);
+
+/* prior-weighted frame (glr.h:160-169) */
+double lgh_glr_logdet (lgh_glr_t *glr, double c);
+int lgh_glr_pow (lgh_glr_t *glr, double c, double p, lgh_Vec in,
+                 lgh_Vec out);
+int lgh_glr_filter (lgh_glr_t *glr, const double *f_lam, double f_c,
+                    lgh_Vec in, lgh_Vec out);
+int lgh_glr_eigs (const lgh_glr_t *glr, int *nkept, const double **lam);
+
+/* ---- extensions --------------------------------------------------------- */
+
+#define LGH_PREC_FP64  0   /* everything FP64 (the plain form)             */
+#define LGH_PREC_MIXED 1   /* FP32 sweeps/blocks, FP64 small dense + core  */
+
+typedef struct lgh_exec_opts
+{
+  int    precision;    /* LGH_PREC_FP64 (default) | LGH_PREC_MIXED       */
+  double inner_rtol;   /* mixed: FP32 inner Z-solve tolerance (1e-5)     */
+  int    max_refine;   /* mixed: FP64 refinement steps per solve (4)     */
+  int    verbose;
+}
+lgh_exec_opts_t;
+
+lgh_exec_opts_t lgh_exec_opts_default (void);
+
+int lgh_glr_compute_ex (lgh_Mat B, lgh_prior_t *prior,
+                        const lgh_glr_opts_t *opts,
+                        const lgh_exec_opts_t *exec, lgh_glr_t **glr,
+                        lgh_glr_report_t *report);
+
+typedef struct lgh_glr_stats
+{
+  int64_t n;
+  int     ell, kept, precision;
+  double  t_build, t_sketch, t_zsolve, t_spmm, t_orth, t_eig, t_check;
+  long    zsolve_calls, zsolve_iters;   /* block-iterations, all solves  */
+  double  zsolve_mean_col_iters;        /* mean per-column iterations    */
+  int64_t device_bytes;                 /* resident state of the object  */
+}
+lgh_glr_stats_t;
+
+int lgh_glr_get_stats (const lgh_glr_t *glr, lgh_glr_stats_t *stats);
+
+/* Copy U (n x kept, column-major, leading dim ld) to device memory.     */
+int lgh_glr_get_U (const lgh_glr_t *glr, double *U_dev, int64_t ld);
+
+/* Batched downstream operations on device column blocks (column-major,
+ * leading dims ldr/ldx), m right-hand sides, nshift shifts c[0..nshift):
+ * output block s (columns s*m .. s*m+m-1 of x) holds the result at c[s].
+ * The Z-solves, which do not depend on c, run once per right-hand side.   */
+int lgh_glr_solve_batch (lgh_glr_t *glr, int nshift, const double *c,
+                         int m, const double *rhs, int64_t ldr, double *x,
+                         int64_t ldx);
+int lgh_glr_sample_batch (lgh_glr_t *glr, int nshift, const double *c,
+                          int m, const double *xi, int64_t ldr, double *x,
+                          int64_t ldx);
+int lgh_glr_logdet_batch (lgh_glr_t *glr, int nshift, const double *c,
+                          double *out);
+
+/* Last error message of the calling thread (empty if none).              */
+const char *lgh_last_error (void);
+
+/* ---- kernel-level test hooks (host arrays in and out; not used by the
+ * build): each runs exactly one device kernel path. ---------------------- */
+int lgh_test_sketch (uint64_t seed, int64_t n, int64_t j0, int k,
+                     double *out);
+int lgh_test_rng_state (uint64_t seed, int64_t n, int64_t j0, int k,
+                        uint64_t *out);
+int lgh_test_spmm (lgh_Mat A, int w, const double *X, double *Y, int fp32);
+int lgh_test_zsolve (lgh_prior_t *prior, int w, const double *X, double *Y,
+                     int fp32);
+int lgh_test_gram (int64_t n, int w, const double *X, double *G);
+int lgh_test_gemm_nn (int64_t n, int k, int m, const double *X,
+                      const double *M, double *Y);
+int lgh_test_potrf (int n, const double *G, int jitter_mode, double *L,
+                    double *Linv, int *info);
+int lgh_test_syev (int n, const double *A, double *w, double *V,
+                   int *sweeps);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LGH_B200_H */

@@ -1,0 +1,191 @@
+/* k_spmm.cu -- CSR times row-major block: Y = A X.
+ *
+ * Replaces the reference's per-column MatMult loop (glr_common_impl.h:
+ * 325-332, and MatMatMult in the Chebyshev core, zsolve_impl.h:123-136).
+ * A group of G lanes (a power of two <= 32) owns one row; lane l covers the
+ * 16-byte vector columns l, l+G, ..., so every nonzero (i, j) gathers the
+ * contiguous row segment X[j, :] with coalesced vector loads, reused from
+ * L1/L2 by the neighbouring rows of the same CTA.  The group's lanes fetch
+ * G (col, val) pairs at once and broadcast them with shuffles.  Each CTA
+ * owns a contiguous row range.  HBM bound; algorithmic bytes
+ * nnz (s_v + 4) + 8 (N + 1) + 2 N w s_x.
+ */
+
+#include "lgh_device.cuh"
+#include "lgh_internal.h"
+
+namespace lgh
+{
+
+template <typename T, typename TV, int CH>
+__global__ void __launch_bounds__ (256)
+k_spmm (int64_t n, const int64_t *__restrict__ rowptr,
+        const int32_t *__restrict__ colidx, const TV *__restrict__ vals,
+        const T *__restrict__ X, int ldx, T *__restrict__ Y, int ldy,
+        int nvec, int glog)
+{
+  constexpr int W = Pack<T>::W;
+  const int G = 1 << glog;
+  const int lane = threadIdx.x & (G - 1);
+  const int group = threadIdx.x >> glog;
+  const int ngroups = blockDim.x >> glog;
+  const unsigned gmask = (G == 32) ? 0xffffffffu
+                         : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+  int64_t r0, r1;
+  block_rows (n, r0, r1);
+  for (int64_t i = r0 + group; i < r1; i += ngroups) {
+    T acc[CH][W];
+#pragma unroll
+    for (int h = 0; h < CH; h++)
+#pragma unroll
+      for (int e = 0; e < W; e++) acc[h][e] = T (0);
+    const int64_t k0 = rowptr[i], k1 = rowptr[i + 1];
+    for (int64_t kb = k0; kb < k1; kb += G) {
+      const int cnt = (int) ((k1 - kb) < G ? (k1 - kb) : G);
+      int mc = 0;
+      T mv = T (0);
+      if (lane < cnt) {
+        mc = colidx[kb + lane];
+        mv = (T) vals[kb + lane];
+      }
+      for (int t = 0; t < cnt; t++) {
+        const int c = __shfl_sync (gmask, mc, t, G);
+        const T v = __shfl_sync (gmask, mv, t, G);
+        const T *xr = X + (int64_t) c * ldx;
+#pragma unroll
+        for (int h = 0; h < CH; h++) {
+          const int vi = lane + h * G;
+          if (vi < nvec) {
+            Pack<T> x = ldp_nc (xr + vi * W);
+#pragma unroll
+            for (int e = 0; e < W; e++) acc[h][e] = fma (v, x.v[e], acc[h][e]);
+          }
+        }
+      }
+    }
+    T *yr = Y + i * ldy;
+#pragma unroll
+    for (int h = 0; h < CH; h++) {
+      const int vi = lane + h * G;
+      if (vi < nvec) {
+        Pack<T> o;
+#pragma unroll
+        for (int e = 0; e < W; e++) o.v[e] = acc[h][e];
+        stp (yr + vi * W, o);
+      }
+    }
+  }
+}
+
+/* Scalar form for single vectors and unaligned views (ld not a multiple
+ * of the 16-byte vector, or an offset base): G lanes split a row's
+ * nonzeros (CSR-vector), reduce with shuffles; columns in a loop. */
+template <typename T, typename TV>
+__global__ void __launch_bounds__ (256)
+k_spmm_scalar (int64_t n, const int64_t *__restrict__ rowptr,
+               const int32_t *__restrict__ colidx, const TV *__restrict__ vals,
+               const T *__restrict__ X, int ldx, T *__restrict__ Y, int ldy,
+               int w)
+{
+  constexpr int G = 8;
+  const int lane = threadIdx.x & (G - 1);
+  const unsigned gmask = 0xffu << ((threadIdx.x & 31) & ~(G - 1));
+  const int64_t row0 = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const int64_t rstride = ((int64_t) gridDim.x * blockDim.x) / G;
+  for (int64_t i = row0; i < n; i += rstride) {
+    const int64_t k0 = rowptr[i], k1 = rowptr[i + 1];
+    for (int c = 0; c < w; c++) {
+      T acc = T (0);
+      for (int64_t k = k0 + lane; k < k1; k += G)
+        acc = fma ((T) vals[k], X[(int64_t) colidx[k] * ldx + c], acc);
+#pragma unroll
+      for (int o = G / 2; o > 0; o >>= 1)
+        acc += __shfl_xor_sync (gmask, acc, o, G);
+      if (lane == 0) Y[i * ldy + c] = acc;
+    }
+  }
+}
+
+/* lanes per row and vector chunks per lane for a width of nvec vectors */
+void
+row_group_shape (int nvec, int &glog, int &ch)
+{
+  int g = 1;
+  glog = 0;
+  while (g < nvec && g < 32) { g <<= 1; glog++; }
+  ch = (nvec + g - 1) / g;
+}
+
+int
+row_grid (int64_t n, int glog)
+{
+  const int rows_per_cta_iter = 256 >> glog;
+  int64_t want = (n + rows_per_cta_iter - 1) / rows_per_cta_iter;
+  int64_t cap = (int64_t) num_sms () * 8;
+  if (want > cap) want = cap;
+  return (int) (want > 0 ? want : 1);
+}
+
+template <typename T, typename TV>
+static int
+spmm_dispatch (const Csr &A, const TV *vals, const T *X, int ldx, T *Y,
+               int ldy, int w, cudaStream_t s)
+{
+  constexpr int W = Pack<T>::W;
+  const int MAXCH = 10;
+  const bool vec_ok = (ldx % W == 0) && (ldy % W == 0)
+                      && ((uintptr_t) X % 16 == 0) && ((uintptr_t) Y % 16 == 0);
+  if (!vec_ok) {
+    int64_t g = (A.n * 8 + 255) / 256;
+    if (g > (int64_t) num_sms () * 16) g = (int64_t) num_sms () * 16;
+    if (g < 1) g = 1;
+    k_spmm_scalar<T, TV><<<(int) g, 256, 0, s>>> (A.n, A.rowptr, A.colidx,
+                                                  vals, X, ldx, Y, ldy, w);
+    LGH_LAUNCH_CHECK ();
+    return 0;
+  }
+  /* column chunks of at most 32 lanes * MAXCH vectors */
+  for (int c0 = 0; c0 < w; c0 += 32 * MAXCH * W) {
+    const int wc = (w - c0) < 32 * MAXCH * W ? (w - c0) : 32 * MAXCH * W;
+    const int nvec = (wc + W - 1) / W;
+    int glog, ch;
+    row_group_shape (nvec, glog, ch);
+    const int grid = row_grid (A.n, glog);
+    const T *Xc = X + c0;
+    T *Yc = Y + c0;
+#define LGH_SPMM_CASE(C)                                                     \
+  case C:                                                                    \
+    k_spmm<T, TV, C><<<grid, 256, 0, s>>> (A.n, A.rowptr, A.colidx, vals,    \
+                                           Xc, ldx, Yc, ldy, nvec, glog);    \
+    break;
+    switch (ch) {
+      LGH_SPMM_CASE (1) LGH_SPMM_CASE (2) LGH_SPMM_CASE (3)
+      LGH_SPMM_CASE (4) LGH_SPMM_CASE (5) LGH_SPMM_CASE (6)
+      LGH_SPMM_CASE (7) LGH_SPMM_CASE (8) LGH_SPMM_CASE (9)
+      LGH_SPMM_CASE (10)
+    default:
+      return set_error (LGH_ERR_SUP, "spmm: unsupported chunking %d", ch);
+    }
+#undef LGH_SPMM_CASE
+    LGH_LAUNCH_CHECK ();
+  }
+  return 0;
+}
+
+template <>
+int
+launch_spmm<double> (const Csr &A, const double *X, int ldx, double *Y,
+                     int ldy, int w, cudaStream_t s)
+{
+  return spmm_dispatch<double, double> (A, A.vals, X, ldx, Y, ldy, w, s);
+}
+
+template <>
+int
+launch_spmm<float> (const Csr &A, const float *X, int ldx, float *Y, int ldy,
+                    int w, cudaStream_t s)
+{
+  return spmm_dispatch<float, float> (A, A.vals32, X, ldx, Y, ldy, w, s);
+}
+
+} /* namespace lgh */

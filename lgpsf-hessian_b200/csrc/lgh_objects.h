@@ -1,0 +1,100 @@
+/* lgh_objects.h -- the opaque objects behind the C ABI handles. */
+
+#ifndef LGH_OBJECTS_H
+#define LGH_OBJECTS_H
+
+#include <vector>
+
+#include "lgh_internal.h"
+
+/* Mat: a device CSR operator (kind 0) or a dense column-block view handed
+ * to blocked prior callbacks (kind 1, MATDENSE layout, not owned). */
+struct lgh_mat_s
+{
+  int refs = 1;
+  int kind = 0;
+  lgh::Csr csr;
+  double *data = nullptr;
+  int64_t nrows = 0;
+  int ncols = 0;
+  int64_t ld = 0;
+};
+
+/* Vec: a device vector; owns its array unless created with an array. */
+struct lgh_vec_s
+{
+  double *d = nullptr;
+  int64_t n = 0;
+  int owns = 0;
+};
+
+/* struct lgh_prior (glr_common_impl.h:81-94) */
+struct lgh_prior
+{
+  int refs = 1;
+  int64_t n = 0;
+  lgh::DBuf<double> mass, msqrt, minvsqrt;
+  lgh::DBuf<double> tmp1, tmp2;
+  /* callbacks path */
+  lgh_prior_callbacks_t cb{};
+  /* Mat path */
+  int is_mat = 0;
+  lgh_Mat Z = nullptr;
+  lgh_prior_mat_opts_t mopts{};
+  lgh::ZsolveCfg zcfg;
+  lgh::ZWork ws64, ws32, wsv;
+  double emin = 0., emax = 0.;
+  int bound_its = 0;
+  lgh::ZsolveStats stats;
+};
+
+/* struct lgh_glr (glr_common_impl.h:252-278), device resident */
+struct lgh_glr
+{
+  int64_t n = 0;
+  lgh_Mat B = nullptr;
+  lgh_prior_t *prior = nullptr;
+  lgh_glr_opts_t opts{};
+  lgh_exec_opts_t exec{};
+  /* build product: U (n x kept, row-major, ld ldu) and the treated,
+   * |lam|-descending spectrum (host mirror for lgh_glr_eigs) */
+  lgh::DBuf<double> U, lam_d, lraw_d;
+  lgh::DBuf<float> U32;
+  int ldu = 4;
+  int kept = 0;
+  std::vector<double> lam_h;
+  /* sketch state for the incremental extension: Q (n x ell) and the raw
+   * projection A = Q^T F Q (ell x ell, column-major) */
+  lgh::DBuf<double> Q, A;
+  lgh::DBuf<float> Q32;
+  int ldq = 4, ell = 0;
+  /* deflation-correction state of the reference (never set here: the
+   * correction stage is not part of this library) */
+  int corrected = 0;
+  double floor = 0.;
+  /* scratch */
+  lgh::DBuf<double> w1, w2, wk, fk, part;
+  lgh::DBuf<unsigned> cnt;
+  /* shift-independent precompute for the batched operations:
+   * W = Z^{-1} M^{1/2} U (n x kept, row-major, ld ldu) */
+  lgh::DBuf<double> Wz;
+  int have_wz = 0;
+  lgh_glr_stats_t stats{};
+};
+
+namespace lgh
+{
+void mat_release (lgh_Mat A);
+int mat_mult_vec (lgh_Mat A, const double *x, double *y);
+void prior_ref (lgh_prior_t *p);
+int prior_applyZ (lgh_prior_t *p, const double *x, double *y);
+int prior_solve_vec (lgh_prior_t *p, const double *x, const double *s_in,
+                     double *y, const double *s_out);
+template <typename T>
+int prior_solve_rows (lgh_prior_t *p, int w, const T *X, int ldx,
+                      const double *s_in, T *Y, int ldy, const double *s_out);
+int launch_vec_div (int64_t n, const double *x, const double *d, double *y,
+                    cudaStream_t s);
+}
+
+#endif /* LGH_OBJECTS_H */

@@ -1,0 +1,720 @@
+/* zsolve.cu -- blocked Z-solves on row-major blocks.
+ *
+ * Restates the reference's Z-solve contract (include/lgpsf_hessian/impl/
+ * zsolve_impl.h) for one device:
+ *   mode 0/1  per-column preconditioned CG (the semantics of the per-column
+ *             KSPSolve of zsolve_impl.h:674-715: CG, zero initial guess,
+ *             preconditioned-residual norm, rtol = ksp_rtol, 10000-iteration
+ *             cap), run for all columns of a block at once with per-column
+ *             alpha/beta and a per-column convergence mask;
+ *   mode 2    fixed-count Chebyshev (zsolve_impl.h:94-141), nit from the
+ *             margined spectral interval.
+ * The preconditioner is Jacobi (the reference's PCGAMG is replaced; the
+ * aggregation V-cycle of mode 3 lives in mg.cu).
+ *
+ * Each CG iteration is two fused kernels:
+ *   k_pcg_pq   p_new = D^{-1} r + beta p_old, computed on the fly at every
+ *              neighbour row, q = Z p_new, and the per-column dot (p, q);
+ *              the last CTA (atomic ticket) reduces the per-CTA partials in
+ *              a fixed order and sets alpha = (r, z) / (p, q).
+ *   k_pcg_upd  x += alpha p, r -= alpha q, z = D^{-1} r, dots (r, z) and
+ *              (z, z); the last CTA sets beta, the convergence mask and the
+ *              count of active columns.
+ * HBM traffic per iteration: 10 N w s (Chebyshev: 6 N w s, one kernel).
+ * Every reduction is deterministic: reruns are bitwise identical and a
+ * column's result does not depend on the other columns of the block.
+ */
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+#include <type_traits>
+#include <unordered_map>
+
+#include "lgh_device.cuh"
+#include "lgh_internal.h"
+
+namespace lgh
+{
+
+void row_group_shape (int nvec, int &glog, int &ch);
+int row_grid (int64_t n, int glog);
+
+constexpr int ZS_THREADS = 256;
+constexpr int ZS_MAXCH = 8;
+
+/* per-column scalar slots in ZWork::scal (each `cap` long) */
+enum { S_RZ = 0, S_ALPHA, S_BETA, S_NORM0, S_NSLOT };
+/* int slots in ZWork::ival */
+enum { I_ACTIVE = 0, I_ITS, I_NSLOT };
+
+struct ZK
+{
+  int64_t n;
+  const int64_t *rowptr;
+  const int32_t *col;
+};
+
+#define ZS_GROUP_SETUP()                                                     \
+  constexpr int W = Pack<T>::W;                                              \
+  const int G = 1 << glog;                                                   \
+  const int lane = threadIdx.x & (G - 1);                                    \
+  const int group = threadIdx.x >> glog;                                     \
+  const int ngroups = blockDim.x >> glog;                                    \
+  const unsigned gmask = (G == 32) ? 0xffffffffu                             \
+      : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));               \
+  (void) gmask;                                                              \
+  int64_t r0, r1;                                                            \
+  block_rows (z.n, r0, r1);
+
+/* ---- init: R = S B (pads zero), X = 0, P = 0; rz, norm0, mask ---------- */
+template <typename T, int CH>
+__global__ void __launch_bounds__ (ZS_THREADS)
+k_pcg_init (ZK z, const T *__restrict__ dinv, const T *__restrict__ Bsrc,
+            int ldb, const double *__restrict__ rs_in, T *X, T *R, T *P,
+            int ld, int nvec, int glog, int w, double *partA, double *partB,
+            unsigned *counter, double *scal, int *ival, int cap)
+{
+  extern __shared__ double red[];
+  ZS_GROUP_SETUP ();
+  double aRZ[CH][W], aZZ[CH][W];
+#pragma unroll
+  for (int h = 0; h < CH; h++)
+#pragma unroll
+    for (int e = 0; e < W; e++) { aRZ[h][e] = 0.; aZZ[h][e] = 0.; }
+  for (int64_t i = r0 + group; i < r1; i += ngroups) {
+    const double sc = rs_in ? rs_in[i] : 1.0;
+    const double di = (double) dinv[i];
+#pragma unroll
+    for (int h = 0; h < CH; h++) {
+      const int vi = lane + h * G;
+      if (vi < nvec) {
+        Pack<T> r;
+#pragma unroll
+        for (int e = 0; e < W; e++) {
+          /* scalar loads guarded by c < w: the source may be a single
+           * vector (ldb = 1) or an unaligned view */
+          const int c = vi * W + e;
+          const T bv = (c < w) ? (T) (sc * (double) Bsrc[i * ldb + c]) : T (0);
+          r.v[e] = bv;
+          const double zz = di * (double) bv;
+          aRZ[h][e] += (double) bv * zz;
+          aZZ[h][e] += zz * zz;
+        }
+        stp (R + i * ld + vi * W, r);
+        stp (X + i * ld + vi * W, pzero<T> ());
+        stp (P + i * ld + vi * W, pzero<T> ());
+      }
+    }
+  }
+  block_colsum_store<T, CH> (aRZ, lane, group, G, nvec, ld, red, partA);
+  block_colsum_store<T, CH> (aZZ, lane, group, G, nvec, ld, red, partB);
+  double *rz = scal + S_RZ * cap, *al = scal + S_ALPHA * cap;
+  double *be = scal + S_BETA * cap, *n0 = scal + S_NORM0 * cap;
+  int *act = ival + I_ACTIVE * cap, *its = ival + I_ITS * cap;
+  bool last = last_block_reduce2 (partA, partB, ld, counter,
+      [&] (int c, double srz, double szz) {
+        rz[c] = srz;
+        n0[c] = sqrt (szz);
+        act[c] = (c < w && szz > 0.) ? 1 : 0;
+        al[c] = 0.;
+        be[c] = 0.;
+        its[c] = 0;
+      });
+  if (last) {
+    __syncthreads ();
+    if (threadIdx.x == 0) {
+      int cnt = 0;
+      for (int c = 0; c < ld; c++) cnt += act[c];
+      ival[I_NSLOT * cap] = cnt;
+    }
+  }
+}
+
+/* ---- p_new on the fly, q = Z p_new, alpha ------------------------------- */
+template <typename T, int CH>
+__global__ void __launch_bounds__ (ZS_THREADS)
+k_pcg_pq (ZK z, const T *__restrict__ vals, const T *__restrict__ dinv,
+          const T *__restrict__ R, const T *__restrict__ Pold,
+          T *__restrict__ Pnew, T *__restrict__ Qv, int ld, int nvec,
+          int glog, int first, double *partA, unsigned *counter,
+          double *scal, int *ival, int cap)
+{
+  extern __shared__ double red[];
+  ZS_GROUP_SETUP ();
+  const double *beta = scal + S_BETA * cap;
+  T bet[CH][W];
+#pragma unroll
+  for (int h = 0; h < CH; h++)
+#pragma unroll
+    for (int e = 0; e < W; e++) {
+      const int c = (lane + h * G) * W + e;
+      bet[h][e] = (!first && c < ld) ? (T) beta[c] : T (0);
+    }
+  double aPQ[CH][W];
+#pragma unroll
+  for (int h = 0; h < CH; h++)
+#pragma unroll
+    for (int e = 0; e < W; e++) aPQ[h][e] = 0.;
+  for (int64_t i = r0 + group; i < r1; i += ngroups) {
+    T acc[CH][W];
+#pragma unroll
+    for (int h = 0; h < CH; h++)
+#pragma unroll
+      for (int e = 0; e < W; e++) acc[h][e] = T (0);
+    const int64_t k0 = z.rowptr[i], k1 = z.rowptr[i + 1];
+    for (int64_t kb = k0; kb < k1; kb += G) {
+      const int cnt = (int) ((k1 - kb) < G ? (k1 - kb) : G);
+      int mc = 0;
+      T mv = T (0), md = T (0);
+      if (lane < cnt) {
+        mc = z.col[kb + lane];
+        mv = vals[kb + lane];
+        md = dinv[mc];
+      }
+      for (int t = 0; t < cnt; t++) {
+        const int c = __shfl_sync (gmask, mc, t, G);
+        const T v = __shfl_sync (gmask, mv, t, G);
+        const T dj = __shfl_sync (gmask, md, t, G);
+#pragma unroll
+        for (int h = 0; h < CH; h++) {
+          const int vi = lane + h * G;
+          if (vi < nvec) {
+            Pack<T> rj = ldp (R + (int64_t) c * ld + vi * W);
+            Pack<T> pj = first ? pzero<T> () : ldp (Pold + (int64_t) c * ld + vi * W);
+#pragma unroll
+            for (int e = 0; e < W; e++)
+              acc[h][e] = fma (v, fma (dj, rj.v[e], bet[h][e] * pj.v[e]),
+                               acc[h][e]);
+          }
+        }
+      }
+    }
+    const T di = dinv[i];
+#pragma unroll
+    for (int h = 0; h < CH; h++) {
+      const int vi = lane + h * G;
+      if (vi < nvec) {
+        Pack<T> ri = ldp (R + i * ld + vi * W);
+        Pack<T> pi = first ? pzero<T> () : ldp (Pold + i * ld + vi * W);
+        Pack<T> pn, q;
+#pragma unroll
+        for (int e = 0; e < W; e++) {
+          pn.v[e] = fma (di, ri.v[e], bet[h][e] * pi.v[e]);
+          q.v[e] = acc[h][e];
+          aPQ[h][e] += (double) pn.v[e] * (double) q.v[e];
+        }
+        stp (Pnew + i * ld + vi * W, pn);
+        stp (Qv + i * ld + vi * W, q);
+      }
+    }
+  }
+  block_colsum_store<T, CH> (aPQ, lane, group, G, nvec, ld, red, partA);
+  const double *rz = scal + S_RZ * cap;
+  double *al = scal + S_ALPHA * cap;
+  int *act = ival + I_ACTIVE * cap;
+  last_block_reduce (partA, ld, counter, [&] (int c, double pq) {
+    if (act[c]) {
+      if (pq != 0. && isfinite (pq)) al[c] = rz[c] / pq;
+      else { al[c] = 0.; act[c] = 0; }
+    } else {
+      al[c] = 0.;
+    }
+  });
+}
+
+/* ---- x += alpha p, r -= alpha q, dots, beta, convergence ---------------- */
+template <typename T, int CH>
+__global__ void __launch_bounds__ (ZS_THREADS)
+k_pcg_upd (ZK z, const T *__restrict__ dinv, T *X, T *R,
+           const T *__restrict__ Pn, const T *__restrict__ Qv, int ld,
+           int nvec, int glog, double *partA, double *partB,
+           unsigned *counter, double *scal, int *ival, int cap, double rtol,
+           int iter, double *hist)
+{
+  extern __shared__ double red[];
+  ZS_GROUP_SETUP ();
+  const double *alpha = scal + S_ALPHA * cap;
+  T al[CH][W];
+#pragma unroll
+  for (int h = 0; h < CH; h++)
+#pragma unroll
+    for (int e = 0; e < W; e++) {
+      const int c = (lane + h * G) * W + e;
+      al[h][e] = (c < ld) ? (T) alpha[c] : T (0);
+    }
+  double aRZ[CH][W], aZZ[CH][W];
+#pragma unroll
+  for (int h = 0; h < CH; h++)
+#pragma unroll
+    for (int e = 0; e < W; e++) { aRZ[h][e] = 0.; aZZ[h][e] = 0.; }
+  for (int64_t i = r0 + group; i < r1; i += ngroups) {
+    const T di = dinv[i];
+#pragma unroll
+    for (int h = 0; h < CH; h++) {
+      const int vi = lane + h * G;
+      if (vi < nvec) {
+        const int64_t o = i * ld + vi * W;
+        Pack<T> x = ldp (X + o), r = ldp (R + o), p = ldp (Pn + o),
+                q = ldp (Qv + o);
+#pragma unroll
+        for (int e = 0; e < W; e++) {
+          x.v[e] = fma (al[h][e], p.v[e], x.v[e]);
+          r.v[e] = fma (-al[h][e], q.v[e], r.v[e]);
+          const double zz = (double) di * (double) r.v[e];
+          aRZ[h][e] += (double) r.v[e] * zz;
+          aZZ[h][e] += zz * zz;
+        }
+        stp (X + o, x);
+        stp (R + o, r);
+      }
+    }
+  }
+  block_colsum_store<T, CH> (aRZ, lane, group, G, nvec, ld, red, partA);
+  block_colsum_store<T, CH> (aZZ, lane, group, G, nvec, ld, red, partB);
+  double *rz = scal + S_RZ * cap, *be = scal + S_BETA * cap;
+  double *al_g = scal + S_ALPHA * cap;
+  const double *n0 = scal + S_NORM0 * cap;
+  int *act = ival + I_ACTIVE * cap, *its = ival + I_ITS * cap;
+  bool last = last_block_reduce2 (partA, partB, ld, counter,
+      [&] (int c, double srz, double szz) {
+        if (!act[c]) { be[c] = 0.; return; }
+        const double b = (rz[c] != 0.) ? srz / rz[c] : 0.;
+        if (hist != nullptr && c == 0 && iter < 10000) {
+          hist[2 * iter] = al_g[0];
+          hist[2 * iter + 1] = b;
+        }
+        rz[c] = srz;
+        be[c] = b;
+        if (sqrt (szz) <= rtol * n0[c] || srz == 0.) {
+          act[c] = 0;
+          be[c] = 0.;
+          al_g[c] = 0.;
+          its[c] = iter + 1;
+        }
+      });
+  if (last) {
+    __syncthreads ();
+    if (threadIdx.x == 0) {
+      int cnt = 0;
+      for (int c = 0; c < ld; c++) cnt += act[c];
+      ival[I_NSLOT * cap] = cnt;
+    }
+  }
+}
+
+/* ---- Chebyshev: d_new = a d + b D^{-1} r (on the fly at neighbours),
+ *      x += d_new, r_new = r - Z d_new (zsolve_impl.h:108-141) ----------- */
+template <typename T, int CH>
+__global__ void __launch_bounds__ (ZS_THREADS)
+k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ dinv, T *X,
+        const T *__restrict__ Rold, T *__restrict__ Rnew,
+        const T *__restrict__ Dold, T *__restrict__ Dnew, int ld, int nvec,
+        int glog, T a, T b, int first)
+{
+  ZS_GROUP_SETUP ();
+  for (int64_t i = r0 + group; i < r1; i += ngroups) {
+    T acc[CH][W];
+#pragma unroll
+    for (int h = 0; h < CH; h++)
+#pragma unroll
+      for (int e = 0; e < W; e++) acc[h][e] = T (0);
+    const int64_t k0 = z.rowptr[i], k1 = z.rowptr[i + 1];
+    for (int64_t kb = k0; kb < k1; kb += G) {
+      const int cnt = (int) ((k1 - kb) < G ? (k1 - kb) : G);
+      int mc = 0;
+      T mv = T (0), md = T (0);
+      if (lane < cnt) {
+        mc = z.col[kb + lane];
+        mv = vals[kb + lane];
+        md = dinv[mc];
+      }
+      for (int t = 0; t < cnt; t++) {
+        const int c = __shfl_sync (gmask, mc, t, G);
+        const T v = __shfl_sync (gmask, mv, t, G);
+        const T bdj = b * __shfl_sync (gmask, md, t, G);
+#pragma unroll
+        for (int h = 0; h < CH; h++) {
+          const int vi = lane + h * G;
+          if (vi < nvec) {
+            Pack<T> rj = ldp (Rold + (int64_t) c * ld + vi * W);
+            Pack<T> dj = first ? pzero<T> () : ldp (Dold + (int64_t) c * ld + vi * W);
+#pragma unroll
+            for (int e = 0; e < W; e++)
+              acc[h][e] = fma (v, fma (bdj, rj.v[e], a * dj.v[e]), acc[h][e]);
+          }
+        }
+      }
+    }
+    const T bdi = b * dinv[i];
+#pragma unroll
+    for (int h = 0; h < CH; h++) {
+      const int vi = lane + h * G;
+      if (vi < nvec) {
+        const int64_t o = i * ld + vi * W;
+        Pack<T> ri = ldp (Rold + o), x = ldp (X + o);
+        Pack<T> di = first ? pzero<T> () : ldp (Dold + o);
+        Pack<T> dn, rn;
+#pragma unroll
+        for (int e = 0; e < W; e++) {
+          dn.v[e] = fma (bdi, ri.v[e], a * di.v[e]);
+          x.v[e] += dn.v[e];
+          rn.v[e] = ri.v[e] - acc[h][e];
+        }
+        stp (X + o, x);
+        stp (Dnew + o, dn);
+        stp (Rnew + o, rn);
+      }
+    }
+  }
+}
+
+/* ---- FP64 residual, R = S B - Z X (pads zero), per-column ||D^{-1} R|| and
+ * ||D^{-1} S B|| (refinement and tests) ---------------------------------- */
+template <typename TO, int CH>
+__global__ void __launch_bounds__ (ZS_THREADS)
+k_zresid (ZK z, const double *__restrict__ vals,
+          const double *__restrict__ dinv, const double *__restrict__ Bm,
+          int ldb, const double *__restrict__ rs_in,
+          const double *__restrict__ X, int ldx, TO *Rout, int ldr, int nvec,
+          int glog, int w, double *partA, double *partB, unsigned *counter,
+          double *out_r, double *out_b)
+{
+  extern __shared__ double red[];
+  using T = double;
+  ZS_GROUP_SETUP ();
+  double aR[CH][W], aB[CH][W];
+#pragma unroll
+  for (int h = 0; h < CH; h++)
+#pragma unroll
+    for (int e = 0; e < W; e++) { aR[h][e] = 0.; aB[h][e] = 0.; }
+  const int ld = nvec * W;
+  for (int64_t i = r0 + group; i < r1; i += ngroups) {
+    double acc[CH][W];
+#pragma unroll
+    for (int h = 0; h < CH; h++)
+#pragma unroll
+      for (int e = 0; e < W; e++) acc[h][e] = 0.;
+    for (int64_t k = z.rowptr[i]; k < z.rowptr[i + 1]; k++) {
+      const int c = z.col[k];
+      const double v = vals[k];
+#pragma unroll
+      for (int h = 0; h < CH; h++) {
+        const int vi = lane + h * G;
+        if (vi < nvec) {
+          Pack<double> xj = ldp (X + (int64_t) c * ldx + vi * W);
+#pragma unroll
+          for (int e = 0; e < W; e++) acc[h][e] = fma (v, xj.v[e], acc[h][e]);
+        }
+      }
+    }
+    const double sc = rs_in ? rs_in[i] : 1.0, di = dinv[i];
+#pragma unroll
+    for (int h = 0; h < CH; h++) {
+      const int vi = lane + h * G;
+      if (vi < nvec) {
+#pragma unroll
+        for (int e = 0; e < W; e++) {
+          const int c = vi * W + e;
+          const double bv = (c < w) ? sc * Bm[i * ldb + c] : 0.;
+          const double r = (c < w) ? bv - acc[h][e] : 0.;
+          aR[h][e] += (di * r) * (di * r);
+          aB[h][e] += (di * bv) * (di * bv);
+          if (Rout) Rout[i * ldr + c] = (TO) r;
+        }
+      }
+    }
+  }
+  if (out_r == nullptr) return;
+  block_colsum_store<double, CH> (aR, lane, group, G, nvec, ld, red, partA);
+  block_colsum_store<double, CH> (aB, lane, group, G, nvec, ld, red, partB);
+  last_block_reduce2 (partA, partB, ld, counter,
+                      [&] (int c, double sr, double sb) {
+                        out_r[c] = sqrt (sr);
+                        if (out_b) out_b[c] = sqrt (sb);
+                      });
+}
+
+/* ---- host side ------------------------------------------------------------ */
+
+/* opt a kernel into > 48 KB of dynamic shared memory, once per kernel */
+static void
+smem_prep (const void *fn, int bytes)
+{
+  static std::mutex mu;
+  static std::unordered_map<const void *, int> done;
+  if (bytes <= 48 * 1024) return;
+  std::lock_guard<std::mutex> lk (mu);
+  auto it = done.find (fn);
+  if (it != done.end () && it->second >= bytes) return;
+  cudaFuncSetAttribute (fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                        bytes);
+  done[fn] = bytes;
+}
+
+template <typename K>
+static void
+set_smem_attr (K kern, int bytes)
+{
+  smem_prep ((const void *) kern, bytes);
+}
+
+static int
+zs_smem_bytes (int glog, int ld)
+{
+  return (ZS_THREADS >> glog) * ld * (int) sizeof (double);
+}
+
+int
+ZWork::alloc (int64_t n_, int cap_, int is32_)
+{
+  cap_ = round_ld (cap_);
+  if (n_ == n && cap_ <= cap && is32_ == is32 && X.p) return 0;
+  n = n_;
+  cap = cap_;
+  is32 = is32_;
+  const size_t es = is32 ? 4 : 8;
+  const size_t blk = (size_t) n * cap * es;
+  LGH_TRY (X.alloc (blk));
+  LGH_TRY (R.alloc (blk));
+  LGH_TRY (P0.alloc (blk));
+  LGH_TRY (P1.alloc (blk));
+  LGH_TRY (Q.alloc (blk));
+  nblocks = num_sms () * 4;
+  LGH_TRY (partA.alloc ((size_t) cap * nblocks));
+  LGH_TRY (partB.alloc ((size_t) cap * nblocks));
+  LGH_TRY (scal.alloc ((size_t) cap * S_NSLOT));
+  LGH_TRY (ival.alloc ((size_t) cap * I_NSLOT + 8));
+  LGH_TRY (counters.alloc (8));
+  LGH_TRY (hist.alloc (2 * 10000 + 16));
+  LGH_CUDA (cudaMemset (counters.p, 0, 8 * sizeof (unsigned)));
+  LGH_CUDA (cudaMemset (ival.p, 0, ((size_t) cap * I_NSLOT + 8) * sizeof (int)));
+  return 0;
+}
+
+template <typename T>
+static const T *
+zvals (const Csr &Z)
+{
+  if constexpr (std::is_same<T, double>::value) return Z.vals;
+  else return Z.vals32;
+}
+
+template <typename T>
+static const T *
+zdinv (const Csr &Z)
+{
+  if constexpr (std::is_same<T, double>::value) return Z.dinv;
+  else return Z.dinv32;
+}
+
+#define ZS_DISPATCH(CHV, ...)                                                \
+  switch (CHV) {                                                             \
+  case 1: { constexpr int CH_ = 1; __VA_ARGS__; } break;                     \
+  case 2: { constexpr int CH_ = 2; __VA_ARGS__; } break;                     \
+  case 3: { constexpr int CH_ = 3; __VA_ARGS__; } break;                     \
+  case 4: { constexpr int CH_ = 4; __VA_ARGS__; } break;                     \
+  case 5: { constexpr int CH_ = 5; __VA_ARGS__; } break;                     \
+  case 6: { constexpr int CH_ = 6; __VA_ARGS__; } break;                     \
+  case 7: { constexpr int CH_ = 7; __VA_ARGS__; } break;                     \
+  case 8: { constexpr int CH_ = 8; __VA_ARGS__; } break;                     \
+  default:                                                                   \
+    return set_error (LGH_ERR_SUP, "zsolve: chunking %d unsupported", CHV);  \
+  }
+
+template <typename T>
+int
+zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
+              int64_t n, int w, const T *Xin, int ldx,
+              const double *rs_in, T *Y, int ldy, const double *rs_out,
+              ZsolveStats *st, int record_hist, cudaStream_t s)
+{
+  constexpr int W = Pack<T>::W;
+  (void) mg;
+  if (w <= 0 || n == 0) return 0;
+  LGH_CHECK (cfg.mode != 3, LGH_ERR_SUP, "zsolve: mode 3 not available");
+  LGH_CHECK (Z.dinv != nullptr, LGH_ERR_ARG_WRONGSTATE, "zsolve: Z has no diagonal");
+  const double t0 = wall ();
+  int tile = ws.cap;
+  if (cfg.mode >= 2 && cfg.tile > 0) tile = std::min (tile, round_ld (cfg.tile));
+  tile = std::max (4, tile & ~3);
+  const int maxcols = 32 * ZS_MAXCH * W;
+  tile = std::min (tile, maxcols);
+  const T *vals = zvals<T> (Z);
+  const T *dinv = zdinv<T> (Z);
+  ZK zk{ Z.n, Z.rowptr, Z.colidx };
+  T *bX = (T *) ws.X.p, *bR = (T *) ws.R.p, *bP0 = (T *) ws.P0.p,
+    *bP1 = (T *) ws.P1.p, *bQ = (T *) ws.Q.p;
+  std::vector<int> its_h;
+
+  for (int c0 = 0; c0 < w; c0 += tile) {
+    const int wt = std::min (tile, w - c0);
+    const int ldt = round_ld (wt);
+    const int nvec = ldt / W;
+    int glog, ch;
+    row_group_shape (nvec, glog, ch);
+    const int grid = std::min (row_grid (n, glog), ws.nblocks);
+    const int smem = zs_smem_bytes (glog, ldt);
+    const int cap = ws.cap;
+    int *nact = ws.ival.p + I_NSLOT * cap;
+
+    ZS_DISPATCH (ch, {
+      auto kf = k_pcg_init<T, CH_>;
+      set_smem_attr (kf, smem);
+      kf<<<grid, ZS_THREADS, smem, s>>> (zk, dinv, Xin + c0, ldx, rs_in, bX,
+                                         bR, bP0, ldt, nvec, glog, wt,
+                                         ws.partA.p, ws.partB.p,
+                                         ws.counters.p, ws.scal.p, ws.ival.p,
+                                         cap);
+    });
+    LGH_LAUNCH_CHECK ();
+
+    int iters = 0;
+    if (cfg.mode <= 1) {
+      T *Pold = bP0, *Pnew = bP1;
+      int h_nact = 1;
+      for (int it = 0; it < cfg.maxit; it++) {
+        ZS_DISPATCH (ch, {
+          auto k1 = k_pcg_pq<T, CH_>;
+          set_smem_attr (k1, smem);
+          k1<<<grid, ZS_THREADS, smem, s>>> (zk, vals, dinv, bR, Pold, Pnew,
+                                             bQ, ldt, nvec, glog, it == 0,
+                                             ws.partA.p, ws.counters.p,
+                                             ws.scal.p, ws.ival.p, cap);
+          auto k2 = k_pcg_upd<T, CH_>;
+          set_smem_attr (k2, smem);
+          k2<<<grid, ZS_THREADS, smem, s>>> (zk, dinv, bX, bR, Pnew, bQ, ldt,
+                                             nvec, glog, ws.partA.p,
+                                             ws.partB.p, ws.counters.p + 1,
+                                             ws.scal.p, ws.ival.p, cap,
+                                             cfg.rtol, it,
+                                             record_hist ? ws.hist.p : nullptr);
+        });
+        LGH_LAUNCH_CHECK ();
+        std::swap (Pold, Pnew);
+        iters = it + 1;
+        if (iters % cfg.check_every == 0 || iters == cfg.maxit || iters <= 2) {
+          LGH_CUDA (cudaMemcpyAsync (&h_nact, nact, sizeof (int),
+                                     cudaMemcpyDeviceToHost, s));
+          LGH_CUDA (cudaStreamSynchronize (s));
+          if (h_nact == 0) break;
+        }
+      }
+      if (st) {
+        its_h.resize (ldt);
+        LGH_CUDA (cudaMemcpyAsync (its_h.data (), ws.ival.p + I_ITS * cap,
+                                   ldt * sizeof (int), cudaMemcpyDeviceToHost, s));
+        std::vector<int> act_h (ldt);
+        LGH_CUDA (cudaMemcpyAsync (act_h.data (), ws.ival.p + I_ACTIVE * cap,
+                                   ldt * sizeof (int), cudaMemcpyDeviceToHost, s));
+        LGH_CUDA (cudaStreamSynchronize (s));
+        for (int c = 0; c < wt; c++) st->col_iters += act_h[c] ? iters : its_h[c];
+        if (h_nact > 0) st->last_maxit_hit = 1;
+        st->cols += wt;
+      }
+    } else {
+      /* Chebyshev, fixed count (zsolve_impl.h:113-139) */
+      const double theta = 0.5 * (cfg.lmax + cfg.lmin);
+      const double delta = 0.5 * (cfg.lmax - cfg.lmin);
+      const double sigma1 = theta / delta;
+      double rho_old = 1.0 / sigma1;
+      T *Ro = bR, *Rn = bQ, *Do = bP0, *Dn = bP1;
+      for (int k = 1; k <= cfg.nit; k++) {
+        double a, b;
+        if (k == 1) { a = 0.; b = 1.0 / theta; }
+        else {
+          const double rho = 1.0 / (2.0 * sigma1 - rho_old);
+          a = rho * rho_old;
+          b = 2.0 * rho / delta;
+          rho_old = rho;
+        }
+        ZS_DISPATCH (ch, {
+          k_cheb<T, CH_><<<grid, ZS_THREADS, 0, s>>> (zk, vals, dinv, bX, Ro, Rn,
+                                                      Do, Dn, ldt, nvec, glog,
+                                                      (T) a, (T) b, k == 1);
+        });
+        LGH_LAUNCH_CHECK ();
+        std::swap (Ro, Rn);
+        std::swap (Do, Dn);
+      }
+      iters = cfg.nit;
+      if (st) { st->col_iters += (long) iters * wt; st->cols += wt; }
+    }
+    if (st) st->block_iters += iters;
+    LGH_TRY (launch_rowscale<T> (n, wt, rs_out, bX, ldt, Y + c0, ldy, s));
+  }
+  if (st) {
+    LGH_CUDA (cudaStreamSynchronize (s));
+    st->calls++;
+    st->seconds += wall () - t0;
+  }
+  return 0;
+}
+
+template int zsolve_block<double> (const Csr &, const ZsolveCfg &, Hierarchy *,
+                                   ZWork &, int64_t, int, const double *, int,
+                                   const double *, double *, int,
+                                   const double *, ZsolveStats *, int,
+                                   cudaStream_t);
+template int zsolve_block<float> (const Csr &, const ZsolveCfg &, Hierarchy *,
+                                  ZWork &, int64_t, int, const float *, int,
+                                  const double *, float *, int, const double *,
+                                  ZsolveStats *, int, cudaStream_t);
+
+/* per-column ||D^{-1}(S B - Z X)||, ||D^{-1} S B|| ; optional R output */
+template <typename TO>
+int
+zresid_launch (const Csr &Z, int64_t n, int w, const double *Bm, int ldb,
+               const double *rs_in, const double *X, int ldx, TO *Rout,
+               int ldr, double *out_r, double *out_b, double *partA,
+               double *partB, unsigned *counter, int nblocks, cudaStream_t s)
+{
+  const int ld = round_ld (w);
+  const int nvec = ld / 2;
+  int glog, ch;
+  row_group_shape (nvec, glog, ch);
+  const int grid = std::min (row_grid (n, glog), nblocks);
+  const int smem = zs_smem_bytes (glog, ld);
+  ZK zk{ Z.n, Z.rowptr, Z.colidx };
+  ZS_DISPATCH (ch, {
+    auto kf = k_zresid<TO, CH_>;
+    set_smem_attr (kf, smem);
+    kf<<<grid, ZS_THREADS, smem, s>>> (zk, Z.vals, Z.dinv, Bm, ldb, rs_in, X,
+                                       ldx, Rout, ldr, nvec, glog, w, partA,
+                                       partB, counter, out_r, out_b);
+  });
+  LGH_LAUNCH_CHECK ();
+  return 0;
+}
+
+template int zresid_launch<double> (const Csr &, int64_t, int, const double *,
+                                    int, const double *, const double *, int,
+                                    double *, int, double *, double *,
+                                    double *, double *, unsigned *, int,
+                                    cudaStream_t);
+template int zresid_launch<float> (const Csr &, int64_t, int, const double *,
+                                   int, const double *, const double *, int,
+                                   float *, int, double *, double *, double *,
+                                   double *, unsigned *, int, cudaStream_t);
+
+int
+zsolve_residual_norms (const Csr &Z, int64_t n, int w, const double *Bm,
+                       int ldb, const double *X, int ldx, double *out,
+                       cudaStream_t s)
+{
+  const int ld = round_ld (w);
+  DBuf<double> pa, pb;
+  DBuf<unsigned> cnt;
+  const int nb = num_sms () * 4;
+  LGH_TRY (pa.alloc ((size_t) ld * nb));
+  LGH_TRY (pb.alloc ((size_t) ld * nb));
+  LGH_TRY (cnt.alloc (4));
+  LGH_CUDA (cudaMemsetAsync (cnt.p, 0, 4 * sizeof (unsigned), s));
+  LGH_TRY (zresid_launch<double> (Z, n, w, Bm, ldb, nullptr, X, ldx,
+                                  (double *) nullptr, 0, out, nullptr, pa.p,
+                                  pb.p, cnt.p, nb, s));
+  LGH_CUDA (cudaStreamSynchronize (s));
+  return 0;
+}
+
+} /* namespace lgh */

@@ -1,0 +1,588 @@
+"""Python mirror of the B200 GLR library's C ABI (include/lgh_b200.h).
+
+A thin ctypes layer over ``liblgh_b200.so``: the same objects and calls as
+the reference's C API (lgh_prior_* / lgh_glr_*, include/lgpsf_hessian/
+prior.h and glr.h), with numpy arrays in and out.  Every call goes to the
+CUDA library; there is no CPU implementation here, and importing this
+module without the built library raises.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "liblgh_b200.so")
+
+P = ctypes.c_void_p
+I64 = ctypes.c_int64
+c_dbl_p = ctypes.POINTER(ctypes.c_double)
+
+LGH_MEM_HOST, LGH_MEM_DEVICE = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+ERR_NAMES = {0: "SUCCESS", 55: "ERR_MEM", 56: "ERR_SUP", 58: "ERR_ORDER",
+             60: "ERR_ARG_SIZ", 62: "ERR_ARG_WRONG",
+             63: "ERR_ARG_OUTOFRANGE", 73: "ERR_ARG_WRONGSTATE",
+             76: "ERR_LIB", 85: "ERR_ARG_NULL", 91: "ERR_NOT_CONVERGED",
+             97: "ERR_GPU"}
+
+
+class LghError(RuntimeError):
+    def __init__(self, code, where, msg):
+        super().__init__("%s failed: %s (%d): %s"
+                         % (where, ERR_NAMES.get(code, "?"), code, msg))
+        self.code = code
+
+
+class GlrOpts(ctypes.Structure):
+    """lgh_glr_opts_t, field for field (include/lgpsf_hessian/glr.h:68-86)."""
+
+    _fields_ = [("ell", ctypes.c_int), ("q_power", ctypes.c_int),
+                ("trunc_abs", ctypes.c_double),
+                ("trunc_rel", ctypes.c_double), ("treat", ctypes.c_int),
+                ("seed", ctypes.c_ulong), ("backend", ctypes.c_int),
+                ("nb", ctypes.c_int), ("panel", ctypes.c_int),
+                ("grid2d", ctypes.c_int), ("check", ctypes.c_int)]
+
+
+class GlrReport(ctypes.Structure):
+    """lgh_glr_report_t (include/lgpsf_hessian/glr.h:90-102)."""
+
+    _fields_ = [("kept", ctypes.c_int), ("lam_abs_max", ctypes.c_double),
+                ("lam_raw_min", ctypes.c_double),
+                ("lam_raw_max", ctypes.c_double),
+                ("next_abs", ctypes.c_double),
+                ("n_negative_raw", ctypes.c_int),
+                ("resid_max", ctypes.c_double),
+                ("t_operator", ctypes.c_double),
+                ("t_dense", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class PriorMatOpts(ctypes.Structure):
+    """lgh_prior_mat_opts_t (include/lgpsf_hessian/prior.h:76-89)."""
+
+    _fields_ = [("ksp_rtol", ctypes.c_double),
+                ("blocked_mode", ctypes.c_int), ("tile", ctypes.c_int),
+                ("cheb_rtol", ctypes.c_double),
+                ("smax_krylov", ctypes.c_int),
+                ("smoother_top", ctypes.c_double),
+                ("nu_force", ctypes.c_int), ("verbose", ctypes.c_int)]
+
+
+class ExecOpts(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int),
+                ("inner_rtol", ctypes.c_double),
+                ("max_refine", ctypes.c_int), ("verbose", ctypes.c_int)]
+
+
+class GlrStats(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("ell", ctypes.c_int),
+                ("kept", ctypes.c_int), ("precision", ctypes.c_int),
+                ("t_build", ctypes.c_double), ("t_sketch", ctypes.c_double),
+                ("t_zsolve", ctypes.c_double), ("t_spmm", ctypes.c_double),
+                ("t_orth", ctypes.c_double), ("t_eig", ctypes.c_double),
+                ("t_check", ctypes.c_double),
+                ("zsolve_calls", ctypes.c_long),
+                ("zsolve_iters", ctypes.c_long),
+                ("zsolve_mean_col_iters", ctypes.c_double),
+                ("device_bytes", ctypes.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+VEC_FN = ctypes.CFUNCTYPE(None, P, P, P)
+MAT_FN = ctypes.CFUNCTYPE(None, P, P, P)
+
+
+class PriorCallbacks(ctypes.Structure):
+    _fields_ = [("applyZ", VEC_FN), ("applyZt", VEC_FN), ("solveZ", VEC_FN),
+                ("solveZt", VEC_FN), ("solveZ_blocked", MAT_FN),
+                ("solveZt_blocked", MAT_FN), ("ctx", P)]
+
+
+_L = None
+
+# every function the header declares: name -> (restype, argtypes)
+SIGNATURES = {
+    "lgh_last_error": (ctypes.c_char_p, []),
+    "lgh_mat_create_csr": (ctypes.c_int, [I64, P, P, P, ctypes.c_int,
+                                          ctypes.POINTER(P)]),
+    "lgh_mat_create_dense": (ctypes.c_int, [I64, P, I64, ctypes.c_int,
+                                            ctypes.POINTER(P)]),
+    "lgh_mat_get_info": (ctypes.c_int, [P, ctypes.POINTER(I64),
+                                        ctypes.POINTER(I64)]),
+    "lgh_mat_mult": (ctypes.c_int, [P, P, P]),
+    "lgh_mat_dense_get_array": (ctypes.c_int, [P, ctypes.POINTER(P),
+                                               ctypes.POINTER(I64),
+                                               ctypes.POINTER(ctypes.c_int),
+                                               ctypes.POINTER(I64)]),
+    "lgh_mat_destroy": (ctypes.c_int, [ctypes.POINTER(P)]),
+    "lgh_vec_create": (ctypes.c_int, [I64, ctypes.POINTER(P)]),
+    "lgh_vec_create_with_array": (ctypes.c_int, [I64, P, ctypes.POINTER(P)]),
+    "lgh_vec_get_array": (ctypes.c_int, [P, ctypes.POINTER(P),
+                                         ctypes.POINTER(I64)]),
+    "lgh_vec_set_host": (ctypes.c_int, [P, P]),
+    "lgh_vec_get_host": (ctypes.c_int, [P, P]),
+    "lgh_vec_destroy": (ctypes.c_int, [ctypes.POINTER(P)]),
+    "lgh_prior_create_callbacks": (ctypes.c_int, [
+        P, ctypes.POINTER(PriorCallbacks), ctypes.POINTER(P)]),
+    "lgh_prior_mat_opts_default": (PriorMatOpts, []),
+    "lgh_prior_create_mat": (ctypes.c_int, [P, P, ctypes.POINTER(PriorMatOpts),
+                                            ctypes.POINTER(P)]),
+    "lgh_prior_create_ksp": (ctypes.c_int, [P, P,
+                                            ctypes.POINTER(PriorMatOpts),
+                                            ctypes.POINTER(P)]),
+    "lgh_prior_destroy": (None, [P]),
+    "lgh_prior_apply": (ctypes.c_int, [P, P, P]),
+    "lgh_prior_solve": (ctypes.c_int, [P, P, P]),
+    "lgh_prior_solve_block": (ctypes.c_int, [P, ctypes.c_int, P, I64, P,
+                                             I64]),
+    "lgh_prior_get_info": (ctypes.c_int, [P, c_dbl_p]),
+    "lgh_glr_opts_default": (GlrOpts, []),
+    "lgh_glr_compute": (ctypes.c_int, [P, P, ctypes.POINTER(GlrOpts),
+                                       ctypes.POINTER(P),
+                                       ctypes.POINTER(GlrReport)]),
+    "lgh_glr_extend": (ctypes.c_int, [P, ctypes.c_int,
+                                      ctypes.POINTER(GlrReport)]),
+    "lgh_glr_destroy": (None, [P]),
+    "lgh_glr_solve": (ctypes.c_int, [P, ctypes.c_double, P, P]),
+    "lgh_glr_apply": (ctypes.c_int, [P, ctypes.c_double, P, P]),
+    "lgh_glr_sample": (ctypes.c_int, [P, ctypes.c_double, P, P]),
+    "lgh_glr_factor": (ctypes.c_int, [P, ctypes.c_double, ctypes.c_int, P,
+                                      P]),
+    "lgh_glr_logdet": (ctypes.c_double, [P, ctypes.c_double]),
+    "lgh_glr_pow": (ctypes.c_int, [P, ctypes.c_double, ctypes.c_double, P,
+                                   P]),
+    "lgh_glr_filter": (ctypes.c_int, [P, c_dbl_p, ctypes.c_double, P, P]),
+    "lgh_glr_eigs": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(c_dbl_p)]),
+    "lgh_exec_opts_default": (ExecOpts, []),
+    "lgh_glr_compute_ex": (ctypes.c_int, [P, P, ctypes.POINTER(GlrOpts),
+                                          ctypes.POINTER(ExecOpts),
+                                          ctypes.POINTER(P),
+                                          ctypes.POINTER(GlrReport)]),
+    "lgh_glr_get_stats": (ctypes.c_int, [P, ctypes.POINTER(GlrStats)]),
+    "lgh_glr_get_U": (ctypes.c_int, [P, P, I64]),
+    "lgh_glr_solve_batch": (ctypes.c_int, [P, ctypes.c_int, c_dbl_p,
+                                           ctypes.c_int, P, I64, P, I64]),
+    "lgh_glr_sample_batch": (ctypes.c_int, [P, ctypes.c_int, c_dbl_p,
+                                            ctypes.c_int, P, I64, P, I64]),
+    "lgh_glr_logdet_batch": (ctypes.c_int, [P, ctypes.c_int, c_dbl_p,
+                                            c_dbl_p]),
+    "lgh_test_sketch": (ctypes.c_int, [ctypes.c_uint64, I64, I64,
+                                       ctypes.c_int, P]),
+    "lgh_test_rng_state": (ctypes.c_int, [ctypes.c_uint64, I64, I64,
+                                          ctypes.c_int, P]),
+    "lgh_test_spmm": (ctypes.c_int, [P, ctypes.c_int, P, P, ctypes.c_int]),
+    "lgh_test_zsolve": (ctypes.c_int, [P, ctypes.c_int, P, P, ctypes.c_int]),
+    "lgh_test_gram": (ctypes.c_int, [I64, ctypes.c_int, P, P]),
+    "lgh_test_gemm_nn": (ctypes.c_int, [I64, ctypes.c_int, ctypes.c_int, P,
+                                        P, P]),
+    "lgh_test_potrf": (ctypes.c_int, [ctypes.c_int, P, ctypes.c_int, P, P,
+                                      P]),
+    "lgh_test_syev": (ctypes.c_int, [ctypes.c_int, P, P, P, P]),
+}
+
+
+def load(path=None):
+    """Load the CUDA library (raises if it has not been built)."""
+    global _L
+    if _L is not None:
+        return _L
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise RuntimeError("liblgh_b200.so not built (%s): run "
+                           "__graft_entry__.build() or make -C "
+                           "lgpsf-hessian_b200" % path)
+    L = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _L = L
+    return L
+
+
+def _chk(rc, where):
+    if rc != 0:
+        msg = load().lgh_last_error().decode(errors="replace")
+        raise LghError(rc, where, msg)
+
+
+def glr_opts(**kw):
+    o = load().lgh_glr_opts_default()
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def prior_opts(**kw):
+    o = load().lgh_prior_mat_opts_default()
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def exec_opts(**kw):
+    o = load().lgh_exec_opts_default()
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class Vec:
+    """Device vector handle (the reference's Vec)."""
+
+    def __init__(self, n=None, data=None, handle=None):
+        L = load()
+        self.h = P()
+        if handle is not None:
+            self.h = handle
+            self.owned = False
+            nn = I64()
+            _chk(L.lgh_vec_get_array(self.h, None, ctypes.byref(nn)),
+                 "lgh_vec_get_array")
+            self.n = nn.value
+            return
+        if data is not None:
+            data = np.ascontiguousarray(data, dtype=np.float64)
+            n = data.shape[0]
+        _chk(L.lgh_vec_create(int(n), ctypes.byref(self.h)), "lgh_vec_create")
+        self.n = int(n)
+        self.owned = True
+        if data is not None:
+            self.set(data)
+
+    def set(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        assert a.shape[0] == self.n
+        _chk(load().lgh_vec_set_host(self.h, a.ctypes.data), "lgh_vec_set_host")
+
+    def get(self):
+        out = np.empty(self.n)
+        _chk(load().lgh_vec_get_host(self.h, out.ctypes.data),
+             "lgh_vec_get_host")
+        return out
+
+    def ptr(self):
+        p = P()
+        _chk(load().lgh_vec_get_array(self.h, ctypes.byref(p), None),
+             "lgh_vec_get_array")
+        return p.value
+
+    def __del__(self):
+        if getattr(self, "owned", False) and _L is not None and self.h:
+            _L.lgh_vec_destroy(ctypes.byref(self.h))
+
+
+class DeviceBlock:
+    """A column-major n x m device block backed by one Vec of n*m."""
+
+    def __init__(self, n, m, data=None):
+        self.n, self.m = n, m
+        self.v = Vec(n * m)
+        if data is not None:
+            self.set(data)
+
+    def set(self, a):
+        a = np.asarray(a, dtype=np.float64).reshape(self.n, self.m)
+        self.v.set(np.asfortranarray(a).reshape(-1, order="F"))
+
+    def get(self):
+        return self.v.get().reshape(self.m, self.n).T.copy()
+
+    def ptr(self):
+        return self.v.ptr()
+
+
+class Mat:
+    """Device CSR operator (the reference's Mat for B and Z)."""
+
+    def __init__(self, csr=None, dense=None):
+        L = load()
+        self.h = P()
+        if dense is not None:
+            D = np.asfortranarray(dense, dtype=np.float64)
+            _chk(L.lgh_mat_create_dense(D.shape[0], D.ctypes.data, D.shape[0],
+                                        LGH_MEM_HOST, ctypes.byref(self.h)),
+                 "lgh_mat_create_dense")
+            self.n = D.shape[0]
+        else:
+            rp = np.ascontiguousarray(csr["rowptr"], dtype=np.int64)
+            ci = np.ascontiguousarray(csr["colidx"], dtype=np.int32)
+            va = np.ascontiguousarray(csr["vals"], dtype=np.float64)
+            _chk(L.lgh_mat_create_csr(len(rp) - 1, rp.ctypes.data,
+                                      ci.ctypes.data, va.ctypes.data,
+                                      LGH_MEM_HOST, ctypes.byref(self.h)),
+                 "lgh_mat_create_csr")
+            self.n = len(rp) - 1
+
+    def info(self):
+        n, nnz = I64(), I64()
+        _chk(load().lgh_mat_get_info(self.h, ctypes.byref(n),
+                                     ctypes.byref(nnz)), "lgh_mat_get_info")
+        return n.value, nnz.value
+
+    def mult(self, x):
+        vx, vy = Vec(data=x), Vec(len(x))
+        _chk(load().lgh_mat_mult(self.h, vx.h, vy.h), "lgh_mat_mult")
+        return vy.get()
+
+    def __del__(self):
+        if _L is not None and getattr(self, "h", None):
+            _L.lgh_mat_destroy(ctypes.byref(self.h))
+
+
+class Prior:
+    """lgh_prior_t: Mat path (Z + mass) or callbacks path."""
+
+    def __init__(self, Z=None, mass=None, opts=None, callbacks=None):
+        L = load()
+        self.h = P()
+        self.mass = Vec(data=mass)
+        self.n = self.mass.n
+        self._keep = []
+        if callbacks is not None:
+            cb = PriorCallbacks()
+            for k in ("applyZ", "applyZt", "solveZ", "solveZt"):
+                fn = callbacks.get(k)
+                setattr(cb, k, VEC_FN(fn) if fn else VEC_FN())
+            for k in ("solveZ_blocked", "solveZt_blocked"):
+                fn = callbacks.get(k)
+                setattr(cb, k, MAT_FN(fn) if fn else MAT_FN())
+            cb.ctx = None
+            self._keep.append(cb)
+            _chk(L.lgh_prior_create_callbacks(self.mass.h, ctypes.byref(cb),
+                                              ctypes.byref(self.h)),
+                 "lgh_prior_create_callbacks")
+        else:
+            o = opts if opts is not None else prior_opts()
+            self.Z = Z
+            _chk(L.lgh_prior_create_mat(Z.h, self.mass.h, ctypes.byref(o),
+                                        ctypes.byref(self.h)),
+                 "lgh_prior_create_mat")
+
+    def info(self):
+        out = np.zeros(8)
+        _chk(load().lgh_prior_get_info(self.h, out.ctypes.data_as(c_dbl_p)),
+             "lgh_prior_get_info")
+        return dict(emin=out[0], emax=out[1], lmin=out[2], lmax=out[3],
+                    nit=int(out[4]), bound_its=int(out[5]),
+                    mean_col_iters=out[6], calls=int(out[7]))
+
+    def apply(self, x):
+        vx, vy = Vec(data=x), Vec(self.n)
+        _chk(load().lgh_prior_apply(self.h, vx.h, vy.h), "lgh_prior_apply")
+        return vy.get()
+
+    def solve(self, x):
+        vx, vy = Vec(data=x), Vec(self.n)
+        _chk(load().lgh_prior_solve(self.h, vx.h, vy.h), "lgh_prior_solve")
+        return vy.get()
+
+    def solve_block(self, X):
+        X = np.asarray(X, dtype=np.float64)
+        m = X.shape[1]
+        bx, by = DeviceBlock(self.n, m, X), DeviceBlock(self.n, m)
+        _chk(load().lgh_prior_solve_block(self.h, m, bx.ptr(), self.n,
+                                          by.ptr(), self.n),
+             "lgh_prior_solve_block")
+        return by.get()
+
+    def __del__(self):
+        if _L is not None and getattr(self, "h", None):
+            _L.lgh_prior_destroy(self.h)
+            self.h = P()
+
+
+class Glr:
+    """lgh_glr_t: build, extend and the downstream operations."""
+
+    def __init__(self, B, prior, opts=None, exec=None):
+        L = load()
+        self.h = P()
+        self.B, self.prior = B, prior
+        o = opts if opts is not None else glr_opts()
+        rep = GlrReport()
+        if exec is None:
+            _chk(L.lgh_glr_compute(B.h, prior.h, ctypes.byref(o),
+                                   ctypes.byref(self.h), ctypes.byref(rep)),
+                 "lgh_glr_compute")
+        else:
+            _chk(L.lgh_glr_compute_ex(B.h, prior.h, ctypes.byref(o),
+                                      ctypes.byref(exec), ctypes.byref(self.h),
+                                      ctypes.byref(rep)), "lgh_glr_compute_ex")
+        self.report = rep.as_dict()
+        self.n = prior.n
+
+    def extend(self, k):
+        rep = GlrReport()
+        _chk(load().lgh_glr_extend(self.h, int(k), ctypes.byref(rep)),
+             "lgh_glr_extend")
+        self.report = rep.as_dict()
+        return self.report
+
+    def eigs(self):
+        nk = ctypes.c_int()
+        p = c_dbl_p()
+        _chk(load().lgh_glr_eigs(self.h, ctypes.byref(nk), ctypes.byref(p)),
+             "lgh_glr_eigs")
+        if nk.value == 0:
+            return np.zeros(0)
+        return np.ctypeslib.as_array(p, shape=(nk.value,)).copy()
+
+    def stats(self):
+        st = GlrStats()
+        _chk(load().lgh_glr_get_stats(self.h, ctypes.byref(st)),
+             "lgh_glr_get_stats")
+        return st.as_dict()
+
+    def U(self):
+        k = len(self.eigs())
+        b = DeviceBlock(self.n, max(k, 1))
+        _chk(load().lgh_glr_get_U(self.h, b.ptr(), self.n), "lgh_glr_get_U")
+        return b.get()[:, :k]
+
+    def _vv(self, fname, c, v, *extra):
+        vx, vy = Vec(data=v), Vec(self.n)
+        f = getattr(load(), fname)
+        _chk(f(self.h, c, *extra, vx.h, vy.h), fname)
+        return vy.get()
+
+    def solve(self, c, rhs):
+        return self._vv("lgh_glr_solve", c, rhs)
+
+    def sample(self, c, xi):
+        return self._vv("lgh_glr_sample", c, xi)
+
+    def apply(self, c, v):
+        return self._vv("lgh_glr_apply", c, v)
+
+    def factor(self, c, which, v):
+        return self._vv("lgh_glr_factor", c, v, int(which))
+
+    def pow(self, c, p, v):
+        return self._vv("lgh_glr_pow", c, v, float(p))
+
+    def filter(self, f_lam, f_c, v):
+        f = np.ascontiguousarray(f_lam, dtype=np.float64)
+        vx, vy = Vec(data=v), Vec(self.n)
+        _chk(load().lgh_glr_filter(self.h, f.ctypes.data_as(c_dbl_p), f_c,
+                                   vx.h, vy.h), "lgh_glr_filter")
+        return vy.get()
+
+    def logdet(self, c):
+        return load().lgh_glr_logdet(self.h, c)
+
+    def logdet_batch(self, cs):
+        cs = np.ascontiguousarray(cs, dtype=np.float64)
+        out = np.empty_like(cs)
+        _chk(load().lgh_glr_logdet_batch(self.h, len(cs),
+                                         cs.ctypes.data_as(c_dbl_p),
+                                         out.ctypes.data_as(c_dbl_p)),
+             "lgh_glr_logdet_batch")
+        return out
+
+    def _batch(self, fname, cs, R):
+        cs = np.ascontiguousarray(cs, dtype=np.float64)
+        R = np.asarray(R, dtype=np.float64)
+        m = R.shape[1]
+        bi = DeviceBlock(self.n, m, R)
+        bo = DeviceBlock(self.n, m * len(cs))
+        _chk(getattr(load(), fname)(self.h, len(cs),
+                                    cs.ctypes.data_as(c_dbl_p), m, bi.ptr(),
+                                    self.n, bo.ptr(), self.n), fname)
+        out = bo.get()
+        return [out[:, s * m:(s + 1) * m] for s in range(len(cs))]
+
+    def solve_batch(self, cs, R):
+        return self._batch("lgh_glr_solve_batch", cs, R)
+
+    def sample_batch(self, cs, R):
+        return self._batch("lgh_glr_sample_batch", cs, R)
+
+    def __del__(self):
+        if _L is not None and getattr(self, "h", None):
+            _L.lgh_glr_destroy(self.h)
+            self.h = P()
+
+
+# ---- kernel-level test hooks --------------------------------------------
+
+
+def test_sketch(seed, n, j0, k):
+    out = np.empty((n, k))
+    _chk(load().lgh_test_sketch(seed, n, j0, k, out.ctypes.data),
+         "lgh_test_sketch")
+    return out
+
+
+def test_rng_state(seed, n, j0, k):
+    out = np.empty((n, k), dtype=np.uint64)
+    _chk(load().lgh_test_rng_state(seed, n, j0, k, out.ctypes.data),
+         "lgh_test_rng_state")
+    return out
+
+
+def test_spmm(A, X, fp32=False):
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    Y = np.empty_like(X)
+    _chk(load().lgh_test_spmm(A.h, X.shape[1], X.ctypes.data, Y.ctypes.data,
+                              1 if fp32 else 0), "lgh_test_spmm")
+    return Y
+
+
+def test_zsolve(prior, X, fp32=False):
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    Y = np.empty_like(X)
+    _chk(load().lgh_test_zsolve(prior.h, X.shape[1], X.ctypes.data,
+                                Y.ctypes.data, 1 if fp32 else 0),
+         "lgh_test_zsolve")
+    return Y
+
+
+def test_gram(X):
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    w = X.shape[1]
+    G = np.empty((w, w), order="F")
+    _chk(load().lgh_test_gram(X.shape[0], w, X.ctypes.data, G.ctypes.data),
+         "lgh_test_gram")
+    return G
+
+
+def test_gemm_nn(X, M):
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    Mf = np.asfortranarray(M, dtype=np.float64)
+    Y = np.empty((X.shape[0], Mf.shape[1]))
+    _chk(load().lgh_test_gemm_nn(X.shape[0], X.shape[1], Mf.shape[1],
+                                 X.ctypes.data, Mf.ctypes.data, Y.ctypes.data),
+         "lgh_test_gemm_nn")
+    return Y
+
+
+def test_potrf(G, jitter_mode=0):
+    Gf = np.asfortranarray(G, dtype=np.float64)
+    n = Gf.shape[0]
+    L = np.empty((n, n), order="F")
+    Li = np.empty((n, n), order="F")
+    info = np.zeros(2, dtype=np.int32)
+    _chk(load().lgh_test_potrf(n, Gf.ctypes.data, jitter_mode, L.ctypes.data,
+                               Li.ctypes.data, info.ctypes.data),
+         "lgh_test_potrf")
+    return L, (Li if info[0] == 0 else None), info
+
+
+def test_syev(A):
+    Af = np.asfortranarray(A, dtype=np.float64)
+    n = Af.shape[0]
+    w = np.empty(n)
+    V = np.empty((n, n), order="F")
+    sw = ctypes.c_int(0)
+    _chk(load().lgh_test_syev(n, Af.ctypes.data, w.ctypes.data, V.ctypes.data,
+                              ctypes.byref(sw)), "lgh_test_syev")
+    return w, V, sw.value
