@@ -1,0 +1,487 @@
+#!/usr/bin/env python
+"""GLR benchmark: one "job" = one GLR build + a 16-RHS solve + a logdet.
+
+Workload (config 2, the plain FP64 GPU configuration): 512^2 uniform grid on
+[0,1]^2 (N = 262144), lumped mass, Z = L + 25 M (5-point Neumann
+Laplacian), B = Gaussian (l = 0.005) x Wendland-C2 (rho = 0.015) kernel
+matrix (~183 nnz/row), GLR rank 200 + oversample 20 (ell = 220, kept capped
+at 200), q = 1, seed 0, Z-solve tolerance 1e-10; 16 N(0,1) right-hand sides
+solved at c = 1 and logdet at c = 1.  Synthetic data generated from the
+configuration's formulas (lgh_b200/problems.py).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Ours: each rank builds its own replica (the build does not shard on one
+node here: replicas, weak scaling); inputs resident in HBM; W untimed jobs,
+then K jobs between a barrier + synchronize, CUDA events on the library's
+stream (the legacy default stream), max over ranks.  Also reported: the
+same jobs end to end through the C ABI from pinned host buffers (e2e), the
+per-kernel roofline of the dominant kernel from the library's live event
+timing, per-RHS solve latency p50/p99, SM clocks sampled during the timed
+region, and the CPU baseline (the oracle on the host cores, a bounded
+sample extrapolated to a job).
+
+--impl reference: the reference's CPU path restated by the oracle
+(oracle/), all host threads, a bounded sample per step, same metric.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "lgpsf-hessian_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+CONFIG = "c2"
+NRHS = 16
+SHIFT = 1.0
+ZRTOL = 1e-10
+ELL, RANK, QPOW, SEED = 220, 200, 1, 0
+METRIC = "GLR jobs/s (build + 16-RHS solve + logdet)"
+UNIT = "jobs/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-cols", type=int, default=0,
+                    help="sketch columns in the CPU sample (0 = host cores)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload(cfg):
+    return {"workload": "c2: 512^2 2D grid (N=%d), B Gaussian x Wendland "
+                        "(%.1f nnz/row), Z = L + 25 M (5-point), ell=%d "
+                        "(rank %d + oversample %d), q=%d, Z-solve rtol %g, "
+                        "%d N(0,1) RHS at c=%g, logdet at c=%g"
+                        % (cfg["N"], cfg["nnz_B"] / cfg["N"], ELL, RANK,
+                           ELL - RANK, QPOW, ZRTOL, NRHS, SHIFT, SHIFT),
+            "N": cfg["N"], "nnz_B": cfg["nnz_B"], "nnz_Z": cfg["nnz_Z"],
+            "ell": ELL, "rank_cap": RANK, "q_power": QPOW, "seed": SEED,
+            "zsolve": "blocked PCG, smoothed-aggregation V-cycle "
+                      "preconditioner, rtol %g" % ZRTOL,
+            "nrhs": NRHS, "shift": SHIFT,
+            "l2": "inputs larger than L2 (ell-wide blocks 461 MB each)"}
+
+
+# --------------------------------------------------------------------------
+# CPU side: the oracle timed on the host cores (bounded sample)
+
+
+def cpu_sample(cfg, cols=0):
+    """Time the oracle (the reference's replicated CPU path restated) on a
+    bounded sample of the job and extrapolate: one F-apply over `cols`
+    sketch columns (columns run in parallel over the host threads), the
+    dense part (two CholQR2 at the full N x ell, the ell x ell eigensolve)
+    and one single-RHS solve (2 Z-solves); job = F-applies over
+    (q+2)*ell + rank columns + 2 CholQR2 + 16 solves (over the threads)."""
+    import oracle
+    nthreads = os.cpu_count() or 1
+    oracle.set_threads(nthreads)
+    cols = cols or nthreads
+    B = oracle.Csr(cfg["B"]["rowptr"], cfg["B"]["colidx"], cfg["B"]["vals"])
+    Z = oracle.Csr(cfg["Z"]["rowptr"], cfg["Z"]["colidx"], cfg["Z"]["vals"])
+    pr = oracle.Prior(Z, cfg["mass"], ksp_rtol=ZRTOL, pc="amg")
+    ctx = oracle.lib().orc_glr_context(B.h, pr.h)
+    N = cfg["N"]
+    X = oracle.sketch(SEED, N, 0, cols)
+    Xc = np.ascontiguousarray(X.T)
+    Yc = np.empty_like(Xc)
+    t0 = time.perf_counter()
+    oracle.lib().orc_glr_apply_F(ctx, cols, Xc.ctypes.data_as(oracle.c_dbl_p),
+                                 Yc.ctypes.data_as(oracle.c_dbl_p))
+    t_f = time.perf_counter() - t0
+    Q = np.asfortranarray(np.random.default_rng(0).standard_normal((N, ELL)))
+    t0 = time.perf_counter()
+    oracle.lib().orc_cholqr2(N, ELL, Q.ctypes.data_as(oracle.c_dbl_p))
+    t_orth = time.perf_counter() - t0
+    T = np.random.default_rng(1).standard_normal((ELL, ELL))
+    t0 = time.perf_counter()
+    oracle.dsyevd(T + T.T, vecs=True)
+    t_eig = time.perf_counter() - t0
+    oracle.lib().orc_glr_destroy(ctx)
+    # one solve = 2 single-column Z-solves ~ the F-apply's per-column
+    # Z-solve cost; columns of the F-apply ran in parallel
+    waves_f = ((QPOW + 2) * ELL + RANK + cols - 1) // cols
+    t_solve_col = t_f / 2.0             # one wave = 2 Z-solves + 1 SpMV
+    waves_s = (NRHS + nthreads - 1) // nthreads
+    job = waves_f * t_f + 2 * (QPOW + 1) * t_orth + t_eig \
+        + waves_s * 2 * t_solve_col
+    sample = ("oracle F-apply of %d sketch columns (%d threads, CG rtol "
+              "%g with a smoothed-aggregation V-cycle PC, the reference's "
+              "CG + PCGAMG: %.1f s), CholQR2 at %dx%d (%.2f s), dsyevd %d "
+              "(%.3f s); job extrapolated as %d F waves + %d CholQR2 + eig + "
+              "%d solve waves = %.1f s"
+              % (cols, nthreads, ZRTOL, t_f, N, ELL, t_orth, ELL, t_eig,
+                 waves_f, 2 * (QPOW + 1), waves_s, job))
+    return dict(value=1.0 / job, unit=UNIT, cores=nthreads, kind="port",
+                sample=sample, job_s=job)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from lgh_b200 import problems as P
+    cfg = P.grid_problem(CONFIG)
+    vals = []
+    info = None
+    for i in range(args.warmup + args.steps):
+        info = cpu_sample(cfg, args.cpu_cols)
+        if i >= args.warmup:
+            vals.append(info["value"])
+    v = statistics.mean(vals)
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (config formulas)", "config": workload(cfg),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": info["cores"],
+                             "kind": "port", "sample": info["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------
+# GPU side
+
+
+class Clocks:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,"
+         "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.th = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [],
+                    "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.th:
+            self.th.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900))
+
+    import lgh_b200 as L
+    from lgh_b200 import problems as P
+
+    L.load()
+    cfg = P.grid_problem(CONFIG)
+    N = cfg["N"]
+    B, Z = L.Mat(cfg["B"]), L.Mat(cfg["Z"])
+    pr = L.Prior(Z=Z, mass=cfg["mass"], opts=L.prior_opts(ksp_rtol=ZRTOL))
+    opts = L.glr_opts(ell=ELL, q_power=QPOW, seed=SEED, trunc_rel=0.0,
+                      check=1)
+    ex = L.exec_opts(rank_cap=RANK)
+    rhs_h = np.random.default_rng(100 + rank).standard_normal((N, NRHS))
+    rhs = L.DeviceBlock(N, NRHS, rhs_h)
+    xout = L.DeviceBlock(N, NRHS)
+    cs = np.array([SHIFT])
+    Lb = L.load()
+
+    def job(timers=None):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record()
+        g = L.Glr(B, pr, opts, exec=ex)
+        ev[1].record()
+        L._chk(Lb.lgh_glr_solve_batch(g.h, 1, cs.ctypes.data_as(L.c_dbl_p),
+                                      NRHS, rhs.ptr(), N, xout.ptr(), N),
+               "lgh_glr_solve_batch")
+        ev[2].record()
+        ld = g.logdet(SHIFT)
+        ev[3].record()
+        if timers is not None:
+            timers.append((ev, g))
+        return g, ld
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        job()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    L.kernel_timing(True)
+    launches0 = Lb.lgh_launch_count()
+    t_start, t_end = torch.cuda.Event(enable_timing=True), \
+        torch.cuda.Event(enable_timing=True)
+    timers = []
+    t_start.record()
+    for _ in range(args.steps):
+        job(timers)
+    t_end.record()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ktimes = L.kernel_timing_get()
+    L.kernel_timing(False)
+    launches = Lb.lgh_launch_count() - launches0
+    clk = clocks.stop()
+    elapsed = t_start.elapsed_time(t_end) / 1e3
+    if world > 1:
+        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    build_s = [ev[0].elapsed_time(ev[1]) / 1e3 for ev, _ in timers]
+    solve_s = [ev[1].elapsed_time(ev[2]) / 1e3 for ev, _ in timers]
+    g_last = timers[-1][1]
+    stats = g_last.stats()
+    report = g_last.report
+
+    # per-RHS latency of the reference-form single solve (lgh_glr_solve)
+    lat = []
+    for j in range(NRHS):
+        v = L.Vec(data=rhs_h[:, j])
+        x = L.Vec(N)
+        e0, e1 = torch.cuda.Event(enable_timing=True), \
+            torch.cuda.Event(enable_timing=True)
+        e0.record()
+        L._chk(Lb.lgh_glr_solve(g_last.h, SHIFT, v.h, x.h), "lgh_glr_solve")
+        e1.record()
+        torch.cuda.synchronize()
+        lat.append(e0.elapsed_time(e1))
+    lat.sort()
+
+    # solve residual against the GLR model operator H~(c) (one RHS, FP64 on
+    # the host): H~ = Z M^{-1/2} (U Lam U^T + c I) M^{-1/2} Z
+    x0 = xout.get()[:, 0]
+    U = g_last.U()
+    lam = g_last.eigs()
+    ms = np.sqrt(cfg["mass"])
+    t1 = P.csr_matvec(cfg["Z"], x0) / ms
+    t2 = SHIFT * t1 + U @ (lam * (U.T @ t1))
+    hx = P.csr_matvec(cfg["Z"], t2 / ms)
+    resid = float(np.linalg.norm(hx - rhs_h[:, 0]) / np.linalg.norm(rhs_h[:, 0]))
+    del U
+
+    # roofline of the dominant kernel (largest share of timed device time)
+    dom = max(ktimes.items(), key=lambda kv: kv[1][0])
+    name, (kms, kn, kbytes) = dom
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs")
+    peak_note = "measured (MEASURED_PEAKS.json hbm_gbs)"
+    if peak is None:
+        peak, peak_note = 6650.0, "fallback 6.65 TB/s"
+    achieved = (kbytes / kn) / (kms / kn / 1e3) / 1e9 if kn else None
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            traffic = json.load(f).get(name)
+    except (OSError, ValueError):
+        pass
+    tot_ms = sum(v[0] for v in ktimes.values()) or 1.0
+    kernels = {k: {"ms": round(v[0], 3), "launches": v[1],
+                   "share": round(v[0] / tot_ms, 4),
+                   "GBps": round((v[2] / v[1]) / (v[0] / v[1] / 1e3) / 1e9, 1)
+                   if v[1] and v[0] > 0 else None}
+               for k, v in ktimes.items() if v[1]}
+
+    line = {"metric": METRIC, "value": world * args.steps / elapsed,
+            "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (config formulas)",
+            "config": dict(workload(cfg), parallelism="replicas%d" % world),
+            "build_s": statistics.mean(build_s),
+            "solves_per_s": NRHS / statistics.mean(solve_s),
+            "solve_p50_ms": lat[len(lat) // 2],
+            "solve_p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+            "solve_residual_model": resid,
+            "kept": report["kept"], "lam_abs_max": report["lam_abs_max"],
+            "next_abs": report["next_abs"], "resid_max": report["resid_max"],
+            "zsolve_mean_col_iters": stats["zsolve_mean_col_iters"],
+            "t_zsolve_s": stats["t_zsolve"], "t_spmm_s": stats["t_spmm"],
+            "roofline": {"kernel": name, "bound": "hbm",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if achieved else None,
+                         "traffic": traffic, "peak_source": peak_note,
+                         "bytes_per_launch": kbytes / kn if kn else None,
+                         "launch_ms": kms / kn if kn else None},
+            "kernels": kernels, "gpu_launches": launches, "clocks": clk}
+
+    if not args.no_e2e:
+        line["e2e"] = run_e2e(args, cfg, L, torch, world, dist)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = {k: v for k, v in cpu_sample(
+            cfg, args.cpu_cols).items() if k != "job_s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_e2e(args, cfg, L, torch, world, dist):
+    """The same jobs through the C ABI from pinned host buffers: every step
+    uploads B, Z, mass (lgh_mat_create_csr from host arrays) and the 16
+    right-hand sides, builds, solves, reads the solutions and the logdet
+    back.  Timed with CUDA events + synchronize, max over ranks."""
+    import ctypes
+    N = cfg["N"]
+    Lb = L.load()
+    pin = {}
+    for nm in ("B", "Z"):
+        for k in ("rowptr", "colidx", "vals"):
+            a = torch.from_numpy(np.ascontiguousarray(cfg[nm][k])).pin_memory()
+            pin[nm + k] = a
+    mass = torch.from_numpy(cfg["mass"].copy()).pin_memory()
+    rhs = torch.from_numpy(np.random.default_rng(7).standard_normal(
+        (NRHS, N))).pin_memory()
+    xh = torch.empty((NRHS, N), dtype=torch.float64).pin_memory()
+    h2d = sum(t.numel() * t.element_size() for t in pin.values()) \
+        + mass.numel() * 8 + rhs.numel() * 8
+    d2h = xh.numel() * 8 + 8
+    opts = L.glr_opts(ell=ELL, q_power=QPOW, seed=SEED, trunc_rel=0.0,
+                      check=1)
+    ex = L.exec_opts(rank_cap=RANK)
+    cs = np.array([SHIFT])
+
+    def step():
+        hB, hZ = ctypes.c_void_p(), ctypes.c_void_p()
+        L._chk(Lb.lgh_mat_create_csr(N, pin["Browptr"].data_ptr(),
+                                     pin["Bcolidx"].data_ptr(),
+                                     pin["Bvals"].data_ptr(), 0,
+                                     ctypes.byref(hB)), "create B")
+        L._chk(Lb.lgh_mat_create_csr(N, pin["Zrowptr"].data_ptr(),
+                                     pin["Zcolidx"].data_ptr(),
+                                     pin["Zvals"].data_ptr(), 0,
+                                     ctypes.byref(hZ)), "create Z")
+        md = mass.to("cuda", non_blocking=True)
+        vm = ctypes.c_void_p()
+        L._chk(Lb.lgh_vec_create_with_array(N, md.data_ptr(),
+                                            ctypes.byref(vm)), "mass")
+        hp = ctypes.c_void_p()
+        po = L.prior_opts(ksp_rtol=ZRTOL)
+        L._chk(Lb.lgh_prior_create_mat(hZ, vm, ctypes.byref(po),
+                                       ctypes.byref(hp)), "prior")
+        hg = ctypes.c_void_p()
+        rep = L.GlrReport()
+        L._chk(Lb.lgh_glr_compute_ex(hB, hp, ctypes.byref(opts),
+                                     ctypes.byref(ex), ctypes.byref(hg),
+                                     ctypes.byref(rep)), "compute")
+        rd = rhs.to("cuda", non_blocking=True)
+        xd = torch.empty((NRHS, N), dtype=torch.float64, device="cuda")
+        L._chk(Lb.lgh_glr_solve_batch(hg, 1, cs.ctypes.data_as(L.c_dbl_p),
+                                      NRHS, rd.data_ptr(), N, xd.data_ptr(),
+                                      N), "solve_batch")
+        xh.copy_(xd, non_blocking=True)
+        ld = Lb.lgh_glr_logdet(hg, SHIFT)
+        Lb.lgh_glr_destroy(hg)
+        Lb.lgh_prior_destroy(hp)
+        Lb.lgh_vec_destroy(ctypes.byref(vm))
+        Lb.lgh_mat_destroy(ctypes.byref(hB))
+        Lb.lgh_mat_destroy(ctypes.byref(hZ))
+        return ld
+
+    step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), \
+        torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    el = e0.elapsed_time(e1) / 1e3
+    if world > 1:
+        t = torch.tensor([el], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        el = float(t.item())
+    return {"value": world * args.steps / el, "unit": UNIT,
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+
+def main():
+    args = parse()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -132,10 +132,12 @@ int lgh_prior_create_callbacks (lgh_Vec mass_lumps,
 /* prior.h:76-89.  On this device the Mat path solves Z with blocked,
  * per-column preconditioned CG (blocked_mode 0/1, rtol ksp_rtol, the
  * reference's per-column KSP semantics) or blocked fixed-count Chebyshev
- * (mode 2, cheb_rtol, bounds from a CG-Lanczos probe widened 0.9/1.1), both
- * Jacobi-preconditioned; mode 3 runs Chebyshev around a block V-cycle on an
- * aggregation hierarchy built from Z.  tile caps the block width of one
- * blocked solve pass.                                                     */
+ * (modes 2/3, cheb_rtol, bounds from a CG-Lanczos probe widened 0.9/1.1),
+ * preconditioned by a block V-cycle on a smoothed-aggregation hierarchy of
+ * Z (Chebyshev-Jacobi smoothers, nu = nu_force or 2, interval
+ * [0.1, smoother_top] lambda_max; dense coarse solve) or by Jacobi
+ * (lgh_prior_create_mat_pc).  tile caps the block width of one blocked
+ * Chebyshev pass.                                                         */
 typedef struct lgh_prior_mat_opts
 {
   double ksp_rtol;     /* per-column solve tolerance (default 1e-12)     */
@@ -154,6 +156,17 @@ lgh_prior_mat_opts_t lgh_prior_mat_opts_default (void);
 int lgh_prior_create_mat (lgh_Mat Z, lgh_Vec mass_lumps,
                           const lgh_prior_mat_opts_t *opts,
                           lgh_prior_t **prior);
+/* The Mat path with an explicit preconditioner choice (lgh_prior_create_mat
+ * takes it from the environment variable LGH_PRIOR_PC_TYPE, "amg" by
+ * default, the counterpart of the reference's -lgh_prior_pc_type option):
+ * LGH_PC_AMG is smoothed-aggregation multigrid (the role of PCGAMG; the
+ * V-cycle of blocked_mode 3), LGH_PC_JACOBI the diagonal.                 */
+#define LGH_PC_AMG    0
+#define LGH_PC_JACOBI 1
+int lgh_prior_create_mat_pc (lgh_Mat Z, lgh_Vec mass_lumps,
+                             const lgh_prior_mat_opts_t *opts, int pc_type,
+                             lgh_prior_t **prior);
+
 /* Always LGH_ERR_SUP: there is no PETSc KSP on this device.              */
 int lgh_prior_create_ksp (lgh_KSP ksp, lgh_Vec mass_lumps,
                           const lgh_prior_mat_opts_t *opts,
@@ -168,9 +181,10 @@ int lgh_prior_solve (lgh_prior_t *prior, lgh_Vec x, lgh_Vec y);
 int lgh_prior_solve_block (lgh_prior_t *prior, int m, const double *X,
                            int64_t ldx, double *Y, int64_t ldy);
 
-/* Diagnostics of a Mat-path prior's Z-solver: out[0..7] = Lanczos emin,
+/* Diagnostics of a Mat-path prior's Z-solver: out[0..11] = Lanczos emin,
  * emax, margined lmin, lmax, Chebyshev nit, probe iterations, mean
- * per-column CG iterations so far, number of solve calls.               */
+ * per-column CG iterations so far, number of solve calls, multigrid
+ * levels, coarse size, multigrid setup seconds, preconditioner type.    */
 int lgh_prior_get_info (const lgh_prior_t *prior, double *out);
 
 /* ---- glr.h --------------------------------------------------------------- */
@@ -269,6 +283,8 @@ typedef struct lgh_exec_opts
   double inner_rtol;   /* mixed: FP32 inner Z-solve tolerance (1e-5)     */
   int    max_refine;   /* mixed: FP64 refinement steps per solve (4)     */
   int    verbose;
+  int    rank_cap;     /* keep at most rank_cap modes ("rank r,
+                          oversample p" = ell r + p, rank_cap r); 0 = off */
 }
 lgh_exec_opts_t;
 
@@ -307,6 +323,18 @@ int lgh_glr_sample_batch (lgh_glr_t *glr, int nshift, const double *c,
                           int64_t ldx);
 int lgh_glr_logdet_batch (lgh_glr_t *glr, int nshift, const double *c,
                           double *out);
+
+/* Per-kernel CUDA-event timing of the hot kernels: switch on (1) / off (0)
+ * (either resets the figures); read accumulated device milliseconds,
+ * launches and algorithmic bytes of kernel id 0 k_pcg_pq, 1 k_pcg_upd,
+ * 2 k_cheb (every 8th launch), 3 k_spmm (the B product), 4 k_pcg_init.
+ * Returns the kernel's name, NULL past the last id.                     */
+int lgh_kernel_timing (int on);
+const char *lgh_kernel_timing_get (int id, double *ms, long *launches,
+                                   double *bytes);
+
+/* Number of this library's kernel launches since the process started.   */
+long lgh_launch_count (void);
 
 /* Last error message of the calling thread (empty if none).              */
 const char *lgh_last_error (void);

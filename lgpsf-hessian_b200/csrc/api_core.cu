@@ -18,6 +18,7 @@
 
 #include "lgh_device.cuh"
 #include "lgh_internal.h"
+#include "lgh_mg.h"
 #include "lgh_objects.h"
 
 namespace lgh
@@ -26,6 +27,7 @@ namespace lgh
 /* ---- errors ---------------------------------------------------------- */
 
 static thread_local std::string g_err;
+long g_launches = 0;
 
 int
 set_error (int code, const char *fmt, ...)
@@ -127,17 +129,18 @@ k_csr_diag (int64_t n, const int64_t *rowptr, const int32_t *col,
 }
 
 __global__ void
-k_check_csr (int64_t n, const int64_t *rowptr, const int32_t *col, int *bad)
+k_check_csr (int64_t n, int64_t ncols, const int64_t *rowptr, const int32_t *col,
+             int *bad)
 {
   for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t) gridDim.x * blockDim.x) {
     if (rowptr[i + 1] < rowptr[i]) { atomicExch (bad, 1); continue; }
     for (int64_t k = rowptr[i]; k < rowptr[i + 1]; k++)
-      if (col[k] < 0 || col[k] >= n) atomicExch (bad, 2);
+      if (col[k] < 0 || col[k] >= ncols) atomicExch (bad, 2);
   }
 }
 
-static int
+int
 csr_finish (Csr &A)
 {
   cudaStream_t s = stream ();
@@ -148,7 +151,8 @@ csr_finish (Csr &A)
   LGH_TRY (flags.alloc (2));
   LGH_CUDA (cudaMemsetAsync (flags.p, 0, 2 * sizeof (int), s));
   const int grid = (int) std::min<int64_t> ((A.n + 255) / 256 + 1, num_sms () * 16);
-  k_check_csr<<<grid, 256, 0, s>>> (A.n, A.rowptr, A.colidx, flags.p);
+  k_check_csr<<<grid, 256, 0, s>>> (A.n, A.ncols > 0 ? A.ncols : A.n,
+                                    A.rowptr, A.colidx, flags.p);
   LGH_LAUNCH_CHECK ();
   int h[2];
   LGH_CUDA (cudaMemcpyAsync (h, flags.p, 2 * sizeof (int), cudaMemcpyDeviceToHost, s));
@@ -189,6 +193,12 @@ const char *
 lgh_last_error (void)
 {
   return g_err.c_str ();
+}
+
+long
+lgh_launch_count (void)
+{
+  return __atomic_load_n (&lgh::g_launches, __ATOMIC_RELAXED);
 }
 
 int
@@ -426,7 +436,7 @@ prior_solve_vec (lgh_prior_t *p, const double *x, const double *s_in,
     prior_zcfg (p, cfg);
     cfg.mode = 0;
     LGH_TRY (p->wsv.alloc (p->n, 4, 0));
-    return zsolve_block<double> (p->Z->csr, cfg, nullptr, p->wsv, p->n, 1, x, 1,
+    return zsolve_block<double> (p->Z->csr, cfg, p->mg, p->wsv, p->n, 1, x, 1,
                                  s_in, y, 1, s_out, &p->stats, 0, s);
   }
   /* callbacks: scale into scratch, call, scale */
@@ -459,7 +469,7 @@ prior_solve_rows (lgh_prior_t *p, int w, const T *X, int ldx,
     int cap = std::min (w, std::is_same<T, double>::value ? 512 : 1024);
     ZWork &ws = std::is_same<T, double>::value ? p->ws64 : p->ws32;
     LGH_TRY (ws.alloc (p->n, cap, std::is_same<T, float>::value));
-    return zsolve_block<T> (p->Z->csr, cfg, nullptr, ws, p->n, w, X, ldx, s_in,
+    return zsolve_block<T> (p->Z->csr, cfg, p->mg, ws, p->n, w, X, ldx, s_in,
                             Y, ldy, s_out, &p->stats, 0, s);
   }
   if constexpr (std::is_same<T, float>::value) {
@@ -580,19 +590,46 @@ int
 lgh_prior_create_mat (lgh_Mat Z, lgh_Vec mass, const lgh_prior_mat_opts_t *opts,
                       lgh_prior_t **prior)
 {
+  /* the preconditioner of the Mat path: aggregation multigrid (the
+   * reference's PCGAMG) unless LGH_PRIOR_PC_TYPE=jacobi, the counterpart
+   * of its "-lgh_prior_pc_type" option (zsolve_impl.h:816-817) */
+  int pc = LGH_PC_AMG;
+  const char *env = getenv ("LGH_PRIOR_PC_TYPE");
+  if (env && (strcmp (env, "jacobi") == 0 || strcmp (env, "JACOBI") == 0))
+    pc = LGH_PC_JACOBI;
+  return lgh_prior_create_mat_pc (Z, mass, opts, pc, prior);
+}
+
+int
+lgh_prior_create_mat_pc (lgh_Mat Z, lgh_Vec mass,
+                         const lgh_prior_mat_opts_t *opts, int pc_type,
+                         lgh_prior_t **prior)
+{
   LGH_CHECK (Z && Z->kind == 0, LGH_ERR_ARG_WRONG, "lgh_prior_create_mat: Z must be a CSR Mat");
   LGH_CHECK (mass && mass->n == Z->csr.n, LGH_ERR_ARG_SIZ, "lgh_prior_create_mat: mass size");
   lgh_prior_mat_opts_t o = opts ? *opts : lgh_prior_mat_opts_default ();
   LGH_CHECK (o.blocked_mode >= 0 && o.blocked_mode <= 3, LGH_ERR_ARG_OUTOFRANGE,
              "lgh_prior_create_mat: blocked_mode %d", o.blocked_mode);
-  LGH_CHECK (o.blocked_mode != 3, LGH_ERR_SUP,
-             "lgh_prior_create_mat: blocked_mode 3 is not available in this build");
+  LGH_CHECK (pc_type == LGH_PC_AMG || pc_type == LGH_PC_JACOBI,
+             LGH_ERR_ARG_OUTOFRANGE, "lgh_prior_create_mat: pc type %d", pc_type);
+  LGH_CHECK (o.blocked_mode != 3 || pc_type == LGH_PC_AMG, LGH_ERR_ARG_WRONG,
+             "lgh_prior_create_mat: blocked_mode 3 needs the multigrid "
+             "preconditioner");
   lgh_prior_t *p;
   LGH_TRY (prior_init_common (mass, &p));
   p->is_mat = 1;
   p->Z = Z;
   Z->refs++;
   p->mopts = o;
+  p->pc_type = pc_type;
+  if (pc_type == LGH_PC_AMG) {
+    const int nu = o.nu_force > 0 ? o.nu_force : 2;
+    int rc = mg_build (Z->csr, o.tile, o.smoother_top, nu, &p->mg);
+    if (rc) { lgh_prior_destroy (p); return rc; }
+    if (o.verbose)
+      printf ("lgh_prior: multigrid %d levels (coarse %d) setup %.3f s\n",
+              (int) p->mg->lev.size (), p->mg->n0, p->mg->setup_s);
+  }
   p->zcfg.mode = o.blocked_mode;
   p->zcfg.rtol = o.ksp_rtol;
   p->zcfg.maxit = 10000;
@@ -615,7 +652,7 @@ lgh_prior_create_mat (lgh_Mat Z, lgh_Vec mass, const lgh_prior_mat_opts_t *opts,
     bc.check_every = 1000000;
     if (!rc) rc = p->wsv.alloc (n, 4, 0);
     ZsolveStats st;
-    if (!rc) rc = zsolve_block<double> (Z->csr, bc, nullptr, p->wsv, n, 1, rhs.p,
+    if (!rc) rc = zsolve_block<double> (Z->csr, bc, p->mg, p->wsv, n, 1, rhs.p,
                                         1, nullptr, y.p, 1, nullptr, &st, 1, s);
     int its = (int) st.col_iters;
     if (!rc && its < 1) rc = set_error (LGH_ERR_NOT_CONVERGED, "prior: bound probe ran 0 iterations");
@@ -664,6 +701,7 @@ void
 lgh_prior_destroy (lgh_prior_t *prior)
 {
   if (prior == NULL || --prior->refs > 0) return;
+  if (prior->mg) mg_destroy (prior->mg);
   if (prior->Z) mat_release (prior->Z);
   delete prior;
 }
@@ -725,6 +763,10 @@ lgh_prior_get_info (const lgh_prior_t *p, double *out)
   out[5] = p->bound_its;
   out[6] = p->stats.cols ? (double) p->stats.col_iters / p->stats.cols : 0.;
   out[7] = (double) p->stats.calls;
+  out[8] = p->mg ? (double) p->mg->lev.size () : 0.;
+  out[9] = p->mg ? (double) p->mg->n0 : 0.;
+  out[10] = p->mg ? p->mg->setup_s : 0.;
+  out[11] = p->pc_type;
   return 0;
 }
 

@@ -14,6 +14,7 @@
 
 #include "lgh_device.cuh"
 #include "lgh_internal.h"
+#include "lgh_ktime.h"
 #include "lgh_objects.h"
 
 namespace lgh
@@ -191,8 +192,17 @@ apply_F (lgh_glr_t *g, int w, const T *X, int ldx, T *Y, int ldy, T *W,
   double t0 = wall ();
   LGH_TRY (prior_solve_rows<T> (g->prior, w, X, ldx, ms, W, ldw, nullptr));
   double t1 = wall ();
+  static thread_local EventRing ring;
+  const bool timing = ktime_on ();
+  if (timing) LGH_TRY (ring.record (s));
   LGH_TRY (launch_spmm<T> (g->B->csr, W, ldw, Y, ldy, w, s));
+  if (timing) LGH_TRY (ring.record (s));
   LGH_CUDA (cudaStreamSynchronize (s));
+  if (timing) {
+    const double bytes = (double) g->B->csr.nnz * (sizeof (T) + 4)
+                         + 8. * (g->n + 1) + 2. * g->n * w * sizeof (T);
+    LGH_TRY (ring.drain ({ K_SPMM }, { bytes }));
+  }
   double t2 = wall ();
   LGH_TRY (prior_solve_rows<T> (g->prior, w, Y, ldy, nullptr, Y, ldy, ms));
   LGH_CUDA (cudaStreamSynchronize (s));
@@ -287,7 +297,16 @@ rayleigh_ritz (lgh_glr_t *g, int ell, const T *Q, int ldq, const double *Araw,
   LGH_CUDA (cudaMemcpyAsync (sel, sm.sel.p, 6 * sizeof (double),
                              cudaMemcpyDeviceToHost, s));
   LGH_CUDA (cudaStreamSynchronize (s));
-  const int kept = (int) sel[0];
+  int kept = (int) sel[0];
+  if (g->exec.rank_cap > 0 && kept > g->exec.rank_cap) {
+    /* rank r with oversampling: keep the r largest |lambda|; the first
+     * mode cut by the cap becomes next_abs */
+    kept = g->exec.rank_cap;
+    double nxt = 0.;
+    LGH_CUDA (cudaMemcpy (&nxt, sm.lam.p + kept, sizeof (double),
+                          cudaMemcpyDeviceToHost));
+    sel[2] = fabs (nxt);
+  }
   rep->kept = kept;
   rep->lam_abs_max = sel[1];
   rep->next_abs = sel[2];
@@ -676,6 +695,7 @@ lgh_exec_opts_default (void)
   e.inner_rtol = 1e-5;
   e.max_refine = 4;
   e.verbose = 0;
+  e.rank_cap = 0;
   return e;
 }
 

@@ -141,6 +141,34 @@ launch_gemm_tn (int64_t n, int m1, int m2, const T *A, int lda, const T *B,
   return 0;
 }
 
+/* the same product with an explicit split count and caller-provided
+ * partial-sum storage of nsplit * m1 * m2 doubles */
+int
+launch_gemm_tn_fixed (int64_t n, int m1, int m2, const double *A, int lda,
+                      const double *B, int ldb, double *C, int ldc,
+                      double *work, int nsplit, cudaStream_t s)
+{
+  if (m1 == 0 || m2 == 0) return 0;
+  if (nsplit < 1) nsplit = 1;
+  int64_t kchunk = (n + nsplit - 1) / nsplit;
+  kchunk = (kchunk + GK - 1) / GK * GK;
+  dim3 grid ((m1 + GB - 1) / GB, (m2 + GB - 1) / GB, nsplit);
+  k_gemm_tn_part<double><<<grid, 256, 0, s>>> (n, m1, m2, A, lda, B, ldb,
+                                               work, kchunk);
+  LGH_LAUNCH_CHECK ();
+  const int64_t total = (int64_t) m1 * m2;
+  int rg = (int) std::min<int64_t> ((total + 255) / 256, num_sms () * 8);
+  k_gemm_tn_reduce<<<rg, 256, 0, s>>> (m1, m2, nsplit, work, C, ldc, 0);
+  LGH_LAUNCH_CHECK ();
+  return 0;
+}
+
+int
+gemm_tn_splits (int64_t n, int m1, int m2)
+{
+  return tn_splits (n, m1, m2);
+}
+
 template int launch_gemm_tn<double> (int64_t, int, int, const double *, int,
                                      const double *, int, double *, int, int,
                                      double *, size_t, cudaStream_t);

@@ -31,9 +31,10 @@ k_spmm (int64_t n, const int64_t *__restrict__ rowptr,
   const int ngroups = blockDim.x >> glog;
   const unsigned gmask = (G == 32) ? 0xffffffffu
                          : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
-  int64_t r0, r1;
-  block_rows (n, r0, r1);
-  for (int64_t i = r0 + group; i < r1; i += ngroups) {
+  /* row tiles of ngroups rows interleaved over the CTAs (L2 locality of
+   * the gathered neighbour rows) */
+  for (int64_t i = (int64_t) blockIdx.x * ngroups + group; i < n;
+       i += (int64_t) gridDim.x * ngroups) {
     T acc[CH][W];
 #pragma unroll
     for (int h = 0; h < CH; h++)

@@ -48,8 +48,11 @@ void clear_error ();
     if (rc_) return rc_;                                                     \
   } while (0)
 
+extern long g_launches;
+
 #define LGH_LAUNCH_CHECK()                                                   \
   do {                                                                       \
+    __atomic_fetch_add (&::lgh::g_launches, 1L, __ATOMIC_RELAXED);           \
     cudaError_t e_ = cudaGetLastError ();                                    \
     if (e_ != cudaSuccess)                                                   \
       return ::lgh::set_error (LGH_ERR_GPU, "%s:%d launch: %s", __FILE__,    \
@@ -75,6 +78,16 @@ struct DBuf
   DBuf () = default;
   DBuf (const DBuf &) = delete;
   DBuf &operator= (const DBuf &) = delete;
+  DBuf (DBuf &&o) noexcept : p (o.p), n (o.n) { o.p = nullptr; o.n = 0; }
+  DBuf &operator= (DBuf &&o) noexcept
+  {
+    if (this != &o) {
+      release ();
+      p = o.p; n = o.n;
+      o.p = nullptr; o.n = 0;
+    }
+    return *this;
+  }
   ~DBuf () { release (); }
   int alloc (size_t count)
   {
@@ -109,6 +122,7 @@ round_ld (int w)
 struct Csr
 {
   int64_t n = 0, nnz = 0;
+  int64_t ncols = 0;        /* 0: square (ncols = n) */
   int64_t *rowptr = nullptr;
   int32_t *colidx = nullptr;
   double *vals = nullptr;
@@ -230,7 +244,7 @@ struct ZWork
   int cap = 0;
   int64_t n = 0;
   int is32 = 0;
-  DBuf<char> X, R, P0, P1, Q;
+  DBuf<char> X, R, P0, P1, Q, Zb;
   DBuf<double> partA, partB;   /* [nblocks][ld] */
   DBuf<double> scal;           /* per-column scalars */
   DBuf<int> ival;              /* active flags / counts */

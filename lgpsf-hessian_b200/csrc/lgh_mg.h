@@ -1,0 +1,58 @@
+/* lgh_mg.h -- the aggregation-multigrid hierarchy (mg.cu). */
+
+#ifndef LGH_MG_H
+#define LGH_MG_H
+
+#include <vector>
+
+#include "lgh_internal.h"
+
+namespace lgh
+{
+
+struct MgLevel
+{
+  Csr A;            /* level operator (level 0 borrows Z's arrays)      */
+  Csr P, R;         /* prolongation n_l x n_{l+1}, restriction = P^T    */
+  int64_t n = 0;
+  double smax = 0., slo = 0., shi = 0.;
+  int nu = 2;
+  int own = 1;
+};
+
+struct MgWork
+{
+  int cap = 0;
+  DBuf<char> B, X, R0, R1, D0, D1;
+};
+
+struct Hierarchy
+{
+  std::vector<MgLevel> lev;   /* 0 = finest */
+  int n0 = 0;                 /* coarsest size (dense inverse)            */
+  DBuf<double> Ainv;          /* n0 x n0                                  */
+  std::vector<MgWork> w64, w32;
+  double setup_s = 0.;
+  ~Hierarchy ();
+};
+
+struct KTrace;
+
+/* X = V(B): one block V-cycle from the finest level (X overwritten);
+ * tr (nullable) records the fine level's kernels for the timing registry */
+template <typename T>
+int mg_vcycle (Hierarchy *h, const T *B, T *X, int ld, int w, cudaStream_t s,
+               KTrace *tr = nullptr);
+
+/* a Chebyshev step on a CSR operator with the Jacobi PC (zsolve.cu) */
+template <typename T>
+int launch_cheb_step (const Csr &A, T *X, const T *Ro, T *Rn, const T *Do,
+                      T *Dn, int ld, double a, double b, int first,
+                      cudaStream_t s);
+
+int csr_finish (Csr &A);
+void csr_free (Csr &A);
+
+} /* namespace lgh */
+
+#endif /* LGH_MG_H */

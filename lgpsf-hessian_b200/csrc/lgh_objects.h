@@ -43,6 +43,8 @@ struct lgh_prior
   lgh_prior_mat_opts_t mopts{};
   lgh::ZsolveCfg zcfg;
   lgh::ZWork ws64, ws32, wsv;
+  int pc_type = 0;              /* LGH_PC_AMG | LGH_PC_JACOBI */
+  lgh::Hierarchy *mg = nullptr; /* aggregation multigrid (AMG PC) */
   double emin = 0., emax = 0.;
   int bound_its = 0;
   lgh::ZsolveStats stats;

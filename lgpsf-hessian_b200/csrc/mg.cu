@@ -1,0 +1,639 @@
+/* mg.cu -- aggregation multigrid for the Z-solves: the device counterpart
+ * of the reference's PCGAMG preconditioner (zsolve_impl.h:808-818) and of
+ * its mode-3 block V-cycle on the harvested hierarchy (zsolve_impl.h:
+ * 198-485).
+ *
+ * Setup (host, once per prior; PCSetUp's role): smoothed aggregation from
+ * Z's CSR -- greedy aggregates of the strength graph, the constant
+ * near-null space, tentative prolongator smoothed by one damped Jacobi step
+ * (omega = 4/3 / lambda_max(D^{-1} A)), Galerkin coarse operators
+ * A_c = P^T A P, until the coarse size drops below a few thousand; the
+ * coarsest operator is inverted densely on the device (Cholesky + inverse
+ * factor, the reference's dense-LU coarse solve).  Per level, the smoothing
+ * interval [0.1, smoother_top] * lambda_max(D^{-1} A_l) from CG-Lanczos
+ * (zsolve_impl.h:284-313, 340-341) and nu = 2 Chebyshev-Jacobi terms.
+ *
+ * Solve (device): the block V-cycle in correction form, every operation on
+ * row-major blocks: Chebyshev-Jacobi pre-smoothing (the fused k_cheb kernel
+ * keeps the residual current), restriction R_c = P^T R (CSR of P^T),
+ * recursion, prolongation X += P X_c, residual refresh and post-smoothing;
+ * coarse level X = A_0^{-1} B as a dense product.
+ */
+
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <type_traits>
+#include <vector>
+
+#include "lgh_device.cuh"
+#include "lgh_internal.h"
+#include "lgh_ktime.h"
+#include "lgh_mg.h"
+
+namespace lgh
+{
+
+/* ---- host CSR helpers -------------------------------------------------- */
+
+struct HCsr
+{
+  int64_t n = 0, m = 0; /* rows, cols */
+  std::vector<int64_t> rp;
+  std::vector<int32_t> ci;
+  std::vector<double> v;
+};
+
+static double
+hcsr_diag (const HCsr &A, int64_t i)
+{
+  for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++)
+    if (A.ci[k] == i) return A.v[k];
+  return 0.;
+}
+
+static void
+hcsr_mult (const HCsr &A, const std::vector<double> &x, std::vector<double> &y)
+{
+  y.assign (A.n, 0.);
+  for (int64_t i = 0; i < A.n; i++) {
+    double s = 0.;
+    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++) s += A.v[k] * x[A.ci[k]];
+    y[i] = s;
+  }
+}
+
+static HCsr
+hcsr_transpose (const HCsr &A)
+{
+  HCsr T;
+  T.n = A.m;
+  T.m = A.n;
+  T.rp.assign (T.n + 1, 0);
+  for (int64_t k = 0; k < A.rp[A.n]; k++) T.rp[A.ci[k] + 1]++;
+  for (int64_t i = 0; i < T.n; i++) T.rp[i + 1] += T.rp[i];
+  T.ci.resize (A.rp[A.n]);
+  T.v.resize (A.rp[A.n]);
+  std::vector<int64_t> pos (T.rp.begin (), T.rp.end () - 1);
+  for (int64_t i = 0; i < A.n; i++)
+    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++) {
+      const int64_t p = pos[A.ci[k]]++;
+      T.ci[p] = (int32_t) i;
+      T.v[p] = A.v[k];
+    }
+  return T;
+}
+
+/* C = A B (Gustavson, dense accumulator), columns sorted per row */
+static HCsr
+hcsr_gemm (const HCsr &A, const HCsr &B)
+{
+  HCsr C;
+  C.n = A.n;
+  C.m = B.m;
+  C.rp.assign (C.n + 1, 0);
+  std::vector<double> acc (B.m, 0.);
+  std::vector<int32_t> mark (B.m, -1), cols;
+  for (int64_t i = 0; i < A.n; i++) {
+    cols.clear ();
+    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++) {
+      const int64_t j = A.ci[k];
+      const double a = A.v[k];
+      for (int64_t q = B.rp[j]; q < B.rp[j + 1]; q++) {
+        const int32_t c = B.ci[q];
+        if (mark[c] != (int32_t) i) {
+          mark[c] = (int32_t) i;
+          acc[c] = 0.;
+          cols.push_back (c);
+        }
+        acc[c] += a * B.v[q];
+      }
+    }
+    std::sort (cols.begin (), cols.end ());
+    for (int32_t c : cols) {
+      C.ci.push_back (c);
+      C.v.push_back (acc[c]);
+    }
+    C.rp[i + 1] = (int64_t) C.ci.size ();
+  }
+  return C;
+}
+
+/* lambda_max(D^{-1} A) from CG-Lanczos with Jacobi (its steps, fixed
+ * hashed probe), the estimate of zsolve_impl.h:284-313; extremal
+ * eigenvalue of the tridiagonal by Sturm bisection */
+static double
+lanczos_lmax (const HCsr &A, int its, uint64_t seed)
+{
+  const int64_t n = A.n;
+  std::vector<double> dinv (n), r (n), z (n), p (n), q (n), x (n, 0.);
+  for (int64_t i = 0; i < n; i++) {
+    const double d = hcsr_diag (A, i);
+    dinv[i] = d != 0. ? 1. / d : 0.;
+    r[i] = 0.5 - (double) ((rng_state_at (seed, i, 0) >> 11) * (1.0 / 9007199254740992.0));
+  }
+  std::vector<double> al, be;
+  double rz = 0., rzold = 0.;
+  for (int64_t i = 0; i < n; i++) { z[i] = dinv[i] * r[i]; rz += r[i] * z[i]; }
+  p = z;
+  for (int k = 0; k < its; k++) {
+    hcsr_mult (A, p, q);
+    double pq = 0.;
+    for (int64_t i = 0; i < n; i++) pq += p[i] * q[i];
+    if (!(pq > 0.)) break;
+    const double a = rz / pq;
+    al.push_back (a);
+    for (int64_t i = 0; i < n; i++) { x[i] += a * p[i]; r[i] -= a * q[i]; }
+    rzold = rz;
+    rz = 0.;
+    for (int64_t i = 0; i < n; i++) { z[i] = dinv[i] * r[i]; rz += r[i] * z[i]; }
+    if (rz <= 1e-300) break;
+    const double b = rz / rzold;
+    be.push_back (b);
+    for (int64_t i = 0; i < n; i++) p[i] = z[i] + b * p[i];
+  }
+  const int m = (int) al.size ();
+  if (m == 0) return 2.0;
+  std::vector<double> d (m), e (m, 0.);
+  for (int k = 0; k < m; k++) {
+    d[k] = 1. / al[k] + (k > 0 ? be[k - 1] / al[k - 1] : 0.);
+    if (k + 1 < m) e[k] = sqrt (fabs (be[k])) / al[k];
+  }
+  /* Gershgorin upper bound, then bisection on the Sturm count */
+  double hi = 0.;
+  for (int k = 0; k < m; k++)
+    hi = std::max (hi, d[k] + fabs (e[k]) + (k > 0 ? fabs (e[k - 1]) : 0.));
+  double lo = 0.;
+  for (int it = 0; it < 200; it++) {
+    const double mid = 0.5 * (lo + hi);
+    int cnt = 0;  /* eigenvalues > mid */
+    double t = d[0] - mid;
+    if (t > 0.) cnt++;
+    for (int k = 1; k < m; k++) {
+      const double den = (t != 0.) ? t : 1e-300;
+      t = d[k] - mid - e[k - 1] * e[k - 1] / den;
+      if (t > 0.) cnt++;
+    }
+    if (cnt >= 1) lo = mid;
+    else hi = mid;
+  }
+  return hi;
+}
+
+/* one smoothed-aggregation coarsening step */
+static void
+sa_coarsen (const HCsr &A, double theta, HCsr &P, int64_t &nc)
+{
+  const int64_t n = A.n;
+  std::vector<double> diag (n);
+  for (int64_t i = 0; i < n; i++) diag[i] = hcsr_diag (A, i);
+  auto strong = [&] (int64_t i, int64_t k) {
+    const int64_t j = A.ci[k];
+    return j != i && fabs (A.v[k]) > theta * sqrt (fabs (diag[i] * diag[j]));
+  };
+  std::vector<int64_t> agg (n, -1);
+  nc = 0;
+  /* pass 1: roots whose strong neighbourhood is free */
+  for (int64_t i = 0; i < n; i++) {
+    if (agg[i] >= 0) continue;
+    bool free_nb = true;
+    for (int64_t k = A.rp[i]; k < A.rp[i + 1] && free_nb; k++)
+      if (strong (i, k) && agg[A.ci[k]] >= 0) free_nb = false;
+    if (!free_nb) continue;
+    agg[i] = nc;
+    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++)
+      if (strong (i, k)) agg[A.ci[k]] = nc;
+    nc++;
+  }
+  /* pass 2: attach to the strongest aggregated neighbour (pass-1 state) */
+  std::vector<int64_t> agg1 = agg;
+  for (int64_t i = 0; i < n; i++) {
+    if (agg1[i] >= 0) continue;
+    double best = -1.;
+    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++)
+      if (strong (i, k) && agg1[A.ci[k]] >= 0 && fabs (A.v[k]) > best) {
+        best = fabs (A.v[k]);
+        agg[i] = agg1[A.ci[k]];
+      }
+  }
+  /* pass 3: leftovers become singletons */
+  for (int64_t i = 0; i < n; i++)
+    if (agg[i] < 0) agg[i] = nc++;
+  /* tentative prolongator (constant near-null space, orthonormal cols) */
+  std::vector<double> sz (nc, 0.);
+  for (int64_t i = 0; i < n; i++) sz[agg[i]] += 1.;
+  std::vector<double> p0 (n);
+  for (int64_t i = 0; i < n; i++) p0[i] = 1. / sqrt (sz[agg[i]]);
+  /* omega = 4/3 / lambda_max(D^{-1}A) */
+  const double lmax = lanczos_lmax (A, 40, 20260813ULL);
+  const double omega = (4.0 / 3.0) / lmax;
+  /* P = (I - omega D^{-1} A) P0, row by row */
+  P.n = n;
+  P.m = nc;
+  P.rp.assign (n + 1, 0);
+  P.ci.clear ();
+  P.v.clear ();
+  std::vector<double> acc;
+  std::vector<int64_t> cols;
+  for (int64_t i = 0; i < n; i++) {
+    cols.clear ();
+    acc.clear ();
+    auto add = [&] (int64_t c, double val) {
+      for (size_t t = 0; t < cols.size (); t++)
+        if (cols[t] == c) { acc[t] += val; return; }
+      cols.push_back (c);
+      acc.push_back (val);
+    };
+    add (agg[i], p0[i]);
+    const double sc = omega / diag[i];
+    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++) {
+      const int64_t j = A.ci[k];
+      add (agg[j], -sc * A.v[k] * p0[j]);
+    }
+    std::vector<size_t> ord (cols.size ());
+    for (size_t t = 0; t < ord.size (); t++) ord[t] = t;
+    std::sort (ord.begin (), ord.end (),
+               [&] (size_t a, size_t b) { return cols[a] < cols[b]; });
+    for (size_t t : ord) {
+      if (acc[t] == 0.) continue;
+      P.ci.push_back ((int32_t) cols[t]);
+      P.v.push_back (acc[t]);
+    }
+    P.rp[i + 1] = (int64_t) P.ci.size ();
+  }
+}
+
+
+/* ---- device kernels ------------------------------------------------------ */
+
+/* Y = A^{-1} B for the dense coarse level: A^{-1} n0 x n0 (symmetric),
+ * B, Y n0 x w row-major (ld) */
+template <typename T>
+__global__ void __launch_bounds__ (256)
+k_dense_apply (int n0, const double *__restrict__ Ainv, const T *__restrict__ B,
+               T *__restrict__ Y, int w, int ld)
+{
+  __shared__ double As[32][33];
+  __shared__ double Bs[32][65];
+  const int i0 = blockIdx.x * 32, c0 = blockIdx.y * 64;
+  const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;  /* 64 x 4 */
+  double acc[8];
+#pragma unroll
+  for (int a = 0; a < 8; a++) acc[a] = 0.;
+  for (int k0 = 0; k0 < n0; k0 += 32) {
+    for (int e = threadIdx.x; e < 32 * 32; e += 256) {
+      const int r = e & 31, k = e >> 5;
+      const int gi = i0 + r, gk = k0 + k;
+      As[r][k] = (gi < n0 && gk < n0) ? Ainv[gi + (size_t) gk * n0] : 0.;
+    }
+    for (int e = threadIdx.x; e < 32 * 64; e += 256) {
+      const int k = e >> 6, c = e & 63;
+      const int gk = k0 + k, gc = c0 + c;
+      Bs[k][c] = (gk < n0 && gc < w) ? (double) B[(size_t) gk * ld + gc] : 0.;
+    }
+    __syncthreads ();
+#pragma unroll 4
+    for (int k = 0; k < 32; k++) {
+      const double b = Bs[k][tx];
+#pragma unroll
+      for (int a = 0; a < 8; a++) acc[a] = fma (As[ty + 4 * a][k], b, acc[a]);
+    }
+    __syncthreads ();
+  }
+#pragma unroll
+  for (int a = 0; a < 8; a++) {
+    const int gi = i0 + ty + 4 * a, gc = c0 + tx;
+    if (gi < n0 && gc < ld) Y[(size_t) gi * ld + gc] = (gc < w) ? (T) acc[a] : T (0);
+  }
+}
+
+/* R = B - A X on row-major blocks (all ld columns; pads of B are zero) */
+template <typename T>
+__global__ void __launch_bounds__ (256)
+k_resid_block (int64_t n, const int64_t *__restrict__ rowptr,
+               const int32_t *__restrict__ col, const T *__restrict__ vals,
+               const T *__restrict__ B, const T *__restrict__ X,
+               T *__restrict__ R, int ld)
+{
+  const int64_t total = n * ld;
+  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t) gridDim.x * blockDim.x) {
+    const int64_t i = e / ld;
+    const int c = (int) (e - i * ld);
+    T s = B[e];
+    for (int64_t k = rowptr[i]; k < rowptr[i + 1]; k++)
+      s = fma (-vals[k], X[(int64_t) col[k] * ld + c], s);
+    R[e] = s;
+  }
+}
+
+/* Y += A X on row-major blocks */
+template <typename T>
+__global__ void __launch_bounds__ (256)
+k_spmm_acc (int64_t n, const int64_t *__restrict__ rowptr,
+            const int32_t *__restrict__ col, const T *__restrict__ vals,
+            const T *__restrict__ X, int ldx, T *__restrict__ Y, int ldy, int w)
+{
+  const int64_t total = n * w;
+  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t) gridDim.x * blockDim.x) {
+    const int64_t i = e / w;
+    const int c = (int) (e - i * w);
+    T s = T (0);
+    for (int64_t k = rowptr[i]; k < rowptr[i + 1]; k++)
+      s = fma (vals[k], X[(int64_t) col[k] * ldx + c], s);
+    Y[i * ldy + c] += s;
+  }
+}
+
+/* ---- host <-> device ------------------------------------------------------ */
+
+/* upload a host CSR into a device Csr (float copy and 1/diag filled) */
+static int
+csr_upload (const HCsr &H, Csr &D)
+{
+  D = Csr ();
+  D.n = H.n;
+  D.ncols = H.m > 0 ? H.m : H.n;
+  D.nnz = H.rp[H.n];
+  LGH_TRY (dalloc ((void **) &D.rowptr, (size_t) (H.n + 1) * sizeof (int64_t)));
+  LGH_TRY (dalloc ((void **) &D.colidx, (size_t) D.nnz * sizeof (int32_t) + 16));
+  LGH_TRY (dalloc ((void **) &D.vals, (size_t) D.nnz * sizeof (double) + 16));
+  LGH_CUDA (cudaMemcpy (D.rowptr, H.rp.data (), (H.n + 1) * sizeof (int64_t),
+                        cudaMemcpyHostToDevice));
+  if (D.nnz) {
+    LGH_CUDA (cudaMemcpy (D.colidx, H.ci.data (), D.nnz * sizeof (int32_t),
+                          cudaMemcpyHostToDevice));
+    LGH_CUDA (cudaMemcpy (D.vals, H.v.data (), D.nnz * sizeof (double),
+                          cudaMemcpyHostToDevice));
+  }
+  return csr_finish (D);
+}
+
+static int
+csr_download (const Csr &D, HCsr &H)
+{
+  H.n = D.n;
+  H.m = D.n;
+  H.rp.resize (D.n + 1);
+  H.ci.resize (D.nnz);
+  H.v.resize (D.nnz);
+  LGH_CUDA (cudaMemcpy (H.rp.data (), D.rowptr, (D.n + 1) * sizeof (int64_t),
+                        cudaMemcpyDeviceToHost));
+  LGH_CUDA (cudaMemcpy (H.ci.data (), D.colidx, D.nnz * sizeof (int32_t),
+                        cudaMemcpyDeviceToHost));
+  LGH_CUDA (cudaMemcpy (H.v.data (), D.vals, D.nnz * sizeof (double),
+                        cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+Hierarchy::~Hierarchy ()
+{
+  for (auto &l : lev) {
+    if (l.own) csr_free (l.A);
+    csr_free (l.P);
+    csr_free (l.R);
+  }
+}
+
+void
+mg_destroy (Hierarchy *h)
+{
+  delete h;
+}
+
+/* smoothed-aggregation hierarchy of Z (level 0 borrows Z's device arrays) */
+int
+mg_build (const Csr &Z, int tile, double smoother_top, int nu, Hierarchy **out)
+{
+  (void) tile;
+  const double t0 = wall ();
+  Hierarchy *h = new Hierarchy ();
+  HCsr A;
+  int rc = csr_download (Z, A);
+  if (rc) { delete h; return rc; }
+  const int64_t coarse_max = 1500;
+  const double theta = 0.0;
+  for (int l = 0; l < 12; l++) {
+    MgLevel lv;
+    lv.n = A.n;
+    lv.nu = nu > 0 ? nu : 2;
+    lv.smax = lanczos_lmax (A, 40, 20260813ULL + (uint64_t) l);
+    lv.slo = 0.1 * lv.smax;
+    lv.shi = smoother_top * lv.smax;
+    if (l == 0) {
+      lv.A = Z;
+      lv.own = 0;
+    } else {
+      rc = csr_upload (A, lv.A);
+      if (rc) { delete h; return rc; }
+    }
+    if (A.n <= coarse_max || l == 11) {
+      /* coarsest: dense inverse on the device, A^{-1} = L^{-T} L^{-1} */
+      const int n0 = (int) A.n;
+      std::vector<double> Dn ((size_t) n0 * n0, 0.);
+      for (int64_t i = 0; i < A.n; i++)
+        for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++)
+          Dn[i + (size_t) A.ci[k] * n0] = A.v[k];
+      h->n0 = n0;
+      DBuf<double> G, G0, Li, work;
+      DBuf<int> info;
+      cudaStream_t s = stream ();
+      rc = G.alloc ((size_t) n0 * n0);
+      if (!rc) rc = G0.alloc ((size_t) n0 * n0);
+      if (!rc) rc = Li.alloc ((size_t) n0 * n0);
+      if (!rc) rc = info.alloc (4);
+      if (!rc) rc = h->Ainv.alloc ((size_t) n0 * n0);
+      if (!rc) rc = work.alloc (gemm_tn_work_elems (n0, n0, n0));
+      if (!rc && cudaMemcpy (G.p, Dn.data (), Dn.size () * sizeof (double),
+                             cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = set_error (LGH_ERR_GPU, "mg: coarse upload");
+      if (!rc) rc = launch_potrf (n0, G.p, G0.p, 1, info.p, s);
+      int hinfo[2] = { 0, 0 };
+      if (!rc && cudaMemcpy (hinfo, info.p, 2 * sizeof (int),
+                             cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = set_error (LGH_ERR_GPU, "mg: coarse info");
+      if (!rc && hinfo[0]) rc = set_error (LGH_ERR_LIB, "mg: coarse operator not SPD");
+      /* Li holds (L^{-1}) transposed: row-major view of L^{-1} */
+      if (!rc) rc = launch_trtri_lower (n0, G.p, Li.p, 1, s);
+      if (!rc) rc = launch_gemm_tn<double> (n0, n0, n0, Li.p, n0, Li.p, n0,
+                                            h->Ainv.p, n0, 1, work.p, work.n, s);
+      if (!rc && cudaStreamSynchronize (s) != cudaSuccess)
+        rc = set_error (LGH_ERR_GPU, "mg: coarse inverse");
+      if (rc) { delete h; return rc; }
+      h->lev.push_back (lv);
+      lv.own = 0;  /* ownership moved into h->lev */
+      break;
+    }
+    HCsr P;
+    int64_t nc = 0;
+    sa_coarsen (A, theta, P, nc);
+    if (nc >= A.n) {
+      /* no coarsening progress: stop here with a dense coarse level is
+       * impossible at this size */
+      delete h;
+      return set_error (LGH_ERR_SUP, "mg: aggregation made no progress at n=%lld",
+                        (long long) A.n);
+    }
+    HCsr R = hcsr_transpose (P);
+    HCsr AP = hcsr_gemm (A, P);
+    HCsr Ac = hcsr_gemm (R, AP);
+    /* symmetrise the Galerkin product against rounding */
+    {
+      HCsr AcT = hcsr_transpose (Ac);
+      for (int64_t i = 0; i < Ac.n; i++)
+        for (int64_t k = Ac.rp[i], kt = AcT.rp[i]; k < Ac.rp[i + 1]; k++, kt++)
+          Ac.v[k] = 0.5 * (Ac.v[k] + AcT.v[kt]);
+    }
+    Ac.m = Ac.n;
+    rc = csr_upload (P, lv.P);
+    if (!rc) rc = csr_upload (R, lv.R);
+    if (rc) { delete h; return rc; }
+    h->lev.push_back (lv);
+    A = std::move (Ac);
+  }
+  h->setup_s = wall () - t0;
+  *out = h;
+  return 0;
+}
+
+/* ---- the block V-cycle ---------------------------------------------------- */
+
+static int
+ew_grid2 (int64_t total)
+{
+  int64_t g = (total + 255) / 256;
+  if (g < 1) g = 1;
+  if (g > num_sms () * 16) g = num_sms () * 16;
+  return (int) g;
+}
+
+template <typename T>
+static int
+mg_work (Hierarchy *h, int ld, MgWork **w0)
+{
+  std::vector<MgWork> &W = std::is_same<T, double>::value ? h->w64 : h->w32;
+  if (W.size () != h->lev.size ()) W.resize (h->lev.size ());
+  for (size_t l = 0; l < h->lev.size (); l++) {
+    MgWork &w = W[l];
+    if (w.cap >= ld) continue;
+    const size_t bytes = (size_t) h->lev[l].n * ld * sizeof (T);
+    LGH_TRY (w.B.alloc (bytes));
+    LGH_TRY (w.X.alloc (bytes));
+    LGH_TRY (w.R0.alloc (bytes));
+    LGH_TRY (w.R1.alloc (bytes));
+    LGH_TRY (w.D0.alloc (bytes));
+    LGH_TRY (w.D1.alloc (bytes));
+    w.cap = ld;
+  }
+  *w0 = W.data ();
+  return 0;
+}
+
+/* Chebyshev-Jacobi smoothing in correction form on level l: R holds
+ * B - A X on entry; nu terms; returns the buffer holding the residual */
+template <typename T>
+static int
+mg_smooth (const MgLevel &lv, T *X, T **Rcur, T **Ralt, T *D0, T *D1, int ld,
+           cudaStream_t s, KTrace *tr)
+{
+  /* X, R, D read and written; the first step reads no D */
+  const double sbase = (double) lv.A.nnz * (sizeof (T) + 4) + 8. * (lv.n + 1);
+  const double sblk = (double) lv.n * ld * sizeof (T);
+  const double theta = 0.5 * (lv.shi + lv.slo);
+  const double delta = 0.5 * (lv.shi - lv.slo);
+  const double sigma1 = theta / delta;
+  double rho_old = 1.0 / sigma1;
+  T *Do = D0, *Dn = D1;
+  for (int k = 1; k <= lv.nu; k++) {
+    double a, b;
+    if (k == 1) { a = 0.; b = 1.0 / theta; }
+    else {
+      const double rho = 1.0 / (2.0 * sigma1 - rho_old);
+      a = rho * rho_old;
+      b = 2.0 * rho / delta;
+      rho_old = rho;
+    }
+    if (tr) LGH_TRY (tr->begin (K_MG_SMOOTH, sbase + (k == 1 ? 5. : 6.) * sblk, s));
+    LGH_TRY (launch_cheb_step<T> (lv.A, X, *Rcur, *Ralt, Do, Dn, ld, a, b,
+                                  k == 1, s));
+    if (tr) LGH_TRY (tr->end (s));
+    std::swap (*Rcur, *Ralt);
+    std::swap (Do, Dn);
+  }
+  return 0;
+}
+
+template <typename T>
+static int
+vcycle_level (Hierarchy *h, MgWork *W, size_t l, const T *B, T *X, int ld,
+              int w, cudaStream_t s, KTrace *trace)
+{
+  const MgLevel &lv = h->lev[l];
+  const int64_t n = lv.n;
+  KTrace *tr = (l == 0) ? trace : nullptr;   /* the fine level only */
+  const double blk = (double) n * ld * sizeof (T);
+  if (l + 1 == h->lev.size ()) {
+    dim3 grid ((unsigned) ((h->n0 + 31) / 32), (unsigned) ((ld + 63) / 64));
+    if (trace) LGH_TRY (trace->begin (K_MG_COARSE,
+                                      (double) h->n0 * h->n0 * 8 + 2. * blk, s));
+    k_dense_apply<T><<<grid, 256, 0, s>>> (h->n0, h->Ainv.p, B, X, w, ld);
+    LGH_LAUNCH_CHECK ();
+    if (trace) LGH_TRY (trace->end (s));
+    return 0;
+  }
+  MgWork &wk = W[l];
+  T *R = (T *) wk.R0.p, *Ra = (T *) wk.R1.p;
+  T *D0 = (T *) wk.D0.p, *D1 = (T *) wk.D1.p;
+  const size_t bytes = (size_t) n * ld * sizeof (T);
+  /* pre-smoothing from X = 0: R = B */
+  LGH_CUDA (cudaMemsetAsync (X, 0, bytes, s));
+  LGH_CUDA (cudaMemcpyAsync (R, B, bytes, cudaMemcpyDeviceToDevice, s));
+  LGH_TRY (mg_smooth<T> (lv, X, &R, &Ra, D0, D1, ld, s, tr));
+  /* restriction, coarse correction, prolongation */
+  MgWork &wc = W[l + 1];
+  T *Bc = (T *) wc.B.p, *Xc = (T *) wc.X.p;
+  const double cblk = (double) h->lev[l + 1].n * ld * sizeof (T);
+  if (tr) LGH_TRY (tr->begin (K_MG_RESTRICT, blk + cblk + 12. * lv.R.nnz, s));
+  LGH_TRY (launch_spmm<T> (lv.R, R, ld, Bc, ld, ld, s));
+  if (tr) LGH_TRY (tr->end (s));
+  LGH_TRY (vcycle_level<T> (h, W, l + 1, Bc, Xc, ld, w, s, trace));
+  const T *pv;
+  if constexpr (std::is_same<T, double>::value) pv = lv.P.vals;
+  else pv = lv.P.vals32;
+  if (tr) LGH_TRY (tr->begin (K_MG_PROLONG, 2. * blk + cblk + 12. * lv.P.nnz, s));
+  k_spmm_acc<T><<<ew_grid2 (n * ld), 256, 0, s>>> (n, lv.P.rowptr, lv.P.colidx,
+                                                   pv, Xc, ld, X, ld, ld);
+  LGH_LAUNCH_CHECK ();
+  if (tr) LGH_TRY (tr->end (s));
+  /* post-smoothing: refresh the residual, then the same polynomial */
+  const T *av;
+  if constexpr (std::is_same<T, double>::value) av = lv.A.vals;
+  else av = lv.A.vals32;
+  if (tr) LGH_TRY (tr->begin (K_MG_RESID, 3. * blk + 12. * lv.A.nnz, s));
+  k_resid_block<T><<<ew_grid2 (n * ld), 256, 0, s>>> (n, lv.A.rowptr,
+                                                      lv.A.colidx, av, B, X, R,
+                                                      ld);
+  LGH_LAUNCH_CHECK ();
+  if (tr) LGH_TRY (tr->end (s));
+  LGH_TRY (mg_smooth<T> (lv, X, &R, &Ra, D0, D1, ld, s, tr));
+  return 0;
+}
+
+template <typename T>
+int
+mg_vcycle (Hierarchy *h, const T *B, T *X, int ld, int w, cudaStream_t s,
+           KTrace *tr)
+{
+  MgWork *W;
+  LGH_TRY (mg_work<T> (h, ld, &W));
+  return vcycle_level<T> (h, W, 0, B, X, ld, w, s, tr);
+}
+
+template int mg_vcycle<double> (Hierarchy *, const double *, double *, int,
+                                int, cudaStream_t, KTrace *);
+template int mg_vcycle<float> (Hierarchy *, const float *, float *, int, int,
+                               cudaStream_t, KTrace *);
+
+} /* namespace lgh */

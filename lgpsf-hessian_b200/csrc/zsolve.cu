@@ -33,6 +33,8 @@
 
 #include "lgh_device.cuh"
 #include "lgh_internal.h"
+#include "lgh_ktime.h"
+#include "lgh_mg.h"
 
 namespace lgh
 {
@@ -64,12 +66,13 @@ struct ZK
   const unsigned gmask = (G == 32) ? 0xffffffffu                             \
       : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));               \
   (void) gmask;                                                              \
-  int64_t r0, r1;                                                            \
-  block_rows (z.n, r0, r1);
+  /* row tiles of ngroups rows interleaved over the CTAs: the resident   \
+   * CTAs sweep one narrow band, so stencil neighbours hit in L2 */      \
+  
 
 /* ---- init: R = S B (pads zero), X = 0, P = 0; rz, norm0, mask ---------- */
 template <typename T, int CH>
-__global__ void __launch_bounds__ (ZS_THREADS)
+__global__ void __launch_bounds__ (ZS_THREADS, (CH * (16 / sizeof (T)) <= 8 ? 3 : 2))
 k_pcg_init (ZK z, const T *__restrict__ dinv, const T *__restrict__ Bsrc,
             int ldb, const double *__restrict__ rs_in, T *X, T *R, T *P,
             int ld, int nvec, int glog, int w, double *partA, double *partB,
@@ -82,7 +85,8 @@ k_pcg_init (ZK z, const T *__restrict__ dinv, const T *__restrict__ Bsrc,
   for (int h = 0; h < CH; h++)
 #pragma unroll
     for (int e = 0; e < W; e++) { aRZ[h][e] = 0.; aZZ[h][e] = 0.; }
-  for (int64_t i = r0 + group; i < r1; i += ngroups) {
+  for (int64_t i = (int64_t) blockIdx.x * ngroups + group; i < z.n;
+       i += (int64_t) gridDim.x * ngroups) {
     const double sc = rs_in ? rs_in[i] : 1.0;
     const double di = (double) dinv[i];
 #pragma unroll
@@ -133,7 +137,7 @@ k_pcg_init (ZK z, const T *__restrict__ dinv, const T *__restrict__ Bsrc,
 
 /* ---- p_new on the fly, q = Z p_new, alpha ------------------------------- */
 template <typename T, int CH>
-__global__ void __launch_bounds__ (ZS_THREADS)
+__global__ void __launch_bounds__ (ZS_THREADS, (CH * (16 / sizeof (T)) <= 8 ? 3 : 2))
 k_pcg_pq (ZK z, const T *__restrict__ vals, const T *__restrict__ dinv,
           const T *__restrict__ R, const T *__restrict__ Pold,
           T *__restrict__ Pnew, T *__restrict__ Qv, int ld, int nvec,
@@ -156,7 +160,8 @@ k_pcg_pq (ZK z, const T *__restrict__ vals, const T *__restrict__ dinv,
   for (int h = 0; h < CH; h++)
 #pragma unroll
     for (int e = 0; e < W; e++) aPQ[h][e] = 0.;
-  for (int64_t i = r0 + group; i < r1; i += ngroups) {
+  for (int64_t i = (int64_t) blockIdx.x * ngroups + group; i < z.n;
+       i += (int64_t) gridDim.x * ngroups) {
     T acc[CH][W];
 #pragma unroll
     for (int h = 0; h < CH; h++)
@@ -225,8 +230,9 @@ k_pcg_pq (ZK z, const T *__restrict__ vals, const T *__restrict__ dinv,
 
 /* ---- x += alpha p, r -= alpha q, dots, beta, convergence ---------------- */
 template <typename T, int CH>
-__global__ void __launch_bounds__ (ZS_THREADS)
-k_pcg_upd (ZK z, const T *__restrict__ dinv, T *X, T *R,
+__global__ void __launch_bounds__ (ZS_THREADS, (CH * (16 / sizeof (T)) <= 8 ? 3 : 2))
+k_pcg_upd (ZK z, const T *__restrict__ dinv, T *__restrict__ X,
+           T *__restrict__ R,
            const T *__restrict__ Pn, const T *__restrict__ Qv, int ld,
            int nvec, int glog, double *partA, double *partB,
            unsigned *counter, double *scal, int *ival, int cap, double rtol,
@@ -248,7 +254,8 @@ k_pcg_upd (ZK z, const T *__restrict__ dinv, T *X, T *R,
   for (int h = 0; h < CH; h++)
 #pragma unroll
     for (int e = 0; e < W; e++) { aRZ[h][e] = 0.; aZZ[h][e] = 0.; }
-  for (int64_t i = r0 + group; i < r1; i += ngroups) {
+  for (int64_t i = (int64_t) blockIdx.x * ngroups + group; i < z.n;
+       i += (int64_t) gridDim.x * ngroups) {
     const T di = dinv[i];
 #pragma unroll
     for (int h = 0; h < CH; h++) {
@@ -306,14 +313,16 @@ k_pcg_upd (ZK z, const T *__restrict__ dinv, T *X, T *R,
 /* ---- Chebyshev: d_new = a d + b D^{-1} r (on the fly at neighbours),
  *      x += d_new, r_new = r - Z d_new (zsolve_impl.h:108-141) ----------- */
 template <typename T, int CH>
-__global__ void __launch_bounds__ (ZS_THREADS)
-k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ dinv, T *X,
+__global__ void __launch_bounds__ (ZS_THREADS, (CH * (16 / sizeof (T)) <= 8 ? 3 : 2))
+k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ dinv,
+        T *__restrict__ X,
         const T *__restrict__ Rold, T *__restrict__ Rnew,
         const T *__restrict__ Dold, T *__restrict__ Dnew, int ld, int nvec,
         int glog, T a, T b, int first)
 {
   ZS_GROUP_SETUP ();
-  for (int64_t i = r0 + group; i < r1; i += ngroups) {
+  for (int64_t i = (int64_t) blockIdx.x * ngroups + group; i < z.n;
+       i += (int64_t) gridDim.x * ngroups) {
     T acc[CH][W];
 #pragma unroll
     for (int h = 0; h < CH; h++)
@@ -369,6 +378,259 @@ k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ dinv, T *X,
   }
 }
 
+/* ---- PCG with an explicit preconditioner z = V(r) (the AMG V-cycle):
+ * p_new = z + beta p_old on the fly at neighbours, q = Z p_new, (p, q) ---- */
+template <typename T, int CH>
+__global__ void __launch_bounds__ (ZS_THREADS, (CH * (16 / sizeof (T)) <= 8 ? 3 : 2))
+k_pcgx_pq (ZK z, const T *__restrict__ vals, const T *__restrict__ Zb,
+           const T *__restrict__ Pold, T *__restrict__ Pnew,
+           T *__restrict__ Qv, int ld, int nvec, int glog, int first,
+           double *partA, unsigned *counter, double *scal, int *ival, int cap)
+{
+  extern __shared__ double red[];
+  ZS_GROUP_SETUP ();
+  const double *beta = scal + S_BETA * cap;
+  T bet[CH][W];
+#pragma unroll
+  for (int h = 0; h < CH; h++)
+#pragma unroll
+    for (int e = 0; e < W; e++) {
+      const int c = (lane + h * G) * W + e;
+      bet[h][e] = (!first && c < ld) ? (T) beta[c] : T (0);
+    }
+  double aPQ[CH][W];
+#pragma unroll
+  for (int h = 0; h < CH; h++)
+#pragma unroll
+    for (int e = 0; e < W; e++) aPQ[h][e] = 0.;
+  for (int64_t i = (int64_t) blockIdx.x * ngroups + group; i < z.n;
+       i += (int64_t) gridDim.x * ngroups) {
+    T acc[CH][W];
+#pragma unroll
+    for (int h = 0; h < CH; h++)
+#pragma unroll
+      for (int e = 0; e < W; e++) acc[h][e] = T (0);
+    const int64_t k0 = z.rowptr[i], k1 = z.rowptr[i + 1];
+    for (int64_t kb = k0; kb < k1; kb += G) {
+      const int cnt = (int) ((k1 - kb) < G ? (k1 - kb) : G);
+      int mc = 0;
+      T mv = T (0);
+      if (lane < cnt) {
+        mc = z.col[kb + lane];
+        mv = vals[kb + lane];
+      }
+      for (int t = 0; t < cnt; t++) {
+        const int c = __shfl_sync (gmask, mc, t, G);
+        const T v = __shfl_sync (gmask, mv, t, G);
+#pragma unroll
+        for (int h = 0; h < CH; h++) {
+          const int vi = lane + h * G;
+          if (vi < nvec) {
+            Pack<T> zj = ldp (Zb + (int64_t) c * ld + vi * W);
+            Pack<T> pj = first ? pzero<T> () : ldp (Pold + (int64_t) c * ld + vi * W);
+#pragma unroll
+            for (int e = 0; e < W; e++)
+              acc[h][e] = fma (v, fma (bet[h][e], pj.v[e], zj.v[e]), acc[h][e]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < CH; h++) {
+      const int vi = lane + h * G;
+      if (vi < nvec) {
+        Pack<T> zi = ldp (Zb + i * ld + vi * W);
+        Pack<T> pi = first ? pzero<T> () : ldp (Pold + i * ld + vi * W);
+        Pack<T> pn, q;
+#pragma unroll
+        for (int e = 0; e < W; e++) {
+          pn.v[e] = fma (bet[h][e], pi.v[e], zi.v[e]);
+          q.v[e] = acc[h][e];
+          aPQ[h][e] += (double) pn.v[e] * (double) q.v[e];
+        }
+        stp (Pnew + i * ld + vi * W, pn);
+        stp (Qv + i * ld + vi * W, q);
+      }
+    }
+  }
+  block_colsum_store<T, CH> (aPQ, lane, group, G, nvec, ld, red, partA);
+  const double *rz = scal + S_RZ * cap;
+  double *al = scal + S_ALPHA * cap;
+  int *act = ival + I_ACTIVE * cap;
+  last_block_reduce (partA, ld, counter, [&] (int c, double pq) {
+    if (act[c]) {
+      if (pq != 0. && isfinite (pq)) al[c] = rz[c] / pq;
+      else { al[c] = 0.; act[c] = 0; }
+    } else {
+      al[c] = 0.;
+    }
+  });
+}
+
+/* x += alpha p, r -= alpha q (no reductions) */
+template <typename T>
+__global__ void
+k_pcgx_upd (int64_t n, int ld, T *__restrict__ X, T *__restrict__ R,
+            const T *__restrict__ Pn,
+            const T *__restrict__ Qv, const double *alpha)
+{
+  constexpr int W = Pack<T>::W;
+  const int nvec = ld / W;
+  const int64_t total = n * nvec;
+  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t) gridDim.x * blockDim.x) {
+    const int64_t i = e / nvec;
+    const int vi = (int) (e - i * nvec);
+    const int64_t o = i * ld + vi * W;
+    Pack<T> x = ldp (X + o), r = ldp (R + o), p = ldp (Pn + o), q = ldp (Qv + o);
+#pragma unroll
+    for (int k = 0; k < W; k++) {
+      const T a = (T) alpha[vi * W + k];
+      x.v[k] = fma (a, p.v[k], x.v[k]);
+      r.v[k] = fma (-a, q.v[k], r.v[k]);
+    }
+    stp (X + o, x);
+    stp (R + o, r);
+  }
+}
+
+/* dots (r, z), (z, z) after the preconditioner: first call sets rz, norm0
+ * and the mask; later calls set beta and test convergence on ||z|| */
+template <typename T, int CH>
+__global__ void __launch_bounds__ (ZS_THREADS, (CH * (16 / sizeof (T)) <= 8 ? 3 : 2))
+k_pcgx_dots (ZK z, const T *__restrict__ R, const T *__restrict__ Zb, int ld,
+             int nvec, int glog, int w, int first, double *partA,
+             double *partB, unsigned *counter, double *scal, int *ival,
+             int cap, double rtol, int iter, double *hist)
+{
+  extern __shared__ double red[];
+  ZS_GROUP_SETUP ();
+  double aRZ[CH][W], aZZ[CH][W];
+#pragma unroll
+  for (int h = 0; h < CH; h++)
+#pragma unroll
+    for (int e = 0; e < W; e++) { aRZ[h][e] = 0.; aZZ[h][e] = 0.; }
+  for (int64_t i = (int64_t) blockIdx.x * ngroups + group; i < z.n;
+       i += (int64_t) gridDim.x * ngroups) {
+#pragma unroll
+    for (int h = 0; h < CH; h++) {
+      const int vi = lane + h * G;
+      if (vi < nvec) {
+        Pack<T> r = ldp (R + i * ld + vi * W), zz = ldp (Zb + i * ld + vi * W);
+#pragma unroll
+        for (int e = 0; e < W; e++) {
+          aRZ[h][e] += (double) r.v[e] * (double) zz.v[e];
+          aZZ[h][e] += (double) zz.v[e] * (double) zz.v[e];
+        }
+      }
+    }
+  }
+  block_colsum_store<T, CH> (aRZ, lane, group, G, nvec, ld, red, partA);
+  block_colsum_store<T, CH> (aZZ, lane, group, G, nvec, ld, red, partB);
+  double *rz = scal + S_RZ * cap, *be = scal + S_BETA * cap;
+  double *al_g = scal + S_ALPHA * cap, *n0 = scal + S_NORM0 * cap;
+  int *act = ival + I_ACTIVE * cap, *its = ival + I_ITS * cap;
+  bool last = last_block_reduce2 (partA, partB, ld, counter,
+      [&] (int c, double srz, double szz) {
+        if (first) {
+          rz[c] = srz;
+          n0[c] = sqrt (szz);
+          act[c] = (c < w && szz > 0.) ? 1 : 0;
+          al_g[c] = 0.;
+          be[c] = 0.;
+          its[c] = 0;
+          return;
+        }
+        if (!act[c]) { be[c] = 0.; return; }
+        const double b = (rz[c] != 0.) ? srz / rz[c] : 0.;
+        if (hist != nullptr && c == 0 && iter < 10000) {
+          hist[2 * iter] = al_g[0];
+          hist[2 * iter + 1] = b;
+        }
+        rz[c] = srz;
+        be[c] = b;
+        if (sqrt (szz) <= rtol * n0[c] || srz == 0.) {
+          act[c] = 0;
+          be[c] = 0.;
+          al_g[c] = 0.;
+          its[c] = iter + 1;
+        }
+      });
+  if (last) {
+    __syncthreads ();
+    if (threadIdx.x == 0) {
+      int cnt = 0;
+      for (int c = 0; c < ld; c++) cnt += act[c];
+      ival[I_NSLOT * cap] = cnt;
+    }
+  }
+}
+
+/* Chebyshev with an explicit preconditioner: d_new = a d + b z on the fly
+ * at neighbours, x += d_new, r_new = r - Z d_new */
+template <typename T, int CH>
+__global__ void __launch_bounds__ (ZS_THREADS, (CH * (16 / sizeof (T)) <= 8 ? 3 : 2))
+k_chebx (ZK z, const T *__restrict__ vals, const T *__restrict__ Zb,
+         T *__restrict__ X,
+         const T *__restrict__ Rold, T *__restrict__ Rnew,
+         const T *__restrict__ Dold, T *__restrict__ Dnew, int ld, int nvec,
+         int glog, T a, T b, int first)
+{
+  ZS_GROUP_SETUP ();
+  for (int64_t i = (int64_t) blockIdx.x * ngroups + group; i < z.n;
+       i += (int64_t) gridDim.x * ngroups) {
+    T acc[CH][W];
+#pragma unroll
+    for (int h = 0; h < CH; h++)
+#pragma unroll
+      for (int e = 0; e < W; e++) acc[h][e] = T (0);
+    const int64_t k0 = z.rowptr[i], k1 = z.rowptr[i + 1];
+    for (int64_t kb = k0; kb < k1; kb += G) {
+      const int cnt = (int) ((k1 - kb) < G ? (k1 - kb) : G);
+      int mc = 0;
+      T mv = T (0);
+      if (lane < cnt) {
+        mc = z.col[kb + lane];
+        mv = vals[kb + lane];
+      }
+      for (int t = 0; t < cnt; t++) {
+        const int c = __shfl_sync (gmask, mc, t, G);
+        const T v = __shfl_sync (gmask, mv, t, G);
+#pragma unroll
+        for (int h = 0; h < CH; h++) {
+          const int vi = lane + h * G;
+          if (vi < nvec) {
+            Pack<T> zj = ldp (Zb + (int64_t) c * ld + vi * W);
+            Pack<T> dj = first ? pzero<T> () : ldp (Dold + (int64_t) c * ld + vi * W);
+#pragma unroll
+            for (int e = 0; e < W; e++)
+              acc[h][e] = fma (v, fma (b, zj.v[e], a * dj.v[e]), acc[h][e]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < CH; h++) {
+      const int vi = lane + h * G;
+      if (vi < nvec) {
+        const int64_t o = i * ld + vi * W;
+        Pack<T> ri = ldp (Rold + o), x = ldp (X + o), zi = ldp (Zb + o);
+        Pack<T> di = first ? pzero<T> () : ldp (Dold + o);
+        Pack<T> dn, rn;
+#pragma unroll
+        for (int e = 0; e < W; e++) {
+          dn.v[e] = fma (b, zi.v[e], a * di.v[e]);
+          x.v[e] += dn.v[e];
+          rn.v[e] = ri.v[e] - acc[h][e];
+        }
+        stp (X + o, x);
+        stp (Dnew + o, dn);
+        stp (Rnew + o, rn);
+      }
+    }
+  }
+}
+
 /* ---- FP64 residual, R = S B - Z X (pads zero), per-column ||D^{-1} R|| and
  * ||D^{-1} S B|| (refinement and tests) ---------------------------------- */
 template <typename TO, int CH>
@@ -389,7 +651,8 @@ k_zresid (ZK z, const double *__restrict__ vals,
 #pragma unroll
     for (int e = 0; e < W; e++) { aR[h][e] = 0.; aB[h][e] = 0.; }
   const int ld = nvec * W;
-  for (int64_t i = r0 + group; i < r1; i += ngroups) {
+  for (int64_t i = (int64_t) blockIdx.x * ngroups + group; i < z.n;
+       i += (int64_t) gridDim.x * ngroups) {
     double acc[CH][W];
 #pragma unroll
     for (int h = 0; h < CH; h++)
@@ -480,6 +743,7 @@ ZWork::alloc (int64_t n_, int cap_, int is32_)
   LGH_TRY (P0.alloc (blk));
   LGH_TRY (P1.alloc (blk));
   LGH_TRY (Q.alloc (blk));
+  LGH_TRY (Zb.alloc (blk));
   nblocks = num_sms () * 4;
   LGH_TRY (partA.alloc ((size_t) cap * nblocks));
   LGH_TRY (partB.alloc ((size_t) cap * nblocks));
@@ -532,17 +796,27 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
   constexpr int W = Pack<T>::W;
   (void) mg;
   if (w <= 0 || n == 0) return 0;
-  LGH_CHECK (cfg.mode != 3, LGH_ERR_SUP, "zsolve: mode 3 not available");
+  LGH_CHECK (cfg.mode != 3 || mg != nullptr, LGH_ERR_SUP,
+             "zsolve: mode 3 needs the multigrid preconditioner");
   LGH_CHECK (Z.dinv != nullptr, LGH_ERR_ARG_WRONGSTATE, "zsolve: Z has no diagonal");
   const double t0 = wall ();
   int tile = ws.cap;
   if (cfg.mode >= 2 && cfg.tile > 0) tile = std::min (tile, round_ld (cfg.tile));
   tile = std::max (4, tile & ~3);
-  const int maxcols = 32 * ZS_MAXCH * W;
+  /* FP32 tiles stop at 4 chunks per lane (their FP64 dot accumulators
+   * would spill beyond that) */
+  const int maxcols = 32 * (sizeof (T) == 4 ? 4 : ZS_MAXCH) * W;
   tile = std::min (tile, maxcols);
   const T *vals = zvals<T> (Z);
   const T *dinv = zdinv<T> (Z);
   ZK zk{ Z.n, Z.rowptr, Z.colidx };
+  /* optional per-kernel event timing (lgh_kernel_timing) */
+  const bool timing = ktime_on ();
+  static thread_local EventRing ring;
+  std::vector<int> tids;
+  std::vector<double> tbytes;
+  const double zbytes = (double) Z.nnz * (sizeof (T) + 4) + 8. * (Z.n + 1)
+                        + (double) Z.n * sizeof (T);
   T *bX = (T *) ws.X.p, *bR = (T *) ws.R.p, *bP0 = (T *) ws.P0.p,
     *bP1 = (T *) ws.P1.p, *bQ = (T *) ws.Q.p;
   std::vector<int> its_h;
@@ -570,10 +844,129 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
     LGH_LAUNCH_CHECK ();
 
     int iters = 0;
-    if (cfg.mode <= 1) {
+    T *bZ = (T *) ws.Zb.p;
+    if (cfg.mode <= 1 && mg != nullptr) {
+      /* PCG with the V-cycle: z = V(r) each iteration (the reference's
+       * per-column CG + PCGAMG, zsolve_impl.h:674-683, 808-818) */
+      const int egrid = std::max (1, std::min (num_sms () * 8,
+                                  (int) ((n * (ldt / W) + 255) / 256)));
+      static thread_local KTrace ktr;
+      KTrace *tr = timing ? &ktr : nullptr;
+      const double bw = (double) n * wt * sizeof (T);
+      LGH_TRY (mg_vcycle<T> (mg, bR, bZ, ldt, wt, s, tr));
+      ZS_DISPATCH (ch, {
+        auto kd = k_pcgx_dots<T, CH_>;
+        set_smem_attr (kd, smem);
+        kd<<<grid, ZS_THREADS, smem, s>>> (zk, bR, bZ, ldt, nvec, glog, wt, 1,
+                                           ws.partA.p, ws.partB.p,
+                                           ws.counters.p + 1, ws.scal.p,
+                                           ws.ival.p, cap, cfg.rtol, 0, nullptr);
+      });
+      LGH_LAUNCH_CHECK ();
       T *Pold = bP0, *Pnew = bP1;
       int h_nact = 1;
       for (int it = 0; it < cfg.maxit; it++) {
+        if (tr) LGH_TRY (tr->begin (K_PCGX_PQ, zbytes + (it == 0 ? 3. : 4.) * bw, s));
+        ZS_DISPATCH (ch, {
+          auto k1 = k_pcgx_pq<T, CH_>;
+          set_smem_attr (k1, smem);
+          k1<<<grid, ZS_THREADS, smem, s>>> (zk, vals, bZ, Pold, Pnew, bQ, ldt,
+                                             nvec, glog, it == 0, ws.partA.p,
+                                             ws.counters.p, ws.scal.p,
+                                             ws.ival.p, cap);
+        });
+        LGH_LAUNCH_CHECK ();
+        if (tr) LGH_TRY (tr->end (s));
+        if (tr) LGH_TRY (tr->begin (K_PCGX_UPD, 6. * bw, s));
+        k_pcgx_upd<T><<<egrid, 256, 0, s>>> (n, ldt, bX, bR, Pnew, bQ,
+                                            ws.scal.p + S_ALPHA * cap);
+        LGH_LAUNCH_CHECK ();
+        if (tr) LGH_TRY (tr->end (s));
+        LGH_TRY (mg_vcycle<T> (mg, bR, bZ, ldt, wt, s, tr));
+        if (tr) LGH_TRY (tr->begin (K_PCGX_DOTS, 2. * bw, s));
+        ZS_DISPATCH (ch, {
+          auto kd = k_pcgx_dots<T, CH_>;
+          kd<<<grid, ZS_THREADS, smem, s>>> (zk, bR, bZ, ldt, nvec, glog, wt, 0,
+                                             ws.partA.p, ws.partB.p,
+                                             ws.counters.p + 1, ws.scal.p,
+                                             ws.ival.p, cap, cfg.rtol, it,
+                                             record_hist ? ws.hist.p : nullptr);
+        });
+        LGH_LAUNCH_CHECK ();
+        if (tr) LGH_TRY (tr->end (s));
+        std::swap (Pold, Pnew);
+        iters = it + 1;
+        if (iters % 2 == 0 || iters == cfg.maxit || iters <= 2) {
+          LGH_CUDA (cudaMemcpyAsync (&h_nact, nact, sizeof (int),
+                                     cudaMemcpyDeviceToHost, s));
+          LGH_CUDA (cudaStreamSynchronize (s));
+          if (tr) LGH_TRY (tr->drain ());
+          if (h_nact == 0) break;
+        }
+      }
+      if (tr && !tr->ids.empty ()) {
+        LGH_CUDA (cudaStreamSynchronize (s));
+        LGH_TRY (tr->drain ());
+      }
+      if (st) {
+        its_h.resize (ldt);
+        std::vector<int> act_h (ldt);
+        LGH_CUDA (cudaMemcpyAsync (its_h.data (), ws.ival.p + I_ITS * cap,
+                                   ldt * sizeof (int), cudaMemcpyDeviceToHost, s));
+        LGH_CUDA (cudaMemcpyAsync (act_h.data (), ws.ival.p + I_ACTIVE * cap,
+                                   ldt * sizeof (int), cudaMemcpyDeviceToHost, s));
+        LGH_CUDA (cudaStreamSynchronize (s));
+        for (int c = 0; c < wt; c++) st->col_iters += act_h[c] ? iters : its_h[c];
+        if (h_nact > 0) st->last_maxit_hit = 1;
+        st->cols += wt;
+      }
+    } else if (cfg.mode >= 2 && mg != nullptr) {
+      /* Chebyshev around the V-cycle (modes 2/3: zsolve_impl.h:108-141
+       * with the AMG / harvested-hierarchy preconditioner) */
+      const double theta = 0.5 * (cfg.lmax + cfg.lmin);
+      const double delta = 0.5 * (cfg.lmax - cfg.lmin);
+      const double sigma1 = theta / delta;
+      double rho_old = 1.0 / sigma1;
+      T *Ro = bR, *Rn = bQ, *Do = bP0, *Dn = bP1;
+      for (int k = 1; k <= cfg.nit; k++) {
+        double a, b;
+        if (k == 1) { a = 0.; b = 1.0 / theta; }
+        else {
+          const double rho = 1.0 / (2.0 * sigma1 - rho_old);
+          a = rho * rho_old;
+          b = 2.0 * rho / delta;
+          rho_old = rho;
+        }
+        static thread_local KTrace ktc;
+        KTrace *tc = (timing && k % 4 == 0) ? &ktc : nullptr;
+        LGH_TRY (mg_vcycle<T> (mg, Ro, bZ, ldt, wt, s, tc));
+        if (tc) LGH_TRY (tc->begin (K_CHEBX, zbytes + 7. * (double) n * wt * sizeof (T), s));
+        ZS_DISPATCH (ch, {
+          k_chebx<T, CH_><<<grid, ZS_THREADS, 0, s>>> (zk, vals, bZ, bX, Ro, Rn,
+                                                       Do, Dn, ldt, nvec, glog,
+                                                       (T) a, (T) b, k == 1);
+        });
+        LGH_LAUNCH_CHECK ();
+        if (tc) {
+          LGH_TRY (tc->end (s));
+          LGH_CUDA (cudaStreamSynchronize (s));
+          LGH_TRY (tc->drain ());
+        }
+        std::swap (Ro, Rn);
+        std::swap (Do, Dn);
+      }
+      iters = cfg.nit;
+      if (st) { st->col_iters += (long) iters * wt; st->cols += wt; }
+    } else if (cfg.mode <= 1) {
+      T *Pold = bP0, *Pnew = bP1;
+      int h_nact = 1;
+      const double bw = (double) n * wt * sizeof (T);
+      for (int it = 0; it < cfg.maxit; it++) {
+        if (timing) {
+          LGH_TRY (ring.record (s));
+          tids.push_back (K_PCG_PQ);
+          tbytes.push_back (zbytes + (it == 0 ? 3. : 4.) * bw);
+        }
         ZS_DISPATCH (ch, {
           auto k1 = k_pcg_pq<T, CH_>;
           set_smem_attr (k1, smem);
@@ -581,6 +974,11 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
                                              bQ, ldt, nvec, glog, it == 0,
                                              ws.partA.p, ws.counters.p,
                                              ws.scal.p, ws.ival.p, cap);
+          if (timing) {
+            LGH_TRY (ring.record (s));
+            tids.push_back (K_PCG_UPD);
+            tbytes.push_back (6. * bw + (double) n * sizeof (T));
+          }
           auto k2 = k_pcg_upd<T, CH_>;
           set_smem_attr (k2, smem);
           k2<<<grid, ZS_THREADS, smem, s>>> (zk, dinv, bX, bR, Pnew, bQ, ldt,
@@ -591,14 +989,30 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
                                              record_hist ? ws.hist.p : nullptr);
         });
         LGH_LAUNCH_CHECK ();
+        if (timing) {
+          LGH_TRY (ring.record (s));
+          tids.push_back (-1);
+          tbytes.push_back (0.);
+        }
         std::swap (Pold, Pnew);
         iters = it + 1;
         if (iters % cfg.check_every == 0 || iters == cfg.maxit || iters <= 2) {
           LGH_CUDA (cudaMemcpyAsync (&h_nact, nact, sizeof (int),
                                      cudaMemcpyDeviceToHost, s));
           LGH_CUDA (cudaStreamSynchronize (s));
+          if (timing) {
+            LGH_TRY (ring.drain (tids, tbytes));
+            tids.clear ();
+            tbytes.clear ();
+          }
           if (h_nact == 0) break;
         }
+      }
+      if (timing && !tids.empty ()) {
+        LGH_CUDA (cudaStreamSynchronize (s));
+        LGH_TRY (ring.drain (tids, tbytes));
+        tids.clear ();
+        tbytes.clear ();
       }
       if (st) {
         its_h.resize (ldt);
@@ -628,16 +1042,33 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
           b = 2.0 * rho / delta;
           rho_old = rho;
         }
+        const bool tk = timing && (k % 8 == 0);
+        if (tk) {
+          LGH_TRY (ring.record (s));
+          tids.push_back (K_CHEB);
+          tbytes.push_back (zbytes + 6. * (double) n * wt * sizeof (T));
+        }
         ZS_DISPATCH (ch, {
           k_cheb<T, CH_><<<grid, ZS_THREADS, 0, s>>> (zk, vals, dinv, bX, Ro, Rn,
                                                       Do, Dn, ldt, nvec, glog,
                                                       (T) a, (T) b, k == 1);
         });
         LGH_LAUNCH_CHECK ();
+        if (tk) {
+          LGH_TRY (ring.record (s));
+          tids.push_back (-1);
+          tbytes.push_back (0.);
+        }
         std::swap (Ro, Rn);
         std::swap (Do, Dn);
       }
       iters = cfg.nit;
+      if (timing && !tids.empty ()) {
+        LGH_CUDA (cudaStreamSynchronize (s));
+        LGH_TRY (ring.drain (tids, tbytes));
+        tids.clear ();
+        tbytes.clear ();
+      }
       if (st) { st->col_iters += (long) iters * wt; st->cols += wt; }
     }
     if (st) st->block_iters += iters;
@@ -660,6 +1091,36 @@ template int zsolve_block<float> (const Csr &, const ZsolveCfg &, Hierarchy *,
                                   ZWork &, int64_t, int, const float *, int,
                                   const double *, float *, int, const double *,
                                   ZsolveStats *, int, cudaStream_t);
+
+/* one Chebyshev-Jacobi step on a CSR operator (the multigrid smoother) */
+template <typename T>
+int
+launch_cheb_step (const Csr &A, T *X, const T *Ro, T *Rn, const T *Do, T *Dn,
+                  int ld, double a, double b, int first, cudaStream_t s)
+{
+  constexpr int W = Pack<T>::W;
+  const int nvec = ld / W;
+  int glog, ch;
+  row_group_shape (nvec, glog, ch);
+  const int grid = std::min (row_grid (A.n, glog), num_sms () * 8);
+  ZK zk{ A.n, A.rowptr, A.colidx };
+  const T *vals = zvals<T> (A);
+  const T *dinv = zdinv<T> (A);
+  ZS_DISPATCH (ch, {
+    k_cheb<T, CH_><<<grid, ZS_THREADS, 0, s>>> (zk, vals, dinv, X, Ro, Rn, Do,
+                                                Dn, ld, nvec, glog, (T) a,
+                                                (T) b, first);
+  });
+  LGH_LAUNCH_CHECK ();
+  return 0;
+}
+
+template int launch_cheb_step<double> (const Csr &, double *, const double *,
+                                       double *, const double *, double *,
+                                       int, double, double, int, cudaStream_t);
+template int launch_cheb_step<float> (const Csr &, float *, const float *,
+                                      float *, const float *, float *, int,
+                                      double, double, int, cudaStream_t);
 
 /* per-column ||D^{-1}(S B - Z X)||, ||D^{-1} S B|| ; optional R output */
 template <typename TO>

@@ -21,6 +21,7 @@ c_dbl_p = ctypes.POINTER(ctypes.c_double)
 
 LGH_MEM_HOST, LGH_MEM_DEVICE = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
+PC_AMG, PC_JACOBI = 0, 1
 ERR_NAMES = {0: "SUCCESS", 55: "ERR_MEM", 56: "ERR_SUP", 58: "ERR_ORDER",
              60: "ERR_ARG_SIZ", 62: "ERR_ARG_WRONG",
              63: "ERR_ARG_OUTOFRANGE", 73: "ERR_ARG_WRONGSTATE",
@@ -76,7 +77,8 @@ class PriorMatOpts(ctypes.Structure):
 class ExecOpts(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int),
                 ("inner_rtol", ctypes.c_double),
-                ("max_refine", ctypes.c_int), ("verbose", ctypes.c_int)]
+                ("max_refine", ctypes.c_int), ("verbose", ctypes.c_int),
+                ("rank_cap", ctypes.c_int)]
 
 
 class GlrStats(ctypes.Structure):
@@ -134,6 +136,10 @@ SIGNATURES = {
     "lgh_prior_mat_opts_default": (PriorMatOpts, []),
     "lgh_prior_create_mat": (ctypes.c_int, [P, P, ctypes.POINTER(PriorMatOpts),
                                             ctypes.POINTER(P)]),
+    "lgh_prior_create_mat_pc": (ctypes.c_int, [P, P,
+                                               ctypes.POINTER(PriorMatOpts),
+                                               ctypes.c_int,
+                                               ctypes.POINTER(P)]),
     "lgh_prior_create_ksp": (ctypes.c_int, [P, P,
                                             ctypes.POINTER(PriorMatOpts),
                                             ctypes.POINTER(P)]),
@@ -174,6 +180,11 @@ SIGNATURES = {
                                             ctypes.c_int, P, I64, P, I64]),
     "lgh_glr_logdet_batch": (ctypes.c_int, [P, ctypes.c_int, c_dbl_p,
                                             c_dbl_p]),
+    "lgh_launch_count": (ctypes.c_long, []),
+    "lgh_kernel_timing": (ctypes.c_int, [ctypes.c_int]),
+    "lgh_kernel_timing_get": (ctypes.c_char_p, [ctypes.c_int, c_dbl_p,
+                                                ctypes.POINTER(ctypes.c_long),
+                                                c_dbl_p]),
     "lgh_test_sketch": (ctypes.c_int, [ctypes.c_uint64, I64, I64,
                                        ctypes.c_int, P]),
     "lgh_test_rng_state": (ctypes.c_int, [ctypes.c_uint64, I64, I64,
@@ -341,7 +352,8 @@ class Mat:
 class Prior:
     """lgh_prior_t: Mat path (Z + mass) or callbacks path."""
 
-    def __init__(self, Z=None, mass=None, opts=None, callbacks=None):
+    def __init__(self, Z=None, mass=None, opts=None, callbacks=None,
+                 pc=None):
         L = load()
         self.h = P()
         self.mass = Vec(data=mass)
@@ -363,17 +375,26 @@ class Prior:
         else:
             o = opts if opts is not None else prior_opts()
             self.Z = Z
-            _chk(L.lgh_prior_create_mat(Z.h, self.mass.h, ctypes.byref(o),
-                                        ctypes.byref(self.h)),
-                 "lgh_prior_create_mat")
+            if pc is None:
+                _chk(L.lgh_prior_create_mat(Z.h, self.mass.h, ctypes.byref(o),
+                                            ctypes.byref(self.h)),
+                     "lgh_prior_create_mat")
+            else:
+                code = {"amg": PC_AMG, "jacobi": PC_JACOBI}[pc]
+                _chk(L.lgh_prior_create_mat_pc(Z.h, self.mass.h,
+                                               ctypes.byref(o), code,
+                                               ctypes.byref(self.h)),
+                     "lgh_prior_create_mat_pc")
 
     def info(self):
-        out = np.zeros(8)
+        out = np.zeros(12)
         _chk(load().lgh_prior_get_info(self.h, out.ctypes.data_as(c_dbl_p)),
              "lgh_prior_get_info")
         return dict(emin=out[0], emax=out[1], lmin=out[2], lmax=out[3],
                     nit=int(out[4]), bound_its=int(out[5]),
-                    mean_col_iters=out[6], calls=int(out[7]))
+                    mean_col_iters=out[6], calls=int(out[7]),
+                    mg_levels=int(out[8]), mg_coarse=int(out[9]),
+                    mg_setup_s=out[10], pc=int(out[11]))
 
     def apply(self, x):
         vx, vy = Vec(data=x), Vec(self.n)
@@ -510,6 +531,25 @@ class Glr:
         if _L is not None and getattr(self, "h", None):
             _L.lgh_glr_destroy(self.h)
             self.h = P()
+
+
+def kernel_timing(on):
+    """Switch the library's per-kernel CUDA-event timing on or off."""
+    _chk(load().lgh_kernel_timing(1 if on else 0), "lgh_kernel_timing")
+
+
+def kernel_timing_get():
+    """{name: (device ms, launches, algorithmic bytes)} since switched on."""
+    out = {}
+    i = 0
+    while True:
+        ms, n, by = ctypes.c_double(), ctypes.c_long(), ctypes.c_double()
+        name = load().lgh_kernel_timing_get(i, ctypes.byref(ms),
+                                            ctypes.byref(n), ctypes.byref(by))
+        if name is None:
+            return out
+        out[name.decode()] = (ms.value, n.value, by.value)
+        i += 1
 
 
 # ---- kernel-level test hooks --------------------------------------------

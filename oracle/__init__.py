@@ -98,7 +98,8 @@ def lib():
     L.orc_prior_create.restype = P
     L.orc_prior_create.argtypes = [I64, P, P, P, P, ctypes.c_double,
                                    ctypes.c_int, ctypes.c_int,
-                                   ctypes.c_double, ctypes.c_int]
+                                   ctypes.c_double, ctypes.c_int,
+                                   ctypes.c_int]
     L.orc_prior_info.argtypes = [P, c_dbl_p]
     L.orc_prior_destroy.argtypes = [P]
     L.orc_prior_solveZ.restype = ctypes.c_int
@@ -207,14 +208,17 @@ class Prior:
     """Mat-path prior (lgh_prior_create_mat): Z as CSR + lumped mass."""
 
     def __init__(self, Z, mass, ksp_rtol=1e-12, mode=0, tile=64,
-                 cheb_rtol=1e-10, bound_maxit=200):
+                 cheb_rtol=1e-10, bound_maxit=200, pc="jacobi"):
+        """pc: "jacobi" (default) or "amg" (the oracle's own smoothed-
+        aggregation V-cycle, the stand-in for the reference's PCGAMG)."""
         self.Z = Z
         self.mass = _f64(mass)
         self.h = lib().orc_prior_create(Z.n, Z.rowptr.ctypes.data,
                                         Z.colidx.ctypes.data,
                                         Z.vals.ctypes.data,
                                         self.mass.ctypes.data, ksp_rtol,
-                                        mode, tile, cheb_rtol, bound_maxit)
+                                        mode, tile, cheb_rtol, bound_maxit,
+                                        1 if pc == "amg" else 0)
         self.n = Z.n
 
     def info(self):

@@ -14,12 +14,13 @@
  *
  * Deliberate deviations from the reference (PETSc is absent here):
  *   - Z-solves: the reference's default per-column KSP is CG + PCGAMG
- *     (zsolve_impl.h:808-818).  GAMG is replaced by a Jacobi preconditioner;
- *     the CG recurrence, the preconditioned-norm stopping test at ksp_rtol
- *     and the 10000-iteration cap follow PETSc's KSPCG defaults.  Blocked
- *     mode 2 runs the reference's Chebyshev core (zsolve_impl.h:108-141)
- *     with that same Jacobi preconditioner, bounds from CG-Lanczos on the
- *     reference's deterministic probe (zsolve_impl.h:737-764).
+ *     (zsolve_impl.h:808-818).  GAMG is replaced by a smoothed-aggregation
+ *     V-cycle written here (or, on request, by Jacobi); the CG recurrence,
+ *     the preconditioned-norm stopping test at ksp_rtol and the 10000-
+ *     iteration cap follow PETSc's KSPCG defaults.  Blocked mode 2 runs the
+ *     reference's Chebyshev core (zsolve_impl.h:108-141) with the Jacobi
+ *     preconditioner, bounds from CG-Lanczos on the reference's
+ *     deterministic probe (zsolve_impl.h:737-764).
  *   - MPI: one rank; every MPI_Allreduce is the identity.
  *
  * Parity pins: the RNG is checked bit-for-bit against the reference's own
@@ -228,6 +229,240 @@ orc_set_threads (int nt)
 }
 
 /* ================================================================== */
+/* aggregation multigrid for the oracle's CG: the stand-in for the
+ * reference's PCGAMG (zsolve_impl.h:808-818).  Smoothed aggregation with
+ * the constant near-null space, Galerkin coarse operators, Chebyshev-
+ * Jacobi smoothing (nu = 2 on [0.1, 1.1] lambda_max(D^{-1}A)), dense
+ * Cholesky on the coarsest level (LAPACK).  One V-cycle per CG
+ * iteration.                                                            */
+
+extern "C" {
+void scipy_dpotrs_ (const char *, const int *, const int *, const double *,
+                    const int *, double *, const int *, int *);
+}
+
+struct orc_mglev
+{
+  orc_csr A, P, R; /* R = P^T */
+  std::vector<double> dinv;
+  double lmax;
+};
+
+struct orc_mg
+{
+  std::vector<orc_mglev> lev;
+  int n0 = 0;
+  std::vector<double> chol; /* coarse Cholesky factor, column-major */
+};
+
+static void
+csr_transpose (const orc_csr &A, int64_t ncols, orc_csr &T)
+{
+  T.n = ncols;
+  T.rowptr.assign (ncols + 1, 0);
+  for (int64_t k = 0; k < A.rowptr[A.n]; k++) T.rowptr[A.colidx[k] + 1]++;
+  for (int64_t i = 0; i < ncols; i++) T.rowptr[i + 1] += T.rowptr[i];
+  T.colidx.resize (A.rowptr[A.n]);
+  T.vals.resize (A.rowptr[A.n]);
+  std::vector<int64_t> pos (T.rowptr.begin (), T.rowptr.end () - 1);
+  for (int64_t i = 0; i < A.n; i++)
+    for (int64_t k = A.rowptr[i]; k < A.rowptr[i + 1]; k++) {
+      int64_t p = pos[A.colidx[k]]++;
+      T.colidx[p] = (int) i;
+      T.vals[p] = A.vals[k];
+    }
+}
+
+static void
+csr_product (const orc_csr &A, const orc_csr &B, int64_t bcols, orc_csr &C)
+{
+  C.n = A.n;
+  C.rowptr.assign (A.n + 1, 0);
+  C.colidx.clear ();
+  C.vals.clear ();
+  std::vector<double> acc (bcols, 0.);
+  std::vector<int64_t> mark (bcols, -1);
+  std::vector<int> cols;
+  for (int64_t i = 0; i < A.n; i++) {
+    cols.clear ();
+    for (int64_t k = A.rowptr[i]; k < A.rowptr[i + 1]; k++) {
+      const int j = A.colidx[k];
+      for (int64_t q = B.rowptr[j]; q < B.rowptr[j + 1]; q++) {
+        const int c = B.colidx[q];
+        if (mark[c] != i) { mark[c] = i; acc[c] = 0.; cols.push_back (c); }
+        acc[c] += A.vals[k] * B.vals[q];
+      }
+    }
+    std::sort (cols.begin (), cols.end ());
+    for (int c : cols) { C.colidx.push_back (c); C.vals.push_back (acc[c]); }
+    C.rowptr[i + 1] = (int64_t) C.colidx.size ();
+  }
+}
+
+/* lambda_max(D^{-1} A) by 30 power iterations from a hashed start */
+static double
+power_lmax (const orc_csr &A, const std::vector<double> &dinv)
+{
+  const int64_t n = A.n;
+  std::vector<double> v (n), w (n);
+  for (int64_t i = 0; i < n; i++) v[i] = 0.5 + orc_randn_at (20260813ULL, i, 0);
+  double nrm = 1.;
+  for (int it = 0; it < 30; it++) {
+    csr_mult (&A, v.data (), w.data ());
+    double s = 0.;
+    for (int64_t i = 0; i < n; i++) { w[i] *= dinv[i]; s += w[i] * w[i]; }
+    nrm = sqrt (s);
+    for (int64_t i = 0; i < n; i++) v[i] = w[i] / nrm;
+  }
+  return nrm;
+}
+
+static orc_mg *
+orc_mg_build (const orc_csr &Z)
+{
+  orc_mg *h = new orc_mg;
+  orc_csr A = Z;
+  for (int l = 0; l < 12; l++) {
+    orc_mglev lv;
+    lv.A = A;
+    lv.dinv.assign (A.n, 0.);
+    for (int64_t i = 0; i < A.n; i++)
+      for (int64_t k = A.rowptr[i]; k < A.rowptr[i + 1]; k++)
+        if (A.colidx[k] == i) lv.dinv[i] = 1. / A.vals[k];
+    lv.lmax = power_lmax (A, lv.dinv) * 1.05;
+    if (A.n <= 1500 || l == 11) {
+      const int n0 = (int) A.n;
+      h->n0 = n0;
+      h->chol.assign ((size_t) n0 * n0, 0.);
+      for (int64_t i = 0; i < A.n; i++)
+        for (int64_t k = A.rowptr[i]; k < A.rowptr[i + 1]; k++)
+          h->chol[i + (size_t) A.colidx[k] * n0] = A.vals[k];
+      int info = 0;
+      scipy_dpotrf_ ("L", &n0, h->chol.data (), &n0, &info);
+      h->lev.push_back (lv);
+      break;
+    }
+    /* greedy aggregation over all off-diagonal couplings */
+    const int64_t n = A.n;
+    std::vector<int64_t> agg (n, -1);
+    int64_t nc = 0;
+    for (int64_t i = 0; i < n; i++) {
+      if (agg[i] >= 0) continue;
+      bool ok = true;
+      for (int64_t k = A.rowptr[i]; k < A.rowptr[i + 1]; k++)
+        if (A.colidx[k] != i && agg[A.colidx[k]] >= 0) { ok = false; break; }
+      if (!ok) continue;
+      agg[i] = nc;
+      for (int64_t k = A.rowptr[i]; k < A.rowptr[i + 1]; k++) agg[A.colidx[k]] = nc;
+      nc++;
+    }
+    std::vector<int64_t> a1 = agg;
+    for (int64_t i = 0; i < n; i++) {
+      if (a1[i] >= 0) continue;
+      double best = -1.;
+      for (int64_t k = A.rowptr[i]; k < A.rowptr[i + 1]; k++) {
+        const int j = A.colidx[k];
+        if (j != i && a1[j] >= 0 && fabs (A.vals[k]) > best) {
+          best = fabs (A.vals[k]);
+          agg[i] = a1[j];
+        }
+      }
+    }
+    for (int64_t i = 0; i < n; i++)
+      if (agg[i] < 0) agg[i] = nc++;
+    std::vector<double> sz (nc, 0.), p0 (n);
+    for (int64_t i = 0; i < n; i++) sz[agg[i]] += 1.;
+    for (int64_t i = 0; i < n; i++) p0[i] = 1. / sqrt (sz[agg[i]]);
+    /* smoothed prolongator P = (I - omega D^{-1} A) P0 */
+    const double omega = (4. / 3.) / (lv.lmax / 1.05);
+    orc_csr P;
+    P.n = n;
+    P.rowptr.assign (n + 1, 0);
+    std::vector<int64_t> cols;
+    std::vector<double> vals;
+    for (int64_t i = 0; i < n; i++) {
+      cols.clear ();
+      vals.clear ();
+      auto add = [&] (int64_t c, double v) {
+        for (size_t t = 0; t < cols.size (); t++)
+          if (cols[t] == c) { vals[t] += v; return; }
+        cols.push_back (c);
+        vals.push_back (v);
+      };
+      add (agg[i], p0[i]);
+      for (int64_t k = A.rowptr[i]; k < A.rowptr[i + 1]; k++)
+        add (agg[A.colidx[k]], -omega * lv.dinv[i] * A.vals[k] * p0[A.colidx[k]]);
+      std::vector<size_t> ord (cols.size ());
+      for (size_t t = 0; t < ord.size (); t++) ord[t] = t;
+      std::sort (ord.begin (), ord.end (),
+                 [&] (size_t a, size_t b) { return cols[a] < cols[b]; });
+      for (size_t t : ord)
+        if (vals[t] != 0.) { P.colidx.push_back ((int) cols[t]); P.vals.push_back (vals[t]); }
+      P.rowptr[i + 1] = (int64_t) P.colidx.size ();
+    }
+    orc_csr R, AP, Ac;
+    csr_transpose (P, nc, R);
+    csr_product (A, P, nc, AP);
+    csr_product (R, AP, nc, Ac);
+    lv.P = P;
+    lv.R = R;
+    h->lev.push_back (lv);
+    A = Ac;
+  }
+  return h;
+}
+
+/* Chebyshev-Jacobi smoothing, correction form (zsolve_impl.h:386-404) */
+static void
+orc_mg_smooth (const orc_mglev &lv, const double *b, double *x)
+{
+  const int64_t n = lv.A.n;
+  const double lo = 0.1 * lv.lmax, hi = 1.1 * lv.lmax / 1.05;
+  const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo);
+  const double sigma1 = theta / delta;
+  double rho_old = 1. / sigma1;
+  std::vector<double> r (n), d (n), ad (n);
+  csr_mult (&lv.A, x, ad.data ());
+  for (int64_t i = 0; i < n; i++) r[i] = b[i] - ad[i];
+  for (int k = 1; k <= 2; k++) {
+    if (k == 1) {
+      for (int64_t i = 0; i < n; i++) d[i] = lv.dinv[i] * r[i] / theta;
+    } else {
+      const double rho = 1. / (2. * sigma1 - rho_old);
+      for (int64_t i = 0; i < n; i++)
+        d[i] = rho * rho_old * d[i] + 2. * rho / delta * lv.dinv[i] * r[i];
+      rho_old = rho;
+    }
+    for (int64_t i = 0; i < n; i++) x[i] += d[i];
+    csr_mult (&lv.A, d.data (), ad.data ());
+    for (int64_t i = 0; i < n; i++) r[i] -= ad[i];
+  }
+}
+
+static void
+orc_mg_vcycle (const orc_mg *h, size_t l, const double *b, double *x)
+{
+  const orc_mglev &lv = h->lev[l];
+  const int64_t n = lv.A.n;
+  if (l + 1 == h->lev.size ()) {
+    int n0 = h->n0, one = 1, info = 0;
+    for (int64_t i = 0; i < n; i++) x[i] = b[i];
+    scipy_dpotrs_ ("L", &n0, &one, h->chol.data (), &n0, x, &n0, &info);
+    return;
+  }
+  for (int64_t i = 0; i < n; i++) x[i] = 0.;
+  orc_mg_smooth (lv, b, x);
+  std::vector<double> r (n), bc (lv.R.n), xc (lv.R.n);
+  csr_mult (&lv.A, x, r.data ());
+  for (int64_t i = 0; i < n; i++) r[i] = b[i] - r[i];
+  csr_mult (&lv.R, r.data (), bc.data ());
+  orc_mg_vcycle (h, l + 1, bc.data (), xc.data ());
+  csr_mult (&lv.P, xc.data (), r.data ());
+  for (int64_t i = 0; i < n; i++) x[i] += r[i];
+  orc_mg_smooth (lv, b, x);
+}
+
+/* ================================================================== */
 /* the prior: glr_common_impl.h:81-244 and zsolve_impl.h:93-141,720-823 */
 
 struct orc_prior
@@ -246,6 +481,7 @@ struct orc_prior
   int nit, bound_its;
   /* counters */
   long cg_its_total, cg_solves;
+  orc_mg *mg; /* aggregation multigrid preconditioner, or NULL (Jacobi) */
 };
 
 /* PCG on one column, Jacobi preconditioner: PETSc KSPCG (Hestenes-Stiefel
@@ -260,8 +496,12 @@ pcg_column (const orc_prior *p, const double *b, double *x, double rtol,
   const int64_t n = p->n;
   std::vector<double> r (b, b + n), z (n), pp (n), w (n);
   double beta = 0., betaold = 1., dp, rnorm0;
+  auto pc = [&] () {
+    if (p->mg) orc_mg_vcycle (p->mg, 0, r.data (), z.data ());
+    else for (int64_t i = 0; i < n; i++) z[i] = p->dinv[i] * r[i];
+  };
   for (int64_t i = 0; i < n; i++) x[i] = 0.;
-  for (int64_t i = 0; i < n; i++) z[i] = p->dinv[i] * r[i];
+  pc ();
   dp = 0.;
   for (int64_t i = 0; i < n; i++) dp += z[i] * z[i];
   dp = sqrt (dp);
@@ -288,7 +528,7 @@ pcg_column (const orc_prior *p, const double *b, double *x, double rtol,
       x[i] += a * pp[i];
       r[i] -= a * w[i];
     }
-    for (int64_t i = 0; i < n; i++) z[i] = p->dinv[i] * r[i];
+    pc ();
     dp = 0.;
     for (int64_t i = 0; i < n; i++) dp += z[i] * z[i];
     dp = sqrt (dp);
@@ -368,7 +608,8 @@ cheb_core_col (const orc_prior *p, double lmin, double lmax, int nit,
 extern "C" orc_prior *
 orc_prior_create (int64_t n, const int64_t *zrowptr, const int *zcol,
                   const double *zval, const double *mass, double ksp_rtol,
-                  int mode, int tile, double cheb_rtol, int bound_maxit)
+                  int mode, int tile, double cheb_rtol, int bound_maxit,
+                  int use_mg)
 {
   orc_prior *p = new orc_prior;
   p->refs = 1;
@@ -398,6 +639,7 @@ orc_prior_create (int64_t n, const int64_t *zrowptr, const int *zcol,
   p->bound_its = 0;
   p->cg_its_total = 0;
   p->cg_solves = 0;
+  p->mg = use_mg ? orc_mg_build (p->Z) : NULL;
   if (mode >= 2) {
     std::vector<double> rhs (n), y (n), al, be;
     for (int64_t i = 0; i < n; i++) rhs[i] = orc_randn_at (0xB0BD5ULL, i, 0);
@@ -426,6 +668,7 @@ extern "C" void
 orc_prior_destroy (orc_prior *p)
 {
   if (p == NULL || --p->refs > 0) return;
+  delete p->mg;
   delete p;
 }
 

@@ -88,19 +88,21 @@ def test_spmm_fp32(w):
     assert _rd(Y, ref) < 1e-5
 
 
-def _prior_mat(mode, tile=8, rtol=1e-12):
+def _prior_mat(mode, tile=8, rtol=1e-12, pc="jacobi"):
     p = P.test_prior_mat_problem()
     Z = L.Mat(p["Z"])
     pr = L.Prior(Z=Z, mass=p["mass"],
                  opts=L.prior_opts(blocked_mode=mode, tile=tile,
-                                   ksp_rtol=rtol))
+                                   ksp_rtol=rtol), pc=pc)
     return p, Z, pr
 
 
-@pytest.mark.parametrize("mode", [0, 2])
-def test_zsolve_prior_mat_gates(mode):
-    """tests/test_prior_mat.cpp:141-190 on the device"""
-    p, Z, pr = _prior_mat(mode)
+@pytest.mark.parametrize("mode,pc", [(0, "jacobi"), (2, "jacobi"),
+                                     (0, "amg"), (2, "amg"), (3, "amg")])
+def test_zsolve_prior_mat_gates(mode, pc):
+    """tests/test_prior_mat.cpp:141-190 on the device, for the Jacobi and
+    the multigrid preconditioner (blocked modes 0, 2, 3)"""
+    p, Z, pr = _prior_mat(mode, pc=pc)
     Zd = P.csr_to_dense(p["Z"])
     b = p["probe"]
     xref = np.linalg.solve(Zd, b)
@@ -128,7 +130,8 @@ def test_cheb_bounds_match_oracle():
 def test_zsolve_pcg_c1_vs_oracle(w):
     cfg = P.grid_problem("c1")
     Z = L.Mat(cfg["Z"])
-    pr = L.Prior(Z=Z, mass=cfg["mass"], opts=L.prior_opts(ksp_rtol=1e-10))
+    pr = L.Prior(Z=Z, mass=cfg["mass"], opts=L.prior_opts(ksp_rtol=1e-10),
+                 pc="jacobi")
     X = np.random.default_rng(3).standard_normal((cfg["N"], w))
     Y = L.test_zsolve(pr, X)
     Zo = oracle.Csr(cfg["Z"]["rowptr"], cfg["Z"]["colidx"], cfg["Z"]["vals"])
@@ -244,3 +247,44 @@ def test_syev_graded_spectrum():
     rs = np.sort(ref[top])
     ws = np.sort(w[np.argsort(-np.abs(w))[:20]])
     assert np.max(np.abs(ws - rs) / np.abs(rs)) < 1e-10
+
+
+@pytest.mark.parametrize("w", [1, 7, 64])
+@pytest.mark.parametrize("mode", [0, 3])
+def test_zsolve_amg_c1(w, mode):
+    """The multigrid-preconditioned Z-solve (CG + V-cycle, the reference's
+    CG + PCGAMG; and Chebyshev around the V-cycle, its mode 3) against a
+    dense solve on config 1; it converges in few iterations."""
+    cfg = P.grid_problem("c1")
+    Z = L.Mat(cfg["Z"])
+    pr = L.Prior(Z=Z, mass=cfg["mass"],
+                 opts=L.prior_opts(ksp_rtol=1e-10, blocked_mode=mode,
+                                   tile=0), pc="amg")
+    info0 = pr.info()
+    assert info0["mg_levels"] >= 2 and info0["mg_coarse"] <= 1500
+    X = np.random.default_rng(8).standard_normal((cfg["N"], w))
+    Y = L.test_zsolve(pr, X)
+    ref = np.linalg.solve(P.csr_to_dense(cfg["Z"]), X)
+    worst = max(_rd(Y[:, j], ref[:, j]) for j in range(w))
+    assert worst < 1e-8
+    info = pr.info()
+    if mode == 0:
+        assert info["mean_col_iters"] < 60
+    else:
+        assert info["nit"] < 60
+
+
+def test_zsolve_amg_c2_shape():
+    """config-2 operator (N = 262144): the hierarchy coarsens to a dense
+    level and the V-cycle CG meets rtol 1e-10 in a few tens of iterations,
+    checked by the FP64 residual."""
+    cfg = P.grid_problem("c2")
+    Z = L.Mat(cfg["Z"])
+    pr = L.Prior(Z=Z, mass=cfg["mass"], opts=L.prior_opts(ksp_rtol=1e-10),
+                 pc="amg")
+    X = np.random.default_rng(9).standard_normal((cfg["N"], 4))
+    Y = L.test_zsolve(pr, X)
+    R = X - P.csr_matvec(cfg["Z"], Y)
+    for j in range(4):
+        assert np.linalg.norm(R[:, j]) / np.linalg.norm(X[:, j]) < 1e-7
+    assert pr.info()["mean_col_iters"] < 80
