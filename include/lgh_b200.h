@@ -280,7 +280,8 @@ int lgh_glr_eigs (const lgh_glr_t *glr, int *nkept, const double **lam);
 typedef struct lgh_exec_opts
 {
   int    precision;    /* LGH_PREC_FP64 (default) | LGH_PREC_MIXED       */
-  double inner_rtol;   /* mixed: FP32 inner Z-solve tolerance (1e-5)     */
+  double inner_rtol;   /* mixed: FP32 Z-solve tolerance of the build
+                          (default 1e-6)                                 */
   int    max_refine;   /* mixed: FP64 refinement steps per solve (4)     */
   int    verbose;
   int    rank_cap;     /* keep at most rank_cap modes ("rank r,
@@ -323,6 +324,53 @@ int lgh_glr_sample_batch (lgh_glr_t *glr, int nshift, const double *c,
                           int64_t ldx);
 int lgh_glr_logdet_batch (lgh_glr_t *glr, int nshift, const double *c,
                           double *out);
+
+/* ---- the request loop ---------------------------------------------------
+ * Continuous batching of solve / sample / logdet requests on a resident GLR
+ * object: a worker thread owns a block of `slots` Z-solve columns; each
+ * column carries its own CG state, so requests that arrive while others run
+ * join the same launches as columns free up, and a request's result does not
+ * depend on what it was batched with.  Admission needs free slots for all of
+ * a request's columns and free device memory for its staging buffers above
+ * hbm_reserve of the total.  While a server runs it owns its GLR object and
+ * prior: do not call other functions on them until lgh_server_destroy.   */
+typedef struct lgh_server lgh_server_t;
+
+#define LGH_REQ_SOLVE  0   /* x = H(c)^{-1} rhs, m columns                */
+#define LGH_REQ_SAMPLE 1   /* x = G^{-T} xi, m columns                    */
+#define LGH_REQ_LOGDET 2   /* *out = logdet at c                          */
+
+typedef struct lgh_server_opts
+{
+  int    slots;        /* Z-solve columns in flight (default 64)          */
+  double hbm_reserve;  /* fraction of device memory kept free (0.05)      */
+  int    verbose;
+}
+lgh_server_opts_t;
+
+typedef struct lgh_server_stats
+{
+  long   completed, columns, ticks, pending;
+  double p50_s, p99_s, max_s;   /* request latency, submit to done        */
+  double columns_per_s;
+}
+lgh_server_stats_t;
+
+lgh_server_opts_t lgh_server_opts_default (void);
+int lgh_server_create (lgh_glr_t *glr, const lgh_server_opts_t *opts,
+                       lgh_server_t **server);
+/* in / out: host column-major blocks (n x m, leading dims ldin / ldout)
+ * that stay valid until the request completes; LGH_REQ_LOGDET writes one
+ * double to out.                                                          */
+int lgh_server_submit (lgh_server_t *server, int kind, double c, int m,
+                       const double *in, int64_t ldin, double *out,
+                       int64_t ldout, int64_t *id);
+/* block until request id completes (or timeout_s passes: LGH_ERR_NOT_
+ * CONVERGED); latency_s (nullable) receives submit-to-done seconds.       */
+int lgh_server_wait (lgh_server_t *server, int64_t id, double timeout_s,
+                     double *latency_s);
+int lgh_server_get_stats (lgh_server_t *server, lgh_server_stats_t *stats);
+void lgh_server_destroy (lgh_server_t *server);
 
 /* Per-kernel CUDA-event timing of the hot kernels: switch on (1) / off (0)
  * (either resets the figures); read accumulated device milliseconds,

@@ -459,13 +459,15 @@ prior_solve_vec (lgh_prior_t *p, const double *x, const double *s_in,
 template <typename T>
 int
 prior_solve_rows (lgh_prior_t *p, int w, const T *X, int ldx,
-                  const double *s_in, T *Y, int ldy, const double *s_out)
+                  const double *s_in, T *Y, int ldy, const double *s_out,
+                  double rtol_override)
 {
   cudaStream_t s = stream ();
   if (w == 0) return 0;
   if (p->is_mat) {
     ZsolveCfg cfg;
     prior_zcfg (p, cfg);
+    if (rtol_override > 0.) cfg.rtol = rtol_override;
     int cap = std::min (w, std::is_same<T, double>::value ? 512 : 1024);
     ZWork &ws = std::is_same<T, double>::value ? p->ws64 : p->ws32;
     LGH_TRY (ws.alloc (p->n, cap, std::is_same<T, float>::value));
@@ -505,10 +507,10 @@ prior_solve_rows (lgh_prior_t *p, int w, const T *X, int ldx,
 
 template int prior_solve_rows<double> (lgh_prior_t *, int, const double *, int,
                                        const double *, double *, int,
-                                       const double *);
+                                       const double *, double);
 template int prior_solve_rows<float> (lgh_prior_t *, int, const float *, int,
                                       const double *, float *, int,
-                                      const double *);
+                                      const double *, double);
 
 void
 prior_ref (lgh_prior_t *p)

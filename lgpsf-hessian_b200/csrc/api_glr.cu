@@ -189,8 +189,11 @@ apply_F (lgh_glr_t *g, int w, const T *X, int ldx, T *Y, int ldy, T *W,
 {
   cudaStream_t s = stream ();
   const double *ms = g->prior->msqrt.p;
+  /* FP32 Z-solves run at the mixed form's inner tolerance */
+  const double rt = std::is_same<T, float>::value
+                    ? std::max (g->exec.inner_rtol, g->prior->zcfg.rtol) : 0.;
   double t0 = wall ();
-  LGH_TRY (prior_solve_rows<T> (g->prior, w, X, ldx, ms, W, ldw, nullptr));
+  LGH_TRY (prior_solve_rows<T> (g->prior, w, X, ldx, ms, W, ldw, nullptr, rt));
   double t1 = wall ();
   static thread_local EventRing ring;
   const bool timing = ktime_on ();
@@ -204,7 +207,7 @@ apply_F (lgh_glr_t *g, int w, const T *X, int ldx, T *Y, int ldy, T *W,
     LGH_TRY (ring.drain ({ K_SPMM }, { bytes }));
   }
   double t2 = wall ();
-  LGH_TRY (prior_solve_rows<T> (g->prior, w, Y, ldy, nullptr, Y, ldy, ms));
+  LGH_TRY (prior_solve_rows<T> (g->prior, w, Y, ldy, nullptr, Y, ldy, ms, rt));
   LGH_CUDA (cudaStreamSynchronize (s));
   double t3 = wall ();
   g->stats.t_zsolve += (t1 - t0) + (t3 - t2);
@@ -692,7 +695,7 @@ lgh_exec_opts_default (void)
 {
   lgh_exec_opts_t e;
   e.precision = LGH_PREC_FP64;
-  e.inner_rtol = 1e-5;
+  e.inner_rtol = 1e-6;
   e.max_refine = 4;
   e.verbose = 0;
   e.rank_cap = 0;

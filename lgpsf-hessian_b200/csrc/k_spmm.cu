@@ -17,12 +17,13 @@
 namespace lgh
 {
 
-template <typename T, typename TV, int CH>
+/* MODE 0: Y = A X;  1: Y += A X;  2: Y = B - A X */
+template <typename T, typename TV, int CH, int MODE>
 __global__ void __launch_bounds__ (256)
 k_spmm (int64_t n, const int64_t *__restrict__ rowptr,
         const int32_t *__restrict__ colidx, const TV *__restrict__ vals,
         const T *__restrict__ X, int ldx, T *__restrict__ Y, int ldy,
-        int nvec, int glog)
+        int nvec, int glog, const T *__restrict__ Bm, int ldb)
 {
   constexpr int W = Pack<T>::W;
   const int G = 1 << glog;
@@ -70,8 +71,18 @@ k_spmm (int64_t n, const int64_t *__restrict__ rowptr,
       const int vi = lane + h * G;
       if (vi < nvec) {
         Pack<T> o;
+        if (MODE == 1) {
+          Pack<T> y = ldp (yr + vi * W);
 #pragma unroll
-        for (int e = 0; e < W; e++) o.v[e] = acc[h][e];
+          for (int e = 0; e < W; e++) o.v[e] = y.v[e] + acc[h][e];
+        } else if (MODE == 2) {
+          Pack<T> b = ldp (Bm + i * ldb + vi * W);
+#pragma unroll
+          for (int e = 0; e < W; e++) o.v[e] = b.v[e] - acc[h][e];
+        } else {
+#pragma unroll
+          for (int e = 0; e < W; e++) o.v[e] = acc[h][e];
+        }
         stp (yr + vi * W, o);
       }
     }
@@ -130,13 +141,18 @@ row_grid (int64_t n, int glog)
 template <typename T, typename TV>
 static int
 spmm_dispatch (const Csr &A, const TV *vals, const T *X, int ldx, T *Y,
-               int ldy, int w, cudaStream_t s)
+               int ldy, int w, cudaStream_t s, int mode = 0,
+               const T *Bm = nullptr, int ldb = 0)
 {
   constexpr int W = Pack<T>::W;
   const int MAXCH = 10;
   const bool vec_ok = (ldx % W == 0) && (ldy % W == 0)
-                      && ((uintptr_t) X % 16 == 0) && ((uintptr_t) Y % 16 == 0);
+                      && ((uintptr_t) X % 16 == 0) && ((uintptr_t) Y % 16 == 0)
+                      && (mode != 2 || (ldb % W == 0 && (uintptr_t) Bm % 16 == 0));
   if (!vec_ok) {
+    if (mode != 0)
+      return set_error (LGH_ERR_ARG_WRONG, "spmm: accumulate/residual forms "
+                        "need 16-byte aligned row-major blocks");
     int64_t g = (A.n * 8 + 255) / 256;
     if (g > (int64_t) num_sms () * 16) g = (int64_t) num_sms () * 16;
     if (g < 1) g = 1;
@@ -154,10 +170,18 @@ spmm_dispatch (const Csr &A, const TV *vals, const T *X, int ldx, T *Y,
     const int grid = row_grid (A.n, glog);
     const T *Xc = X + c0;
     T *Yc = Y + c0;
+    const T *Bc = Bm ? Bm + c0 : nullptr;
 #define LGH_SPMM_CASE(C)                                                     \
   case C:                                                                    \
-    k_spmm<T, TV, C><<<grid, 256, 0, s>>> (A.n, A.rowptr, A.colidx, vals,    \
-                                           Xc, ldx, Yc, ldy, nvec, glog);    \
+    if (mode == 0)                                                           \
+      k_spmm<T, TV, C, 0><<<grid, 256, 0, s>>> (A.n, A.rowptr, A.colidx,     \
+          vals, Xc, ldx, Yc, ldy, nvec, glog, Bc, ldb);                      \
+    else if (mode == 1)                                                      \
+      k_spmm<T, TV, C, 1><<<grid, 256, 0, s>>> (A.n, A.rowptr, A.colidx,     \
+          vals, Xc, ldx, Yc, ldy, nvec, glog, Bc, ldb);                      \
+    else                                                                     \
+      k_spmm<T, TV, C, 2><<<grid, 256, 0, s>>> (A.n, A.rowptr, A.colidx,     \
+          vals, Xc, ldx, Yc, ldy, nvec, glog, Bc, ldb);                      \
     break;
     switch (ch) {
       LGH_SPMM_CASE (1) LGH_SPMM_CASE (2) LGH_SPMM_CASE (3)
@@ -187,6 +211,27 @@ launch_spmm<float> (const Csr &A, const float *X, int ldx, float *Y, int ldy,
                     int w, cudaStream_t s)
 {
   return spmm_dispatch<float, float> (A, A.vals32, X, ldx, Y, ldy, w, s);
+}
+
+/* Y += A X (mode 1) or Y = B - A X (mode 2) on aligned row-major blocks */
+template <>
+int
+launch_spmm_mode<double> (const Csr &A, const double *X, int ldx, double *Y,
+                          int ldy, int w, int mode, const double *Bm, int ldb,
+                          cudaStream_t s)
+{
+  return spmm_dispatch<double, double> (A, A.vals, X, ldx, Y, ldy, w, s, mode,
+                                        Bm, ldb);
+}
+
+template <>
+int
+launch_spmm_mode<float> (const Csr &A, const float *X, int ldx, float *Y,
+                         int ldy, int w, int mode, const float *Bm, int ldb,
+                         cudaStream_t s)
+{
+  return spmm_dispatch<float, float> (A, A.vals32, X, ldx, Y, ldy, w, s, mode,
+                                      Bm, ldb);
 }
 
 } /* namespace lgh */

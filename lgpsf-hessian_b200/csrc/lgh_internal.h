@@ -148,6 +148,11 @@ template <typename T>
 int launch_spmm (const Csr &A, const T *X, int ldx, T *Y, int ldy, int w,
                  cudaStream_t s);
 
+/* Y += A X (mode 1) or Y = B - A X (mode 2) */
+template <typename T>
+int launch_spmm_mode (const Csr &A, const T *X, int ldx, T *Y, int ldy, int w,
+                      int mode, const T *Bm, int ldb, cudaStream_t s);
+
 /* elementwise / block helpers (k_vec.cu) */
 template <typename T>
 int launch_rowscale (int64_t n, int w, const double *scale, const T *X,

@@ -92,9 +92,12 @@ void prior_ref (lgh_prior_t *p);
 int prior_applyZ (lgh_prior_t *p, const double *x, double *y);
 int prior_solve_vec (lgh_prior_t *p, const double *x, const double *s_in,
                      double *y, const double *s_out);
+/* rtol_override > 0 replaces the prior's tolerance (FP32 solves of the
+ * mixed build run at the execution options' inner tolerance) */
 template <typename T>
 int prior_solve_rows (lgh_prior_t *p, int w, const T *X, int ldx,
-                      const double *s_in, T *Y, int ldy, const double *s_out);
+                      const double *s_in, T *Y, int ldy, const double *s_out,
+                      double rtol_override = 0.);
 int launch_vec_div (int64_t n, const double *x, const double *d, double *y,
                     cudaStream_t s);
 }

@@ -16,8 +16,9 @@
  * Solve (device): the block V-cycle in correction form, every operation on
  * row-major blocks: Chebyshev-Jacobi pre-smoothing (the fused k_cheb kernel
  * keeps the residual current), restriction R_c = P^T R (CSR of P^T),
- * recursion, prolongation X += P X_c, residual refresh and post-smoothing;
- * coarse level X = A_0^{-1} B as a dense product.
+ * recursion, prolongation X += P X_c and the residual refresh R = B - A X
+ * (the accumulate and residual forms of the row-group CSR product),
+ * post-smoothing; coarse level X = A_0^{-1} B as a dense product.
  */
 
 #include <math.h>
@@ -308,45 +309,6 @@ k_dense_apply (int n0, const double *__restrict__ Ainv, const T *__restrict__ B,
   }
 }
 
-/* R = B - A X on row-major blocks (all ld columns; pads of B are zero) */
-template <typename T>
-__global__ void __launch_bounds__ (256)
-k_resid_block (int64_t n, const int64_t *__restrict__ rowptr,
-               const int32_t *__restrict__ col, const T *__restrict__ vals,
-               const T *__restrict__ B, const T *__restrict__ X,
-               T *__restrict__ R, int ld)
-{
-  const int64_t total = n * ld;
-  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (int64_t) gridDim.x * blockDim.x) {
-    const int64_t i = e / ld;
-    const int c = (int) (e - i * ld);
-    T s = B[e];
-    for (int64_t k = rowptr[i]; k < rowptr[i + 1]; k++)
-      s = fma (-vals[k], X[(int64_t) col[k] * ld + c], s);
-    R[e] = s;
-  }
-}
-
-/* Y += A X on row-major blocks */
-template <typename T>
-__global__ void __launch_bounds__ (256)
-k_spmm_acc (int64_t n, const int64_t *__restrict__ rowptr,
-            const int32_t *__restrict__ col, const T *__restrict__ vals,
-            const T *__restrict__ X, int ldx, T *__restrict__ Y, int ldy, int w)
-{
-  const int64_t total = n * w;
-  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (int64_t) gridDim.x * blockDim.x) {
-    const int64_t i = e / w;
-    const int c = (int) (e - i * w);
-    T s = T (0);
-    for (int64_t k = rowptr[i]; k < rowptr[i + 1]; k++)
-      s = fma (vals[k], X[(int64_t) col[k] * ldx + c], s);
-    Y[i * ldy + c] += s;
-  }
-}
-
 /* ---- host <-> device ------------------------------------------------------ */
 
 /* upload a host CSR into a device Csr (float copy and 1/diag filled) */
@@ -500,15 +462,6 @@ mg_build (const Csr &Z, int tile, double smoother_top, int nu, Hierarchy **out)
 
 /* ---- the block V-cycle ---------------------------------------------------- */
 
-static int
-ew_grid2 (int64_t total)
-{
-  int64_t g = (total + 255) / 256;
-  if (g < 1) g = 1;
-  if (g > num_sms () * 16) g = num_sms () * 16;
-  return (int) g;
-}
-
 template <typename T>
 static int
 mg_work (Hierarchy *h, int ld, MgWork **w0)
@@ -519,8 +472,10 @@ mg_work (Hierarchy *h, int ld, MgWork **w0)
     MgWork &w = W[l];
     if (w.cap >= ld) continue;
     const size_t bytes = (size_t) h->lev[l].n * ld * sizeof (T);
-    LGH_TRY (w.B.alloc (bytes));
-    LGH_TRY (w.X.alloc (bytes));
+    if (l > 0) {   /* the finest level's B and X are the caller's */
+      LGH_TRY (w.B.alloc (bytes));
+      LGH_TRY (w.X.alloc (bytes));
+    }
     LGH_TRY (w.R0.alloc (bytes));
     LGH_TRY (w.R1.alloc (bytes));
     LGH_TRY (w.D0.alloc (bytes));
@@ -599,23 +554,12 @@ vcycle_level (Hierarchy *h, MgWork *W, size_t l, const T *B, T *X, int ld,
   LGH_TRY (launch_spmm<T> (lv.R, R, ld, Bc, ld, ld, s));
   if (tr) LGH_TRY (tr->end (s));
   LGH_TRY (vcycle_level<T> (h, W, l + 1, Bc, Xc, ld, w, s, trace));
-  const T *pv;
-  if constexpr (std::is_same<T, double>::value) pv = lv.P.vals;
-  else pv = lv.P.vals32;
   if (tr) LGH_TRY (tr->begin (K_MG_PROLONG, 2. * blk + cblk + 12. * lv.P.nnz, s));
-  k_spmm_acc<T><<<ew_grid2 (n * ld), 256, 0, s>>> (n, lv.P.rowptr, lv.P.colidx,
-                                                   pv, Xc, ld, X, ld, ld);
-  LGH_LAUNCH_CHECK ();
+  LGH_TRY (launch_spmm_mode<T> (lv.P, Xc, ld, X, ld, ld, 1, nullptr, 0, s));
   if (tr) LGH_TRY (tr->end (s));
   /* post-smoothing: refresh the residual, then the same polynomial */
-  const T *av;
-  if constexpr (std::is_same<T, double>::value) av = lv.A.vals;
-  else av = lv.A.vals32;
   if (tr) LGH_TRY (tr->begin (K_MG_RESID, 3. * blk + 12. * lv.A.nnz, s));
-  k_resid_block<T><<<ew_grid2 (n * ld), 256, 0, s>>> (n, lv.A.rowptr,
-                                                      lv.A.colidx, av, B, X, R,
-                                                      ld);
-  LGH_LAUNCH_CHECK ();
+  LGH_TRY (launch_spmm_mode<T> (lv.A, X, ld, R, ld, ld, 2, B, ld, s));
   if (tr) LGH_TRY (tr->end (s));
   LGH_TRY (mg_smooth<T> (lv, X, &R, &Ra, D0, D1, ld, s, tr));
   return 0;

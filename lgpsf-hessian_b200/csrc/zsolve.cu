@@ -501,7 +501,8 @@ __global__ void __launch_bounds__ (ZS_THREADS, (CH * (16 / sizeof (T)) <= 8 ? 3 
 k_pcgx_dots (ZK z, const T *__restrict__ R, const T *__restrict__ Zb, int ld,
              int nvec, int glog, int w, int first, double *partA,
              double *partB, unsigned *counter, double *scal, int *ival,
-             int cap, double rtol, int iter, double *hist)
+             int cap, double rtol, int iter, double *hist,
+             const int *fresh)
 {
   extern __shared__ double red[];
   ZS_GROUP_SETUP ();
@@ -532,7 +533,7 @@ k_pcgx_dots (ZK z, const T *__restrict__ R, const T *__restrict__ Zb, int ld,
   int *act = ival + I_ACTIVE * cap, *its = ival + I_ITS * cap;
   bool last = last_block_reduce2 (partA, partB, ld, counter,
       [&] (int c, double srz, double szz) {
-        if (first) {
+        if (first || (fresh != nullptr && fresh[c])) {
           rz[c] = srz;
           n0[c] = sqrt (szz);
           act[c] = (c < w && szz > 0.) ? 1 : 0;
@@ -860,7 +861,7 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
         kd<<<grid, ZS_THREADS, smem, s>>> (zk, bR, bZ, ldt, nvec, glog, wt, 1,
                                            ws.partA.p, ws.partB.p,
                                            ws.counters.p + 1, ws.scal.p,
-                                           ws.ival.p, cap, cfg.rtol, 0, nullptr);
+                                           ws.ival.p, cap, cfg.rtol, 0, nullptr, nullptr);
       });
       LGH_LAUNCH_CHECK ();
       T *Pold = bP0, *Pnew = bP1;
@@ -890,7 +891,8 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
                                              ws.partA.p, ws.partB.p,
                                              ws.counters.p + 1, ws.scal.p,
                                              ws.ival.p, cap, cfg.rtol, it,
-                                             record_hist ? ws.hist.p : nullptr);
+                                             record_hist ? ws.hist.p : nullptr,
+                                             nullptr);
         });
         LGH_LAUNCH_CHECK ();
         if (tr) LGH_TRY (tr->end (s));
@@ -1091,6 +1093,80 @@ template int zsolve_block<float> (const Csr &, const ZsolveCfg &, Hierarchy *,
                                   ZWork &, int64_t, int, const float *, int,
                                   const double *, float *, int, const double *,
                                   ZsolveStats *, int, cudaStream_t);
+
+/* ---- one tick of the request loop's slot block (server.cu) ------------- */
+
+template <typename T>
+int
+server_tick_pq (const Csr &Z, const T *Zb, const T *Pold, T *Pnew, T *Q, int ld,
+                ZWork &ws, cudaStream_t s)
+{
+  constexpr int W = Pack<T>::W;
+  const int nvec = ld / W;
+  int glog, ch;
+  row_group_shape (nvec, glog, ch);
+  const int grid = std::min (row_grid (Z.n, glog), ws.nblocks);
+  const int smem = zs_smem_bytes (glog, ld);
+  ZK zk{ Z.n, Z.rowptr, Z.colidx };
+  ZS_DISPATCH (ch, {
+    auto k1 = k_pcgx_pq<T, CH_>;
+    set_smem_attr (k1, smem);
+    k1<<<grid, ZS_THREADS, smem, s>>> (zk, zvals<T> (Z), Zb, Pold, Pnew, Q, ld,
+                                       nvec, glog, 0, ws.partA.p,
+                                       ws.counters.p, ws.scal.p, ws.ival.p,
+                                       ws.cap);
+  });
+  LGH_LAUNCH_CHECK ();
+  return 0;
+}
+
+template <typename T>
+int
+server_tick_upd (int64_t n, int ld, T *X, T *R, const T *Pn, const T *Q,
+                 ZWork &ws, cudaStream_t s)
+{
+  constexpr int W = Pack<T>::W;
+  const int egrid = std::max (1, std::min (num_sms () * 8,
+                              (int) ((n * (ld / W) + 255) / 256)));
+  k_pcgx_upd<T><<<egrid, 256, 0, s>>> (n, ld, X, R, Pn, Q,
+                                       ws.scal.p + S_ALPHA * ws.cap);
+  LGH_LAUNCH_CHECK ();
+  return 0;
+}
+
+template <typename T>
+int
+server_tick_dots (const Csr &Z, const T *R, const T *Zb, int ld, int w,
+                  const int *fresh, double rtol, ZWork &ws, cudaStream_t s)
+{
+  constexpr int W = Pack<T>::W;
+  const int nvec = ld / W;
+  int glog, ch;
+  row_group_shape (nvec, glog, ch);
+  const int grid = std::min (row_grid (Z.n, glog), ws.nblocks);
+  const int smem = zs_smem_bytes (glog, ld);
+  ZK zk{ Z.n, Z.rowptr, Z.colidx };
+  ZS_DISPATCH (ch, {
+    auto kd = k_pcgx_dots<T, CH_>;
+    set_smem_attr (kd, smem);
+    kd<<<grid, ZS_THREADS, smem, s>>> (zk, R, Zb, ld, nvec, glog, w, 0,
+                                       ws.partA.p, ws.partB.p,
+                                       ws.counters.p + 1, ws.scal.p, ws.ival.p,
+                                       ws.cap, rtol, 0, nullptr, fresh);
+  });
+  LGH_LAUNCH_CHECK ();
+  return 0;
+}
+
+template int server_tick_pq<double> (const Csr &, const double *, const double *,
+                                     double *, double *, int, ZWork &,
+                                     cudaStream_t);
+template int server_tick_upd<double> (int64_t, int, double *, double *,
+                                      const double *, const double *, ZWork &,
+                                      cudaStream_t);
+template int server_tick_dots<double> (const Csr &, const double *,
+                                       const double *, int, int, const int *,
+                                       double, ZWork &, cudaStream_t);
 
 /* one Chebyshev-Jacobi step on a CSR operator (the multigrid smoother) */
 template <typename T>

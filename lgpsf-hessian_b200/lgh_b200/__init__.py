@@ -81,6 +81,21 @@ class ExecOpts(ctypes.Structure):
                 ("rank_cap", ctypes.c_int)]
 
 
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("slots", ctypes.c_int), ("hbm_reserve", ctypes.c_double),
+                ("verbose", ctypes.c_int)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_long), ("columns", ctypes.c_long),
+                ("ticks", ctypes.c_long), ("pending", ctypes.c_long),
+                ("p50_s", ctypes.c_double), ("p99_s", ctypes.c_double),
+                ("max_s", ctypes.c_double), ("columns_per_s", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class GlrStats(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int64), ("ell", ctypes.c_int),
                 ("kept", ctypes.c_int), ("precision", ctypes.c_int),
@@ -180,6 +195,16 @@ SIGNATURES = {
                                             ctypes.c_int, P, I64, P, I64]),
     "lgh_glr_logdet_batch": (ctypes.c_int, [P, ctypes.c_int, c_dbl_p,
                                             c_dbl_p]),
+    "lgh_server_opts_default": (ServerOpts, []),
+    "lgh_server_create": (ctypes.c_int, [P, ctypes.POINTER(ServerOpts),
+                                         ctypes.POINTER(P)]),
+    "lgh_server_submit": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_int, P, I64, P, I64,
+                                         ctypes.POINTER(I64)]),
+    "lgh_server_wait": (ctypes.c_int, [P, I64, ctypes.c_double,
+                                       ctypes.POINTER(ctypes.c_double)]),
+    "lgh_server_get_stats": (ctypes.c_int, [P, ctypes.POINTER(ServerStats)]),
+    "lgh_server_destroy": (None, [P]),
     "lgh_launch_count": (ctypes.c_long, []),
     "lgh_kernel_timing": (ctypes.c_int, [ctypes.c_int]),
     "lgh_kernel_timing_get": (ctypes.c_char_p, [ctypes.c_int, c_dbl_p,
@@ -550,6 +575,66 @@ def kernel_timing_get():
             return out
         out[name.decode()] = (ms.value, n.value, by.value)
         i += 1
+
+
+class Server:
+    """The request loop (lgh_server_*) over a resident Glr object."""
+
+    SOLVE, SAMPLE, LOGDET = 0, 1, 2
+
+    def __init__(self, glr, slots=64, hbm_reserve=0.05):
+        L = load()
+        o = L.lgh_server_opts_default()
+        o.slots = slots
+        o.hbm_reserve = hbm_reserve
+        self.h = P()
+        self.glr = glr
+        self.n = glr.n
+        self._bufs = {}
+        _chk(L.lgh_server_create(glr.h, ctypes.byref(o), ctypes.byref(self.h)),
+             "lgh_server_create")
+
+    def submit(self, kind, c, X=None):
+        """Queue a request; returns its id.  X: (n, m) host block."""
+        L = load()
+        rid = I64()
+        if kind == self.LOGDET:
+            out = np.zeros(1)
+            _chk(L.lgh_server_submit(self.h, kind, c, 0, None, 0,
+                                     out.ctypes.data, 1, ctypes.byref(rid)),
+                 "lgh_server_submit")
+            self._bufs[rid.value] = (None, out)
+            return rid.value
+        Xin = np.asfortranarray(X, dtype=np.float64)
+        out = np.zeros_like(Xin, order="F")
+        _chk(L.lgh_server_submit(self.h, kind, c, Xin.shape[1],
+                                 Xin.ctypes.data, self.n, out.ctypes.data,
+                                 self.n, ctypes.byref(rid)),
+             "lgh_server_submit")
+        self._bufs[rid.value] = (Xin, out)
+        return rid.value
+
+    def wait(self, rid, timeout=600.0):
+        lat = ctypes.c_double()
+        _chk(load().lgh_server_wait(self.h, rid, timeout, ctypes.byref(lat)),
+             "lgh_server_wait")
+        _, out = self._bufs.pop(rid)
+        return (out[0] if out.ndim == 1 else np.ascontiguousarray(out)), \
+            lat.value
+
+    def stats(self):
+        st = ServerStats()
+        _chk(load().lgh_server_get_stats(self.h, ctypes.byref(st)),
+             "lgh_server_get_stats")
+        return st.as_dict()
+
+    def close(self):
+        if _L is not None and getattr(self, "h", None):
+            _L.lgh_server_destroy(self.h)
+            self.h = P()
+
+    def __del__(self):
+        self.close()
 
 
 # ---- kernel-level test hooks --------------------------------------------
