@@ -372,6 +372,19 @@ int lgh_server_wait (lgh_server_t *server, int64_t id, double timeout_s,
 int lgh_server_get_stats (lgh_server_t *server, lgh_server_stats_t *stats);
 void lgh_server_destroy (lgh_server_t *server);
 
+/* G = X^T X (w x w, column-major, ldg) of a row-major device block X
+ * (n x w, ldx) without any device allocation.  No counterpart in the
+ * reference: for callers that fix the device memory budget up front and
+ * forbid a library to allocate.  Its split-K partial sums live in one
+ * fixed 8 MiB device array inside the library, so w <= 1024 (w * w <=
+ * 2^20 doubles; larger w returns LGH_ERR_ARG_OUTOFRANGE).  Make the first
+ * call on each device before any stream capture begins (it looks the
+ * array's address up once per device).  Calls share that array: calls from
+ * different host threads race on it and must be serialised.  The call
+ * synchronises before returning.                                          */
+int lgh_gram_noalloc (int64_t n, int w, const double *X, int64_t ldx,
+                      double *G, int64_t ldg);
+
 /* Per-kernel CUDA-event timing of the hot kernels: switch on (1) / off (0)
  * (either resets the figures); read accumulated device milliseconds,
  * launches and algorithmic bytes of kernel id 0 k_pcg_pq, 1 k_pcg_upd,

@@ -217,6 +217,7 @@ SIGNATURES = {
     "lgh_test_spmm": (ctypes.c_int, [P, ctypes.c_int, P, P, ctypes.c_int]),
     "lgh_test_zsolve": (ctypes.c_int, [P, ctypes.c_int, P, P, ctypes.c_int]),
     "lgh_test_gram": (ctypes.c_int, [I64, ctypes.c_int, P, P]),
+    "lgh_gram_noalloc": (ctypes.c_int, [I64, ctypes.c_int, P, I64, P, I64]),
     "lgh_test_gemm_nn": (ctypes.c_int, [I64, ctypes.c_int, ctypes.c_int, P,
                                         P, P]),
     "lgh_test_potrf": (ctypes.c_int, [ctypes.c_int, P, ctypes.c_int, P, P,
