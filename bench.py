@@ -18,7 +18,8 @@ stream (the legacy default stream), max over ranks.  Also reported: the
 same jobs end to end through the C ABI from pinned host buffers (e2e), the
 per-kernel roofline of the dominant kernel from the library's live event
 timing, per-RHS solve latency p50/p99, SM clocks sampled during the timed
-region, and the CPU baseline (the oracle on the host cores, a bounded
+region, a Poisson request stream through the request loop (serving), and
+the CPU baseline (the oracle on the host cores, a bounded
 sample extrapolated to a job).
 
 --impl reference: the reference's CPU path restated by the oracle
@@ -60,6 +61,14 @@ def parse():
                     help="sketch columns in the CPU sample (0 = host cores)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-rate", type=float, default=20.0)
+    ap.add_argument("--serve-s", type=float, default=5.0)
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--config", default="c2", choices=["c2", "c3", "c4"],
+                    help="c2: the headline job (default); c3 / c4: the "
+                         "mixed-precision 3D extend and the batched-shift "
+                         "workloads, one JSON line each")
     return ap.parse_args()
 
 
@@ -278,19 +287,25 @@ def run_ours(args):
     clocks.start()
     L.kernel_timing(True)
     launches0 = Lb.lgh_launch_count()
+    rt0 = L.runtime_counters()
     t_start, t_end = torch.cuda.Event(enable_timing=True), \
         torch.cuda.Event(enable_timing=True)
     timers = []
+    torch.cuda.nvtx.range_push("timed")
     t_start.record()
     for _ in range(args.steps):
         job(timers)
     t_end.record()
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
     ktimes = L.kernel_timing_get()
     L.kernel_timing(False)
     launches = Lb.lgh_launch_count() - launches0
+    rt1 = L.runtime_counters()
+    runtime = {k: (rt1[k] - rt0[k]) / args.steps
+               for k in ("allocs", "alloc_s", "frees", "free_s")}
     clk = clocks.stop()
     elapsed = t_start.elapsed_time(t_end) / 1e3
     if world > 1:
@@ -393,8 +408,16 @@ def run_ours(args):
                          "traffic": traffic, "peak_source": peak_note,
                          "bytes_per_launch": kbytes / kn if kn else None,
                          "launch_ms": kms / kn if kn else None},
-            "kernels": kernels, "gpu_launches": launches, "clocks": clk}
+            "kernels": kernels, "gpu_launches": launches, "clocks": clk,
+            "host_per_job": dict(runtime, **{k: stats[k] for k in (
+                "t_build", "t_sketch", "t_zsolve", "t_spmm", "t_orth",
+                "t_eig", "t_check")})}
 
+    if not args.no_mixed:
+        line["mixed"] = run_mixed_job(args, B, pr, opts, N, g_last, rhs, xout,
+                                      L, torch)
+    if not args.no_serve:
+        line["serving"] = run_serving(args, g_last, N, L)
     if not args.no_e2e:
         line["e2e"] = run_e2e(args, cfg, L, torch, world, dist)
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -406,6 +429,130 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def _sin_max(U1, U2):
+    """Largest principal angle (sine) between two orthonormal column sets."""
+    sv = np.linalg.svd(U2.T @ U1, compute_uv=False)
+    return float(np.sqrt(max(0.0, 1.0 - float(np.min(sv)) ** 2)))
+
+
+def accuracy_vs_fp64(g64, g32, x64, x32, c):
+    """Errors of a mixed-precision result against the FP64 one on the same
+    inputs: eigenvalues (relative to the largest, and per eigenvalue),
+    the largest principal angle of the leading 20 eigenvectors, solve
+    agreement, logdet relative difference."""
+    l64, l32 = g64.eigs(), g32.eigs()
+    k = min(len(l64), len(l32))
+    d = np.abs(l32[:k] - l64[:k])
+    kk = min(20, k)
+    U64, U32 = g64.U()[:, :kk], g32.U()[:, :kk]
+    ld64, ld32 = g64.logdet(c), g32.logdet(c)
+    return {"kept_fp64": int(len(l64)), "kept_mixed": int(len(l32)),
+            "eig_err_rel_max": float(d.max() / abs(l64[0])),
+            "eig_err_rel_each": float(np.max(d / np.abs(l64[:k]))),
+            "subspace_sin_top%d" % kk: _sin_max(U64, U32),
+            "solve_rel_diff": float(np.linalg.norm(x32 - x64)
+                                    / np.linalg.norm(x64)),
+            "logdet_rel_diff": float(abs(ld32 - ld64) / abs(ld64))}
+
+
+def run_mixed_job(args, B, pr, opts, N, g64, rhs, xout, L, torch):
+    """The same job (build + 16-RHS solve + logdet) with LGH_PREC_MIXED:
+    FP32 sketch blocks, F-applies and CholQR2 sweeps (FP64 accumulation),
+    FP64 Rayleigh-Ritz; solves through FP32 Z-sweeps refined in FP64 to the
+    same Z tolerance.  Timed like the headline (CUDA events, W warm-up
+    jobs), errors against the FP64 job's results."""
+    Lb = L.load()
+    ex = L.exec_opts(rank_cap=RANK, precision=L.PREC_MIXED)
+    cs = np.array([SHIFT])
+    xm = L.DeviceBlock(N, NRHS)
+    x64 = xout.get()
+
+    def job():
+        g = L.Glr(B, pr, opts, exec=ex)
+        L._chk(Lb.lgh_glr_solve_batch(g.h, 1, cs.ctypes.data_as(L.c_dbl_p),
+                                      NRHS, rhs.ptr(), N, xm.ptr(), N),
+               "lgh_glr_solve_batch")
+        g.logdet(SHIFT)
+        return g
+
+    for _ in range(max(1, args.warmup - 2)):
+        job()
+    torch.cuda.synchronize()
+    info0 = pr.info()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    bt, st = [], []
+    g = None
+    for _ in range(args.steps):
+        evs[0].record()
+        g = L.Glr(B, pr, opts, exec=ex)
+        evs[1].record()
+        L._chk(Lb.lgh_glr_solve_batch(g.h, 1, cs.ctypes.data_as(L.c_dbl_p),
+                                      NRHS, rhs.ptr(), N, xm.ptr(), N),
+               "lgh_glr_solve_batch")
+        g.logdet(SHIFT)
+        evs[2].record()
+        torch.cuda.synchronize()
+        bt.append(evs[0].elapsed_time(evs[1]) / 1e3)
+        st.append(evs[1].elapsed_time(evs[2]) / 1e3)
+    info1 = pr.info()
+    acc = accuracy_vs_fp64(g64, g, x64, xm.get(), SHIFT)
+    calls = info1["refine_calls"] - info0["refine_calls"]
+    steps = info1["refine_steps"] - info0["refine_steps"]
+    out = {"jobs_per_s": 1.0 / (statistics.mean(bt) + statistics.mean(st)),
+           "build_s": statistics.mean(bt),
+           "solves_per_s": NRHS / statistics.mean(st),
+           "refine_steps_per_solve": steps / calls if calls else None,
+           "inner_rtol": ex.inner_rtol}
+    out.update(acc)
+    return out
+
+
+def run_serving(args, g, N, L):
+    """Continuous batching through the request loop (lgh_server_*) on the
+    built object: a seeded Poisson stream at --serve-rate requests/s for
+    --serve-s seconds, 60/30/10 solve/sample/logdet, m ~ U{1..64} columns,
+    shifts log-uniform in [1e-3, 1e3]; submit-to-done latency per request
+    and completed columns per second (first submit to last completion)."""
+    rng = np.random.default_rng(2024)
+    rate, window = args.serve_rate, args.serve_s
+    t, arrivals = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > window:
+            break
+        u = rng.random()
+        kind = 0 if u < 0.6 else (1 if u < 0.9 else 2)
+        m = int(rng.integers(1, 65))
+        c = float(10.0 ** rng.uniform(-3, 3))
+        arrivals.append((t, kind, m, c))
+    mmax = max(m for _, k, m, _ in arrivals if k != 2)
+    pool = np.asfortranarray(rng.standard_normal((N, mmax)))
+    sv = L.Server(g, slots=64)
+    ids = []
+    t0 = time.perf_counter()
+    for ta, kind, m, c in arrivals:
+        dt = ta - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        ids.append(sv.submit(kind, c, None if kind == 2 else pool[:, :m]))
+    lat = []
+    for i in ids:
+        lat.append(sv.wait(i, timeout=600.0)[1])
+    t1 = time.perf_counter()
+    st = sv.stats()
+    sv.close()
+    lat.sort()
+    cols = sum(m for _, k, m, _ in arrivals if k != 2)
+    return {"requests": len(arrivals), "offered_per_s": rate,
+            "window_s": window, "slots": 64, "columns": cols,
+            "columns_per_s": cols / (t1 - t0),
+            "p50_ms": 1e3 * lat[len(lat) // 2],
+            "p99_ms": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+            "max_ms": 1e3 * lat[-1], "ticks": st["ticks"],
+            "mix": "60/30/10 solve/sample/logdet, m~U{1..64}, "
+                   "c log-uniform [1e-3, 1e3]"}
 
 
 def run_e2e(args, cfg, L, torch, world, dist):
@@ -490,12 +637,136 @@ def run_e2e(args, cfg, L, torch, world, dist):
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
 
 
+def _events(torch, k):
+    return [torch.cuda.Event(enable_timing=True) for _ in range(k)]
+
+
+def run_c3(args):
+    """Config 3: 96^3 3D grid (N = 884736), Z = h L + 16 M (7-point),
+    B Gaussian (0.012) x Wendland (0.025), a = 1 + sin sin sin / 2;
+    lgh_glr_compute at ell = 200 then lgh_glr_extend by 200 (to 400), in
+    mixed precision and in FP64 on the same inputs; build and extend
+    seconds and the mixed-vs-FP64 errors.  One JSON line."""
+    import torch
+    import lgh_b200 as L
+    from lgh_b200 import problems as P
+    torch.cuda.set_device(0)
+    cfg = P.grid_problem("c3")
+    N = cfg["N"]
+    B, Z = L.Mat(cfg["B"]), L.Mat(cfg["Z"])
+    pr = L.Prior(Z=Z, mass=cfg["mass"], opts=L.prior_opts(ksp_rtol=ZRTOL))
+    opts = L.glr_opts(ell=200, q_power=1, seed=SEED, trunc_rel=0.0, check=1)
+    rhs = np.random.default_rng(5).standard_normal(N)
+    res = {}
+    gs = {}
+    for name, prec in (("mixed", L.PREC_MIXED), ("fp64", L.PREC_FP64)):
+        ex = L.exec_opts(precision=prec)
+        L.Glr(B, pr, L.glr_opts(ell=40, seed=SEED, check=0), exec=ex)  # warm
+        ev = _events(torch, 3)
+        ev[0].record()
+        g = L.Glr(B, pr, opts, exec=ex)
+        ev[1].record()
+        g.extend(200)
+        ev[2].record()
+        torch.cuda.synchronize()
+        res[name] = {"build_s": ev[0].elapsed_time(ev[1]) / 1e3,
+                     "extend_s": ev[1].elapsed_time(ev[2]) / 1e3,
+                     "kept": int(len(g.eigs()))}
+        gs[name] = g
+    x64 = gs["fp64"].solve(1.0, rhs)
+    x32 = gs["mixed"].solve(1.0, rhs)
+    res["mixed_vs_fp64"] = accuracy_vs_fp64(gs["fp64"], gs["mixed"], x64, x32,
+                                            1.0)
+    line = {"metric": "GLR build + extend seconds (ell 200 -> 400)",
+            "value": res["mixed"]["build_s"] + res["mixed"]["extend_s"],
+            "unit": "s", "higher_is_better": False, "n_gpus": 1,
+            "dtype": "f32 blocks / f64 core (mixed)",
+            "data": "synthetic (config formulas)",
+            "config": {"workload": "c3: 96^3 3D grid (N=%d), B %.1f nnz/row, "
+                                   "Z = h L + 16 M (7-point), ell 200 then "
+                                   "extend 200, q=1, Z rtol %g"
+                                   % (N, cfg["nnz_B"] / N, ZRTOL),
+                       "N": N, "nnz_B": cfg["nnz_B"]},
+            "results": res}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_c4(args):
+    """Config 4: the C2 operator built once at ell = 420 (rank cap 400),
+    then 64 shifts log-spaced in [1e-3, 1e3] x 256 N(0,1) right-hand sides
+    through lgh_glr_solve_batch and lgh_glr_sample_batch (shift-independent
+    Z-solves once, per-shift Woodbury combinations), and logdet at all 64
+    shifts; FP64 and mixed.  Right-hand-side columns per second.  One JSON
+    line."""
+    import torch
+    import lgh_b200 as L
+    from lgh_b200 import problems as P
+    torch.cuda.set_device(0)
+    cfg = P.grid_problem(CONFIG)
+    N = cfg["N"]
+    B, Z = L.Mat(cfg["B"]), L.Mat(cfg["Z"])
+    pr = L.Prior(Z=Z, mass=cfg["mass"], opts=L.prior_opts(ksp_rtol=ZRTOL))
+    cs = np.logspace(-3, 3, 64)
+    m = 256
+    R = L.DeviceBlock(N, m, np.random.default_rng(8).standard_normal((N, m)))
+    Xo = L.DeviceBlock(N, m * len(cs))
+    Lb = L.load()
+    res = {}
+    for name, prec in (("fp64", L.PREC_FP64), ("mixed", L.PREC_MIXED)):
+        ex = L.exec_opts(precision=prec, rank_cap=400)
+        g = L.Glr(B, pr, L.glr_opts(ell=420, seed=SEED, trunc_rel=0.0,
+                                    check=0), exec=ex)
+        csp = cs.ctypes.data_as(L.c_dbl_p)
+        ld = np.empty_like(cs)
+        # warm-up (also forms W = Z^{-1} M^{1/2} U once per build)
+        L._chk(Lb.lgh_glr_solve_batch(g.h, 1, csp, 8, R.ptr(), N, Xo.ptr(),
+                                      N), "warm")
+        torch.cuda.synchronize()
+        ev = _events(torch, 4)
+        ev[0].record()
+        L._chk(Lb.lgh_glr_solve_batch(g.h, len(cs), csp, m, R.ptr(), N,
+                                      Xo.ptr(), N), "solve_batch")
+        ev[1].record()
+        L._chk(Lb.lgh_glr_sample_batch(g.h, len(cs), csp, m, R.ptr(), N,
+                                       Xo.ptr(), N), "sample_batch")
+        ev[2].record()
+        L._chk(Lb.lgh_glr_logdet_batch(g.h, len(cs), csp,
+                                       ld.ctypes.data_as(L.c_dbl_p)), "ld")
+        ev[3].record()
+        torch.cuda.synchronize()
+        ts = ev[0].elapsed_time(ev[1]) / 1e3
+        tp = ev[1].elapsed_time(ev[2]) / 1e3
+        res[name] = {"kept": int(len(g.eigs())), "solve_s": ts,
+                     "sample_s": tp,
+                     "logdet_64_ms": ev[2].elapsed_time(ev[3]),
+                     "solve_cols_per_s": m * len(cs) / ts,
+                     "sample_cols_per_s": m * len(cs) / tp}
+        del g
+    line = {"metric": "batched solve columns/s (64 shifts x 256 RHS)",
+            "value": res["mixed"]["solve_cols_per_s"], "unit": "columns/s",
+            "higher_is_better": True, "n_gpus": 1,
+            "dtype": "f32 sweeps / f64 core (mixed); fp64 beside",
+            "data": "synthetic (config formulas)",
+            "config": {"workload": "c4: c2 operator, ell 420 (rank 400), "
+                                   "64 shifts log-spaced [1e-3, 1e3] x 256 "
+                                   "RHS, solve + sample + logdet",
+                       "N": N},
+            "results": res}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.config == "c3":
+        return run_c3(args)
+    if args.config == "c4":
+        return run_c4(args)
     return run_ours(args)
 
 

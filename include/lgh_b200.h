@@ -181,10 +181,11 @@ int lgh_prior_solve (lgh_prior_t *prior, lgh_Vec x, lgh_Vec y);
 int lgh_prior_solve_block (lgh_prior_t *prior, int m, const double *X,
                            int64_t ldx, double *Y, int64_t ldy);
 
-/* Diagnostics of a Mat-path prior's Z-solver: out[0..11] = Lanczos emin,
+/* Diagnostics of a Mat-path prior's Z-solver: out[0..13] = Lanczos emin,
  * emax, margined lmin, lmax, Chebyshev nit, probe iterations, mean
  * per-column CG iterations so far, number of solve calls, multigrid
- * levels, coarse size, multigrid setup seconds, preconditioner type.    */
+ * levels, coarse size, multigrid setup seconds, preconditioner type,
+ * mixed-precision refined solves, and their refinement steps.          */
 int lgh_prior_get_info (const lgh_prior_t *prior, double *out);
 
 /* ---- glr.h --------------------------------------------------------------- */
@@ -332,8 +333,11 @@ int lgh_glr_logdet_batch (lgh_glr_t *glr, int nshift, const double *c,
  * join the same launches as columns free up, and a request's result does not
  * depend on what it was batched with.  Admission needs free slots for all of
  * a request's columns and free device memory for its staging buffers above
- * hbm_reserve of the total.  While a server runs it owns its GLR object and
- * prior: do not call other functions on them until lgh_server_destroy.   */
+ * hbm_reserve of the total.  The loop has its own stream and work
+ * buffers and only reads the GLR object and its prior, so the read-only
+ * operations (solve, sample, logdet and their batched forms) may be
+ * called beside it; lgh_glr_extend and the destroy calls must wait until
+ * lgh_server_destroy.                                                    */
 typedef struct lgh_server lgh_server_t;
 
 #define LGH_REQ_SOLVE  0   /* x = H(c)^{-1} rhs, m columns                */
@@ -396,6 +400,11 @@ const char *lgh_kernel_timing_get (int id, double *ms, long *launches,
 
 /* Number of this library's kernel launches since the process started.   */
 long lgh_launch_count (void);
+
+/* Host-side runtime counters since the process started: out[0..4] =
+ * device allocations, seconds in them, device frees, seconds in them,
+ * kernel launches.                                                        */
+int lgh_runtime_counters (double *out);
 
 /* Last error message of the calling thread (empty if none).              */
 const char *lgh_last_error (void);

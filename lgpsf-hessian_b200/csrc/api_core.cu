@@ -14,6 +14,7 @@
 #include <string.h>
 
 #include <chrono>
+#include <map>
 #include <mutex>
 
 #include "lgh_device.cuh"
@@ -88,10 +89,24 @@ wall ()
       .count ();
 }
 
+RuntimeCounters g_rt;
+
+static std::mutex g_rt_mu;
+
+static void
+rt_add (double &sec, long &cnt, double dt)
+{
+  std::lock_guard<std::mutex> lk (g_rt_mu);
+  sec += dt;
+  cnt++;
+}
+
 int
 dalloc (void **p, size_t bytes)
 {
+  const double t0 = wall ();
   cudaError_t e = cudaMalloc (p, bytes ? bytes : 256);
+  rt_add (g_rt.alloc_s, g_rt.allocs, wall () - t0);
   if (e != cudaSuccess) {
     *p = nullptr;
     cudaGetLastError ();
@@ -104,7 +119,10 @@ dalloc (void **p, size_t bytes)
 void
 dfree (void *p)
 {
-  if (p) cudaFree (p);
+  if (!p) return;
+  const double t0 = wall ();
+  cudaFree (p);
+  rt_add (g_rt.free_s, g_rt.frees, wall () - t0);
 }
 
 /* ---- CSR helpers --------------------------------------------------------- */
@@ -126,6 +144,19 @@ k_csr_diag (int64_t n, const int64_t *rowptr, const int32_t *col,
     dinv32[i] = (float) di;
     atomicMax (maxnnz, (int) (rowptr[i + 1] - rowptr[i]));
   }
+}
+
+__global__ void
+k_csr_vd (int64_t n, const int64_t *rowptr, const int32_t *col,
+          const double *vals, const double *dinv, double *vd, float *vd32)
+{
+  for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t) gridDim.x * blockDim.x)
+    for (int64_t k = rowptr[i]; k < rowptr[i + 1]; k++) {
+      const double v = vals[k] * dinv[col[k]];
+      vd[k] = v;
+      vd32[k] = (float) v;
+    }
 }
 
 __global__ void
@@ -165,6 +196,14 @@ csr_finish (Csr &A)
   LGH_CUDA (cudaMemcpyAsync (h, flags.p, sizeof (int), cudaMemcpyDeviceToHost, s));
   LGH_CUDA (cudaStreamSynchronize (s));
   A.max_row_nnz = h[0];
+  if (A.ncols == 0 || A.ncols == A.n) {
+    LGH_TRY (dalloc ((void **) &A.vd, (size_t) A.nnz * sizeof (double) + 16));
+    LGH_TRY (dalloc ((void **) &A.vd32, (size_t) A.nnz * sizeof (float) + 16));
+    k_csr_vd<<<grid, 256, 0, s>>> (A.n, A.rowptr, A.colidx, A.vals, A.dinv,
+                                   A.vd, A.vd32);
+    LGH_LAUNCH_CHECK ();
+    LGH_CUDA (cudaStreamSynchronize (s));
+  }
   return 0;
 }
 
@@ -177,6 +216,8 @@ csr_free (Csr &A)
   dfree (A.vals32);
   dfree (A.dinv);
   dfree (A.dinv32);
+  dfree (A.vd);
+  dfree (A.vd32);
   A = Csr ();
 }
 
@@ -193,6 +234,19 @@ const char *
 lgh_last_error (void)
 {
   return g_err.c_str ();
+}
+
+int
+lgh_runtime_counters (double *out)
+{
+  LGH_CHECK (out, LGH_ERR_ARG_NULL, "lgh_runtime_counters: NULL");
+  std::lock_guard<std::mutex> lk (g_rt_mu);
+  out[0] = (double) g_rt.allocs;
+  out[1] = g_rt.alloc_s;
+  out[2] = (double) g_rt.frees;
+  out[3] = g_rt.free_s;
+  out[4] = (double) __atomic_load_n (&lgh::g_launches, __ATOMIC_RELAXED);
+  return 0;
 }
 
 long
@@ -505,6 +559,50 @@ prior_solve_rows (lgh_prior_t *p, int w, const T *X, int ldx,
   }
 }
 
+/* the same FP64 solve to the prior's tolerance through FP32 sweeps and FP64
+ * iterative refinement (Mat priors; callback priors solve in FP64).  X and
+ * Y must not overlap. */
+int
+prior_solve_refined (lgh_prior_t *p, int w, const double *X, int ldx,
+                     const double *s_in, double *Y, int ldy,
+                     const double *s_out, double inner_rtol, int max_steps)
+{
+  if (w == 0) return 0;
+  if (!p->is_mat)
+    return prior_solve_rows<double> (p, w, X, ldx, s_in, Y, ldy, s_out);
+  ZsolveCfg cfg;
+  prior_zcfg (p, cfg);
+  LGH_TRY (p->ws32.alloc (p->n, std::min (w, 1024), 1));
+  int steps = 0;
+  const int rc = zsolve_refined (p->Z->csr, cfg, p->mg, p->ws32, p->n, w, X, ldx,
+                                 s_in, Y, ldy, s_out, inner_rtol, max_steps,
+                                 &p->stats, &steps, stream ());
+  p->refine_calls++;
+  p->refine_steps += steps;
+  return rc;
+}
+
+int
+resident_ctas (const void *fn, int threads, int smem)
+{
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, int> cache;
+  std::lock_guard<std::mutex> lk (mu);
+  const auto key = std::make_pair (fn, smem * 4096 + threads);
+  auto it = cache.find (key);
+  if (it != cache.end ()) return it->second;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor (&per_sm, fn, threads,
+                                                     (size_t) smem)
+      != cudaSuccess) {
+    cudaGetLastError ();
+    per_sm = 0;
+  }
+  const int r = per_sm > 0 ? per_sm * num_sms () : 0;
+  cache[key] = r;
+  return r;
+}
+
 template int prior_solve_rows<double> (lgh_prior_t *, int, const double *, int,
                                        const double *, double *, int,
                                        const double *, double);
@@ -769,6 +867,8 @@ lgh_prior_get_info (const lgh_prior_t *p, double *out)
   out[9] = p->mg ? (double) p->mg->n0 : 0.;
   out[10] = p->mg ? p->mg->setup_s : 0.;
   out[11] = p->pc_type;
+  out[12] = (double) p->refine_calls;
+  out[13] = (double) p->refine_steps;
   return 0;
 }
 

@@ -99,6 +99,16 @@ k_logdet (int kept, const double *lam, int nshift, const double *c,
   if (threadIdx.x == 0) out[sidx] = red[0];
 }
 
+/* logdet at nshift device-resident shifts into device out[] */
+int
+launch_logdet (int kept, const double *lam, int nshift, const double *c,
+               double *out, cudaStream_t s)
+{
+  k_logdet<<<nshift, 256, 0, s>>> (kept, lam, nshift, c, out);
+  LGH_LAUNCH_CHECK ();
+  return 0;
+}
+
 /* T = (A + A^T)/2 (glr_common_impl.h:490-494) */
 __global__ void
 k_symmetrize (int n, const double *A, double *T)
@@ -597,16 +607,29 @@ check_vecs (lgh_glr_t *g, lgh_Vec a, lgh_Vec b, const char *who)
   return 0;
 }
 
+/* the FP64 Z-solves of the downstream block operations: FP64 sweeps, or
+ * for a mixed-precision object FP32 sweeps refined in FP64 to the prior's
+ * tolerance.  X and Y must not overlap. */
+static int
+glr_zsolve (lgh_glr_t *g, int w, const double *X, int ldx, const double *s_in,
+            double *Y, int ldy, const double *s_out)
+{
+  if (g->exec.precision == LGH_PREC_MIXED)
+    return prior_solve_refined (g->prior, w, X, ldx, s_in, Y, ldy, s_out,
+                                g->exec.inner_rtol, g->exec.max_refine);
+  return prior_solve_rows<double> (g->prior, w, X, ldx, s_in, Y, ldy, s_out);
+}
+
 /* W = Z^{-1} M^{1/2} U, once per build (the shift-independent precompute of
  * the batched operations) */
-static int
+int
 ensure_wz (lgh_glr_t *g)
 {
   if (g->have_wz || g->kept == 0) return 0;
   LGH_TRY (g->Wz.alloc ((size_t) g->n * g->ldu));
   LGH_CUDA (cudaMemsetAsync (g->Wz.p, 0, (size_t) g->n * g->ldu * sizeof (double), stream ()));
-  LGH_TRY (prior_solve_rows<double> (g->prior, g->kept, g->U.p, g->ldu,
-                                     g->prior->msqrt.p, g->Wz.p, g->ldu, nullptr));
+  LGH_TRY (glr_zsolve (g, g->kept, g->U.p, g->ldu, g->prior->msqrt.p, g->Wz.p,
+                       g->ldu, nullptr));
   g->have_wz = 1;
   return 0;
 }
@@ -636,13 +659,14 @@ batch_op (lgh_glr_t *g, int kind, int nshift, const double *c, int m,
   const double *ms = g->prior->msqrt.p;
   if (kind == 0) {
     /* r2 = M^{1/2} Z^{-1} r (into R), y0 = Z^{-1} M^{1/2} r2 */
-    LGH_TRY (prior_solve_rows<double> (g->prior, m, R.p, ldm, nullptr, R.p, ldm, ms));
+    LGH_TRY (glr_zsolve (g, m, R.p, ldm, nullptr, Xs.p, ldm, ms));
+    R.swap (Xs);
   }
   /* sample: r2 = xi */
   if (kept > 0)
     LGH_TRY (launch_gemm_tn<double> (n, kept, m, g->U.p, g->ldu, R.p, ldm, Wc.p,
                                      kept, 0, work.p, work.n, s));
-  LGH_TRY (prior_solve_rows<double> (g->prior, m, R.p, ldm, ms, Y0.p, ldm, nullptr));
+  LGH_TRY (glr_zsolve (g, m, R.p, ldm, ms, Y0.p, ldm, nullptr));
   for (int si = 0; si < nshift; si++) {
     const double cs = ch[si];
     const double fc = (kind == 0) ? 1. / cs : 1. / sqrt (cs);

@@ -33,22 +33,42 @@ k_spmm (int64_t n, const int64_t *__restrict__ rowptr,
   const unsigned gmask = (G == 32) ? 0xffffffffu
                          : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
   /* row tiles of ngroups rows interleaved over the CTAs (L2 locality of
-   * the gathered neighbour rows) */
-  for (int64_t i = (int64_t) blockIdx.x * ngroups + group; i < n;
-       i += (int64_t) gridDim.x * ngroups) {
+   * the gathered neighbour rows); the next row's bounds and first G
+   * (column, value) pairs are loaded during the current row's gathers */
+  const int64_t stride = (int64_t) gridDim.x * ngroups;
+  int64_t i = (int64_t) blockIdx.x * ngroups + group;
+  int64_t k0 = 0, k1 = 0;
+  int mc = 0;
+  T mv = T (0);
+  if (i < n) {
+    k0 = rowptr[i];
+    k1 = rowptr[i + 1];
+    if (lane < k1 - k0) {
+      mc = colidx[k0 + lane];
+      mv = (T) vals[k0 + lane];
+    }
+  }
+  for (; i < n; i += stride) {
+    const int64_t inx = i + stride;
+    int64_t k0n = 0, k1n = 0;
+    if (inx < n) {
+      k0n = rowptr[inx];
+      k1n = rowptr[inx + 1];
+    }
     T acc[CH][W];
 #pragma unroll
     for (int h = 0; h < CH; h++)
 #pragma unroll
       for (int e = 0; e < W; e++) acc[h][e] = T (0);
-    const int64_t k0 = rowptr[i], k1 = rowptr[i + 1];
     for (int64_t kb = k0; kb < k1; kb += G) {
       const int cnt = (int) ((k1 - kb) < G ? (k1 - kb) : G);
-      int mc = 0;
-      T mv = T (0);
-      if (lane < cnt) {
-        mc = colidx[kb + lane];
-        mv = (T) vals[kb + lane];
+      if (kb != k0) {
+        mc = 0;
+        mv = T (0);
+        if (lane < cnt) {
+          mc = colidx[kb + lane];
+          mv = (T) vals[kb + lane];
+        }
       }
       for (int t = 0; t < cnt; t++) {
         const int c = __shfl_sync (gmask, mc, t, G);
@@ -85,6 +105,14 @@ k_spmm (int64_t n, const int64_t *__restrict__ rowptr,
         }
         stp (yr + vi * W, o);
       }
+    }
+    k0 = k0n;
+    k1 = k1n;
+    mc = 0;
+    mv = T (0);
+    if (inx < n && lane < k1n - k0n) {
+      mc = colidx[k0n + lane];
+      mv = (T) vals[k0n + lane];
     }
   }
 }
@@ -174,13 +202,13 @@ spmm_dispatch (const Csr &A, const TV *vals, const T *X, int ldx, T *Y,
 #define LGH_SPMM_CASE(C)                                                     \
   case C:                                                                    \
     if (mode == 0)                                                           \
-      k_spmm<T, TV, C, 0><<<grid, 256, 0, s>>> (A.n, A.rowptr, A.colidx,     \
+      k_spmm<T, TV, C, 0><<<fit_grid (k_spmm<T, TV, C, 0>, grid, 256, 0), 256, 0, s>>> (A.n, A.rowptr, A.colidx,     \
           vals, Xc, ldx, Yc, ldy, nvec, glog, Bc, ldb);                      \
     else if (mode == 1)                                                      \
-      k_spmm<T, TV, C, 1><<<grid, 256, 0, s>>> (A.n, A.rowptr, A.colidx,     \
+      k_spmm<T, TV, C, 1><<<fit_grid (k_spmm<T, TV, C, 1>, grid, 256, 0), 256, 0, s>>> (A.n, A.rowptr, A.colidx,     \
           vals, Xc, ldx, Yc, ldy, nvec, glog, Bc, ldb);                      \
     else                                                                     \
-      k_spmm<T, TV, C, 2><<<grid, 256, 0, s>>> (A.n, A.rowptr, A.colidx,     \
+      k_spmm<T, TV, C, 2><<<fit_grid (k_spmm<T, TV, C, 2>, grid, 256, 0), 256, 0, s>>> (A.n, A.rowptr, A.colidx,     \
           vals, Xc, ldx, Yc, ldy, nvec, glog, Bc, ldb);                      \
     break;
     switch (ch) {

@@ -50,6 +50,14 @@ void clear_error ();
 
 extern long g_launches;
 
+/* host-side runtime counters (lgh_runtime_counters) */
+struct RuntimeCounters
+{
+  long allocs = 0, frees = 0;
+  double alloc_s = 0., free_s = 0.;
+};
+extern RuntimeCounters g_rt;
+
 #define LGH_LAUNCH_CHECK()                                                   \
   do {                                                                       \
     __atomic_fetch_add (&::lgh::g_launches, 1L, __ATOMIC_RELAXED);           \
@@ -129,6 +137,10 @@ struct Csr
   float *vals32 = nullptr;
   double *dinv = nullptr;   /* 1 / diag (Jacobi), filled on demand */
   float *dinv32 = nullptr;
+  double *vd = nullptr;     /* vals[k] / diag[col[k]] (square operators):
+                               the Jacobi-scaled product without a
+                               dependent gather of the diagonal */
+  float *vd32 = nullptr;
   int max_row_nnz = 0;
 };
 
@@ -147,6 +159,21 @@ int launch_rng_state (uint64_t seed, int64_t n, int64_t j0, int k,
 template <typename T>
 int launch_spmm (const Csr &A, const T *X, int ldx, T *Y, int ldy, int w,
                  cudaStream_t s);
+
+/* CTAs of kernel fn (threads per CTA, dynamic shared memory) that are
+ * resident on the device at once (occupancy x SMs; cached per kernel).
+ * Row-group kernels walk interleaved row tiles with a stride loop, so a
+ * grid of exactly this size runs in one wave: the resident CTAs sweep one
+ * band of rows together (stencil neighbours hit in L2) and no tail wave
+ * is left. */
+int resident_ctas (const void *fn, int threads, int smem);
+template <typename K>
+inline int
+fit_grid (K kern, int want, int threads, int smem)
+{
+  const int r = resident_ctas ((const void *) kern, threads, smem);
+  return (r > 0 && r < want) ? r : want;
+}
 
 /* Y += A X (mode 1) or Y = B - A X (mode 2) */
 template <typename T>
@@ -275,6 +302,17 @@ int zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg,
 int zsolve_residual_norms (const Csr &Z, int64_t n, int w, const double *Bm,
                            int ldb, const double *X, int ldx, double *out,
                            cudaStream_t s);
+
+/* Z Y = S X to FP64 accuracy (per-column Jacobi-scaled residual <= rtol of
+ * cfg) by mixed-precision iterative refinement with FP32 inner solves to
+ * inner_rtol; FP64 X, Y (ldy >= round_ld (w)).  steps_out (nullable):
+ * corrections taken. */
+int zsolve_refined (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg,
+                    ZWork &ws32, int64_t n, int w, const double *X, int ldx,
+                    const double *rowscale_in, double *Y, int ldy,
+                    const double *rowscale_out, double inner_rtol,
+                    int max_steps, ZsolveStats *st, int *steps_out,
+                    cudaStream_t s);
 
 /* mode 3: build / destroy the hierarchy from Z (device), CSR on host */
 int mg_build (const Csr &Z, int tile, double smoother_top, int nu,

@@ -39,16 +39,27 @@ struct Hierarchy
 struct KTrace;
 
 /* X = V(B): one block V-cycle from the finest level (X overwritten);
- * tr (nullable) records the fine level's kernels for the timing registry */
+ * tr (nullable) records the fine level's kernels for the timing registry;
+ * work (nullable) gives the level buffers of a caller that runs V-cycles
+ * beside the hierarchy's own users (the request loop), else the
+ * hierarchy's shared buffers are used */
 template <typename T>
 int mg_vcycle (Hierarchy *h, const T *B, T *X, int ld, int w, cudaStream_t s,
-               KTrace *tr = nullptr);
+               KTrace *tr = nullptr, std::vector<MgWork> *work = nullptr);
 
-/* a Chebyshev step on a CSR operator with the Jacobi PC (zsolve.cu) */
+/* a Chebyshev step on a CSR operator with the Jacobi PC (zsolve.cu):
+ * d_new = a d + b D^{-1} r; x += d_new; r_new = r - A d_new.  flags:
+ * CHEB_FIRST (no d yet: a ignored, D not read), CHEB_ZERO_X (x is zero:
+ * X not read, only written), CHEB_STORE_D (write d_new for a next step) */
+enum { CHEB_FIRST = 1, CHEB_ZERO_X = 2, CHEB_STORE_D = 4 };
 template <typename T>
 int launch_cheb_step (const Csr &A, T *X, const T *Ro, T *Rn, const T *Do,
-                      T *Dn, int ld, double a, double b, int first,
+                      T *Dn, int ld, double a, double b, int flags,
                       cudaStream_t s);
+/* the same step's x update alone, for a last step whose r_new is unused */
+template <typename T>
+int launch_cheb_tail (const Csr &A, T *X, const T *R, const T *D, int ld,
+                      double a, double b, int first, cudaStream_t s);
 
 int csr_finish (Csr &A);
 void csr_free (Csr &A);

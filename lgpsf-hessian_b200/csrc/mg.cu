@@ -464,9 +464,10 @@ mg_build (const Csr &Z, int tile, double smoother_top, int nu, Hierarchy **out)
 
 template <typename T>
 static int
-mg_work (Hierarchy *h, int ld, MgWork **w0)
+mg_work (Hierarchy *h, int ld, MgWork **w0, std::vector<MgWork> *own)
 {
-  std::vector<MgWork> &W = std::is_same<T, double>::value ? h->w64 : h->w32;
+  std::vector<MgWork> &W = own ? *own
+                           : (std::is_same<T, double>::value ? h->w64 : h->w32);
   if (W.size () != h->lev.size ()) W.resize (h->lev.size ());
   for (size_t l = 0; l < h->lev.size (); l++) {
     MgWork &w = W[l];
@@ -490,16 +491,23 @@ mg_work (Hierarchy *h, int ld, MgWork **w0)
  * B - A X on entry; nu terms; returns the buffer holding the residual */
 template <typename T>
 static int
-mg_smooth (const MgLevel &lv, T *X, T **Rcur, T **Ralt, T *D0, T *D1, int ld,
-           cudaStream_t s, KTrace *tr)
+mg_smooth (const MgLevel &lv, T *X, const T *B, T *R, T *Ra, T *D0, T *D1,
+           int ld, bool pre, T **Rout, cudaStream_t s, KTrace *tr)
 {
-  /* X, R, D read and written; the first step reads no D */
+  /* pre: nu steps from X = 0 with the residual B (read, never written);
+   * the residual after the last step is returned in *Rout.  post: from X
+   * with the residual in R; the last step only updates X (its residual is
+   * not needed), so it runs without the Z product.  Algorithmic bytes per
+   * step: the operator (gather steps) plus the blocks each step reads and
+   * writes. */
   const double sbase = (double) lv.A.nnz * (sizeof (T) + 4) + 8. * (lv.n + 1);
   const double sblk = (double) lv.n * ld * sizeof (T);
   const double theta = 0.5 * (lv.shi + lv.slo);
   const double delta = 0.5 * (lv.shi - lv.slo);
   const double sigma1 = theta / delta;
   double rho_old = 1.0 / sigma1;
+  const T *Ro = pre ? B : R;
+  T *Rn = pre ? R : Ra;
   T *Do = D0, *Dn = D1;
   for (int k = 1; k <= lv.nu; k++) {
     double a, b;
@@ -510,13 +518,27 @@ mg_smooth (const MgLevel &lv, T *X, T **Rcur, T **Ralt, T *D0, T *D1, int ld,
       b = 2.0 * rho / delta;
       rho_old = rho;
     }
-    if (tr) LGH_TRY (tr->begin (K_MG_SMOOTH, sbase + (k == 1 ? 5. : 6.) * sblk, s));
-    LGH_TRY (launch_cheb_step<T> (lv.A, X, *Rcur, *Ralt, Do, Dn, ld, a, b,
-                                  k == 1, s));
+    const bool last = (k == lv.nu);
+    if (!pre && last) {
+      const double tb = (k == 1 ? 3. : 4.) * sblk + (double) lv.n * sizeof (T);
+      if (tr) LGH_TRY (tr->begin (K_MG_TAIL, tb, s));
+      LGH_TRY (launch_cheb_tail<T> (lv.A, X, Ro, Do, ld, a, b, k == 1, s));
+      if (tr) LGH_TRY (tr->end (s));
+      break;
+    }
+    const bool zx = pre && k == 1;
+    const int flags = (k == 1 ? CHEB_FIRST : 0) | (zx ? CHEB_ZERO_X : 0)
+                      | (last ? 0 : CHEB_STORE_D);
+    const double nblk = 1. + (k == 1 ? 0. : 1.) + (zx ? 0. : 1.)   /* reads */
+                        + 2. + (last ? 0. : 1.);                     /* writes */
+    if (tr) LGH_TRY (tr->begin (K_MG_SMOOTH, sbase + nblk * sblk, s));
+    LGH_TRY (launch_cheb_step<T> (lv.A, X, Ro, Rn, Do, Dn, ld, a, b, flags, s));
     if (tr) LGH_TRY (tr->end (s));
-    std::swap (*Rcur, *Ralt);
+    Ro = Rn;
+    Rn = (Rn == R) ? Ra : R;
     std::swap (Do, Dn);
   }
+  if (Rout) *Rout = (T *) Ro;
   return 0;
 }
 
@@ -541,17 +563,16 @@ vcycle_level (Hierarchy *h, MgWork *W, size_t l, const T *B, T *X, int ld,
   MgWork &wk = W[l];
   T *R = (T *) wk.R0.p, *Ra = (T *) wk.R1.p;
   T *D0 = (T *) wk.D0.p, *D1 = (T *) wk.D1.p;
-  const size_t bytes = (size_t) n * ld * sizeof (T);
-  /* pre-smoothing from X = 0: R = B */
-  LGH_CUDA (cudaMemsetAsync (X, 0, bytes, s));
-  LGH_CUDA (cudaMemcpyAsync (R, B, bytes, cudaMemcpyDeviceToDevice, s));
-  LGH_TRY (mg_smooth<T> (lv, X, &R, &Ra, D0, D1, ld, s, tr));
+  /* pre-smoothing from X = 0 (the first step writes X without reading
+   * it and reads the residual straight from B) */
+  T *Rc = nullptr;
+  LGH_TRY (mg_smooth<T> (lv, X, B, R, Ra, D0, D1, ld, true, &Rc, s, tr));
   /* restriction, coarse correction, prolongation */
   MgWork &wc = W[l + 1];
   T *Bc = (T *) wc.B.p, *Xc = (T *) wc.X.p;
   const double cblk = (double) h->lev[l + 1].n * ld * sizeof (T);
   if (tr) LGH_TRY (tr->begin (K_MG_RESTRICT, blk + cblk + 12. * lv.R.nnz, s));
-  LGH_TRY (launch_spmm<T> (lv.R, R, ld, Bc, ld, ld, s));
+  LGH_TRY (launch_spmm<T> (lv.R, Rc, ld, Bc, ld, ld, s));
   if (tr) LGH_TRY (tr->end (s));
   LGH_TRY (vcycle_level<T> (h, W, l + 1, Bc, Xc, ld, w, s, trace));
   if (tr) LGH_TRY (tr->begin (K_MG_PROLONG, 2. * blk + cblk + 12. * lv.P.nnz, s));
@@ -561,23 +582,25 @@ vcycle_level (Hierarchy *h, MgWork *W, size_t l, const T *B, T *X, int ld,
   if (tr) LGH_TRY (tr->begin (K_MG_RESID, 3. * blk + 12. * lv.A.nnz, s));
   LGH_TRY (launch_spmm_mode<T> (lv.A, X, ld, R, ld, ld, 2, B, ld, s));
   if (tr) LGH_TRY (tr->end (s));
-  LGH_TRY (mg_smooth<T> (lv, X, &R, &Ra, D0, D1, ld, s, tr));
+  LGH_TRY (mg_smooth<T> (lv, X, nullptr, R, Ra, D0, D1, ld, false, nullptr, s,
+                         tr));
   return 0;
 }
 
 template <typename T>
 int
 mg_vcycle (Hierarchy *h, const T *B, T *X, int ld, int w, cudaStream_t s,
-           KTrace *tr)
+           KTrace *tr, std::vector<MgWork> *work)
 {
   MgWork *W;
-  LGH_TRY (mg_work<T> (h, ld, &W));
+  LGH_TRY (mg_work<T> (h, ld, &W, work));
   return vcycle_level<T> (h, W, 0, B, X, ld, w, s, tr);
 }
 
 template int mg_vcycle<double> (Hierarchy *, const double *, double *, int,
-                                int, cudaStream_t, KTrace *);
+                                int, cudaStream_t, KTrace *,
+                                std::vector<MgWork> *);
 template int mg_vcycle<float> (Hierarchy *, const float *, float *, int, int,
-                               cudaStream_t, KTrace *);
+                               cudaStream_t, KTrace *, std::vector<MgWork> *);
 
 } /* namespace lgh */

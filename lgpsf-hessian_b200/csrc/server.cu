@@ -21,6 +21,9 @@
  *   logdet (shift c): sum log(lam + c) - log c, at admission.
  * Admission: a request waits until enough slots are free for all of its
  * columns and the device has room for its staging buffers plus a reserve.
+ * The loop has its own stream, Z-solve workspace and V-cycle level
+ * buffers; it only reads the GLR object (U, lambda, W) and the prior's
+ * operators, so other read-only calls may run beside it.
  */
 
 #include <math.h>
@@ -56,62 +59,101 @@ template <typename T>
 int server_tick_dots (const Csr &Z, const T *R, const T *Zb, int ld, int w,
                       const int *fresh, double rtol, ZWork &ws, cudaStream_t s);
 
-/* column copy between a contiguous device column and a strided column of
- * a row-major block, with an optional row scale */
+int ensure_wz (lgh_glr_t *g);
+int launch_logdet (int kept, const double *lam, int nshift, const double *c,
+                   double *out, cudaStream_t s);
+
+/* a contiguous device column into column `col` of a row-major block, with
+ * an optional row scale; the same column of X and of the next direction
+ * block are cleared (a fresh CG start) */
 __global__ void
-k_col_in (int64_t n, const double *src, const double *scale, double *blk,
-          int ld, int col)
+k_col_place (int64_t n, const double *src, const double *scale, double *R,
+             double *X, double *P, int ld, int col)
 {
   for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t) gridDim.x * blockDim.x)
-    blk[i * ld + col] = scale ? scale[i] * src[i] : src[i];
-}
-
-__global__ void
-k_col_out (int64_t n, const double *blk, int ld, int col, const double *scale,
-           double *dst)
-{
-  for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t) gridDim.x * blockDim.x)
-    dst[i] = scale ? scale[i] * blk[i * ld + col] : blk[i * ld + col];
-}
-
-__global__ void
-k_col_zero (int64_t n, double *blk, int ld, int col)
-{
-  for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t) gridDim.x * blockDim.x)
-    blk[i * ld + col] = 0.;
-}
-
-/* D[k] = (f(lam_k + c) - f(c)) w[k] for one column; kind 0 solve, 1 sample */
-__global__ void
-k_coef_col (int kept, const double *lam, double c, int kind, const double *w,
-            double *d)
-{
-  const double fc = (kind == 0) ? 1. / c : 1. / sqrt (c);
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < kept;
-       k += gridDim.x * blockDim.x) {
-    const double x = lam[k] + c;
-    const double f = (kind == 0) ? 1. / x : 1. / sqrt (x);
-    d[k] = (f - fc) * w[k];
+       i += (int64_t) gridDim.x * blockDim.x) {
+    R[i * ld + col] = scale ? scale[i] * src[i] : src[i];
+    X[i * ld + col] = 0.;
+    P[i * ld + col] = 0.;
   }
 }
 
+/* H[i, t] = colscale[t] * rowscale[i] * X[i, slot[t]] (rowscale nullable) */
 __global__ void
-k_logdet1 (int kept, const double *lam, double c, double *out)
+k_gather_slots (int64_t n, const double *__restrict__ X, int ld,
+                const int *__restrict__ slot, const double *__restrict__ colscale,
+                const double *__restrict__ rowscale, int k, double *H, int ldh)
 {
-  __shared__ double red[256];
-  double s = 0.;
-  const double lc = log (c);
-  for (int i = threadIdx.x; i < kept; i += blockDim.x) s += log (lam[i] + c) - lc;
-  red[threadIdx.x] = s;
-  __syncthreads ();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-    __syncthreads ();
+  const int64_t total = n * k;
+  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t) gridDim.x * blockDim.x) {
+    const int64_t i = e / k;
+    const int t = (int) (e - i * k);
+    double v = colscale[t] * X[i * ld + slot[t]];
+    if (rowscale) v *= rowscale[i];
+    H[i * ldh + t] = v;
   }
-  if (threadIdx.x == 0) *out = red[0];
+}
+
+/* second Z-solve of a solve request, in place: R = mass * X, X = 0, P = 0 */
+__global__ void
+k_restage (int64_t n, double *X, double *R, double *P, int ld,
+           const int *__restrict__ slot, int k, const double *__restrict__ mass)
+{
+  const int64_t total = n * k;
+  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t) gridDim.x * blockDim.x) {
+    const int64_t i = e / k;
+    const int64_t o = i * ld + slot[(int) (e - i * k)];
+    R[o] = mass[i] * X[o];
+    X[o] = 0.;
+    P[o] = 0.;
+  }
+}
+
+/* dst[t][i] = H[i, t] */
+__global__ void
+k_scatter_cols (int64_t n, const double *__restrict__ H, int ldh, int k,
+                double *const *dst)
+{
+  const int64_t total = n * k;
+  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t) gridDim.x * blockDim.x) {
+    const int t = (int) (e / n);
+    const int64_t i = e - (int64_t) t * n;
+    dst[t][i] = H[i * ldh + t];
+  }
+}
+
+/* coefficient columns kept x k: D[:, t] = (f(lam + c_t) - f(c_t)) w_t with
+ * f = 1/x (solve) or x^{-1/2} (sample); the same arithmetic as the batched
+ * operations' shift coefficients */
+__global__ void
+k_coef_cols (int kept, const double *__restrict__ lam, int k,
+             const double *__restrict__ c, const int *__restrict__ kind,
+             const double *const *w, double *D)
+{
+  const int64_t total = (int64_t) kept * k;
+  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t) gridDim.x * blockDim.x) {
+    const int t = (int) (e / kept);
+    const int j = (int) (e - (int64_t) t * kept);
+    const double cs = c[t], x = lam[j] + cs;
+    const double f = kind[t] == 0 ? 1. / x - 1. / cs : 1. / sqrt (x) - 1. / sqrt (cs);
+    D[e] = f * w[t][j];
+  }
+}
+
+/* wdst[t][0..kept) = C[:, t] */
+__global__ void
+k_put_coef (int kept, int k, const double *__restrict__ C, double *const *wdst)
+{
+  const int64_t total = (int64_t) kept * k;
+  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t) gridDim.x * blockDim.x) {
+    const int t = (int) (e / kept);
+    wdst[t][e - (int64_t) t * kept] = C[e];
+  }
 }
 
 static int
@@ -138,7 +180,6 @@ struct SReq
   int cols_left = 0;
   int status = 1;   /* 1 pending/active, 0 done, < 0 error */
   double t_submit = 0., t_done = 0.;
-  std::vector<int> stage;   /* per column */
 };
 
 struct Slot
@@ -146,6 +187,21 @@ struct Slot
   SReq *req = nullptr;
   int col = -1;
   int stage = 0;  /* 1: first Z-solve, 2: second (solve only) */
+};
+
+/* per-tick description of the harvested columns, copied to the device */
+struct Harvest
+{
+  static constexpr int MAXS = 512;
+  int slot_a[MAXS];          /* solve columns leaving stage 1 */
+  int slot_b[MAXS];          /* columns leaving their last stage */
+  int kind_b[MAXS];
+  double one[MAXS];
+  double scale_b[MAXS];      /* 1/c (solve) or c^{-1/2} (sample) */
+  double c_b[MAXS];
+  double *wdst_a[MAXS];      /* request coefficient columns */
+  const double *wsrc_b[MAXS];
+  double *out_b[MAXS];       /* request output columns */
 };
 
 } /* namespace lgh */
@@ -165,13 +221,15 @@ struct lgh_server
   int64_t next_id = 1;
   int err = 0;
   std::string errmsg;
-  /* slot block */
+  /* slot block and per-tick staging */
   lgh::ZWork ws;
-  lgh::DBuf<double> Pold_extra;
+  std::vector<lgh::MgWork> mgw;   /* own V-cycle level buffers */
   std::vector<lgh::Slot> slots;
   lgh::DBuf<int> fresh_d;
   std::vector<int> fresh_h;
-  lgh::DBuf<double> colbuf, coefbuf, gemmwork;
+  lgh::DBuf<double> H, coef, gemmwork, ldc, ldo;
+  lgh::DBuf<char> hv_d;
+  std::unique_ptr<lgh::Harvest> hv;
   /* statistics */
   long completed = 0, ticks = 0, cols_done = 0;
   std::vector<double> lat;
@@ -193,8 +251,8 @@ srv_fail (lgh_server_t *sv, int rc)
   return rc;
 }
 
-/* admit as many pending requests as slots and memory allow (host side) */
-static int
+/* admit pending requests in arrival order while slots and memory allow */
+static void
 srv_admit (lgh_server_t *sv, std::vector<SReq *> &admitted)
 {
   std::lock_guard<std::mutex> lk (sv->mu);
@@ -202,30 +260,180 @@ srv_admit (lgh_server_t *sv, std::vector<SReq *> &admitted)
   for (auto &sl : sv->slots) free_slots += sl.req == nullptr;
   while (!sv->pending.empty ()) {
     SReq *r = sv->pending.front ();
-    if (r->kind != 2 && r->m > free_slots) break;
-    size_t fb = 0, tb = 0;
-    cudaMemGetInfo (&fb, &tb);
-    const double need = (double) sv->g->n * r->m * 16 + (double) sv->g->kept * r->m * 8;
-    if ((double) fb - need < sv->reserve * (double) tb && r->kind != 2) break;
+    if (r->kind != 2) {
+      if (r->m > free_slots) break;
+      size_t fb = 0, tb = 0;
+      if (cudaMemGetInfo (&fb, &tb) == cudaSuccess) {
+        const double need = (double) sv->g->n * r->m * 16.
+                            + (double) std::max (sv->g->kept, 1) * r->m * 8.;
+        if ((double) fb - need < sv->reserve * (double) tb) break;
+      }
+      free_slots -= r->m;
+    }
     sv->pending.pop_front ();
     admitted.push_back (r);
-    if (r->kind != 2) free_slots -= r->m;
   }
+}
+
+static void
+srv_finish (lgh_server_t *sv, SReq *r, int rc)
+{
+  std::lock_guard<std::mutex> lk (sv->mu);
+  r->status = rc ? -rc : 0;
+  r->t_done = wall ();
+  sv->lat.push_back (r->t_done - r->t_submit);
+  sv->completed++;
+  sv->t_last = r->t_done;
+  r->din.release ();
+  r->dout.release ();
+  r->wcoef.release ();
+  sv->done_cv.notify_all ();
+}
+
+/* logdet requests complete at admission with the kernel of lgh_glr_logdet */
+static int
+srv_logdet (lgh_server_t *sv, SReq *r)
+{
+  lgh_glr_t *g = sv->g;
+  double v = 0.;
+  if (g->kept > 0) {
+    LGH_CUDA (cudaMemcpyAsync (sv->ldc.p, &r->c, 8, cudaMemcpyHostToDevice, sv->s));
+    LGH_TRY (launch_logdet (g->kept, g->lam_d.p, 1, sv->ldc.p, sv->ldo.p, sv->s));
+    LGH_CUDA (cudaMemcpyAsync (&v, sv->ldo.p, 8, cudaMemcpyDeviceToHost, sv->s));
+    LGH_CUDA (cudaStreamSynchronize (sv->s));
+  }
+  if (r->hout) *r->hout = v;
+  srv_finish (sv, r, 0);
   return 0;
 }
 
-/* write a column into slot `sl`: R = rhs, X = 0, next-Pold = 0, fresh */
+/* stage a solve / sample request's columns into free slots */
 static int
-srv_place (lgh_server_t *sv, int sl, const double *rhs, const double *scale,
-           double *Pnext)
+srv_start (lgh_server_t *sv, SReq *r, double *Pold)
 {
-  const int64_t n = sv->g->n;
+  lgh_glr_t *g = sv->g;
+  const int64_t n = g->n;
+  const int kept = g->kept;
+  cudaStream_t s = sv->s;
   double *X = (double *) sv->ws.X.p, *R = (double *) sv->ws.R.p;
-  k_col_in<<<cgrid (n), 256, 0, sv->s>>> (n, rhs, scale, R, sv->ld, sl);
-  k_col_zero<<<cgrid (n), 256, 0, sv->s>>> (n, X, sv->ld, sl);
-  k_col_zero<<<cgrid (n), 256, 0, sv->s>>> (n, Pnext, sv->ld, sl);
-  LGH_LAUNCH_CHECK ();
-  sv->fresh_h[sl] = 1;
+  LGH_TRY (r->din.alloc ((size_t) n * r->m));
+  LGH_TRY (r->dout.alloc ((size_t) n * r->m));
+  LGH_TRY (r->wcoef.alloc ((size_t) std::max (kept, 1) * r->m));
+  LGH_CUDA (cudaMemcpy2DAsync (r->din.p, n * 8, r->hin, r->ldin * 8, n * 8, r->m,
+                               cudaMemcpyHostToDevice, s));
+  if (r->kind == 1 && kept > 0) {
+    /* sample: w = U^T xi before any Z-solve */
+    const int ldh = sv->ld;
+    LGH_TRY (launch_colmajor_to_rowmajor (n, r->m, r->din.p, n, sv->H.p, ldh,
+                                          nullptr, s));
+    LGH_TRY (launch_gemm_tn<double> (n, kept, r->m, g->U.p, g->ldu, sv->H.p, ldh,
+                                     r->wcoef.p, kept, 0, sv->gemmwork.p,
+                                     sv->gemmwork.n, s));
+  }
+  r->cols_left = r->m;
+  int j = 0;
+  for (int sl = 0; sl < sv->cap && j < r->m; sl++) {
+    Slot &S = sv->slots[sl];
+    if (S.req) continue;
+    S.req = r;
+    S.col = j;
+    S.stage = 1;
+    /* first right-hand side: r (solve) or M^{1/2} xi (sample) */
+    k_col_place<<<cgrid (n), 256, 0, s>>> (n, r->din.p + (size_t) j * n,
+                                           r->kind == 1 ? g->prior->msqrt.p : nullptr,
+                                           R, X, Pold, sv->ld, sl);
+    LGH_LAUNCH_CHECK ();
+    sv->fresh_h[sl] = 1;
+    j++;
+  }
+  LGH_CHECK (j == r->m, LGH_ERR_ARG_WRONG, "server: admitted without free slots");
+  return 0;
+}
+
+/* columns whose Z-solve converged this tick move on: solve stage 1 ->
+ * U^T coefficients and the second Z-solve; last stage -> the Woodbury
+ * combination, the output column, and request completion */
+static int
+srv_harvest (lgh_server_t *sv, const std::vector<int> &act, double *Pold)
+{
+  lgh_glr_t *g = sv->g;
+  const int64_t n = g->n;
+  const int kept = g->kept, ld = sv->ld, ldh = sv->ld;
+  cudaStream_t s = sv->s;
+  double *X = (double *) sv->ws.X.p, *R = (double *) sv->ws.R.p;
+  Harvest &h = *sv->hv;
+  int ka = 0, kb = 0;
+  std::vector<SReq *> fin;
+  for (int sl = 0; sl < sv->cap; sl++) {
+    Slot &S = sv->slots[sl];
+    if (!S.req || act[sl] || sv->fresh_h[sl]) continue;
+    SReq *r = S.req;
+    if (r->kind == 0 && S.stage == 1) {
+      h.slot_a[ka] = sl;
+      h.one[ka] = 1.;
+      h.wdst_a[ka] = r->wcoef.p + (size_t) S.col * std::max (kept, 1);
+      ka++;
+      S.stage = 2;
+      sv->fresh_h[sl] = 1;
+    } else {
+      h.slot_b[kb] = sl;
+      h.kind_b[kb] = r->kind;
+      h.c_b[kb] = r->c;
+      h.scale_b[kb] = r->kind == 0 ? 1. / r->c : 1. / sqrt (r->c);
+      h.wsrc_b[kb] = r->wcoef.p + (size_t) S.col * std::max (kept, 1);
+      h.out_b[kb] = r->dout.p + (size_t) S.col * n;
+      kb++;
+      S.req = nullptr;
+      S.col = -1;
+      S.stage = 0;
+      if (--r->cols_left == 0) fin.push_back (r);
+    }
+  }
+  if (ka == 0 && kb == 0) return 0;
+  Harvest *hd = (Harvest *) sv->hv_d.p;
+  LGH_CUDA (cudaMemcpyAsync (hd, &h, sizeof (Harvest), cudaMemcpyHostToDevice, s));
+  if (ka > 0) {
+    /* r2 = M^{1/2} y1 -> w = U^T r2; then the second right-hand side M y1 */
+    if (kept > 0) {
+      k_gather_slots<<<cgrid (n * ka), 256, 0, s>>> (n, X, ld, hd->slot_a, hd->one,
+                                                     g->prior->msqrt.p, ka, sv->H.p, ldh);
+      LGH_LAUNCH_CHECK ();
+      LGH_TRY (launch_gemm_tn<double> (n, kept, ka, g->U.p, g->ldu, sv->H.p, ldh,
+                                       sv->coef.p, kept, 0, sv->gemmwork.p,
+                                       sv->gemmwork.n, s));
+      k_put_coef<<<cgrid ((int64_t) kept * ka), 256, 0, s>>> (kept, ka, sv->coef.p,
+                                                              hd->wdst_a);
+      LGH_LAUNCH_CHECK ();
+    }
+    k_restage<<<cgrid (n * ka), 256, 0, s>>> (n, X, R, Pold, ld, hd->slot_a, ka,
+                                              g->prior->mass.p);
+    LGH_LAUNCH_CHECK ();
+  }
+  if (kb > 0) {
+    /* x = a y0 + W diag(f(lam + c) - f(c)) w */
+    k_gather_slots<<<cgrid (n * kb), 256, 0, s>>> (n, X, ld, hd->slot_b, hd->scale_b,
+                                                   nullptr, kb, sv->H.p, ldh);
+    LGH_LAUNCH_CHECK ();
+    if (kept > 0) {
+      k_coef_cols<<<cgrid ((int64_t) kept * kb), 256, 0, s>>> (kept, g->lam_d.p, kb,
+                                                               hd->c_b, hd->kind_b,
+                                                               hd->wsrc_b, sv->coef.p);
+      LGH_LAUNCH_CHECK ();
+      LGH_TRY (launch_gemm_nn<double> (n, kept, kb, 1.0, g->Wz.p, g->ldu, sv->coef.p,
+                                       kept, 1.0, sv->H.p, ldh, sv->H.p, ldh, s));
+    }
+    k_scatter_cols<<<cgrid (n * kb), 256, 0, s>>> (n, sv->H.p, ldh, kb, hd->out_b);
+    LGH_LAUNCH_CHECK ();
+    sv->cols_done += kb;
+  }
+  for (SReq *r : fin) {
+    LGH_CUDA (cudaMemcpy2DAsync (r->hout, r->ldout * 8, r->dout.p, n * 8, n * 8, r->m,
+                                 cudaMemcpyDeviceToHost, s));
+  }
+  if (!fin.empty ()) {
+    LGH_CUDA (cudaStreamSynchronize (s));
+    for (SReq *r : fin) srv_finish (sv, r, 0);
+  }
   return 0;
 }
 
@@ -241,69 +449,24 @@ srv_loop (lgh_server_t *sv)
   double *P0 = (double *) sv->ws.P0.p, *P1 = (double *) sv->ws.P1.p;
   double *Q = (double *) sv->ws.Q.p, *Zb = (double *) sv->ws.Zb.p;
   double *Pold = P0, *Pnew = P1;
-  const double *ms = p->msqrt.p, *mass = p->mass.p;
-  const int kept = g->kept;
   int rc = 0;
-  cudaMemsetAsync (P0, 0, (size_t) n * ld * 8, s);
-  cudaMemsetAsync (P1, 0, (size_t) n * ld * 8, s);
-  cudaMemsetAsync (R, 0, (size_t) n * ld * 8, s);
-  cudaMemsetAsync (X, 0, (size_t) n * ld * 8, s);
-  cudaMemsetAsync (sv->ws.ival.p, 0, sv->ws.ival.n * sizeof (int), s);
-  cudaStreamSynchronize (s);
+  const size_t blk = (size_t) n * ld * sizeof (double);
+  if (cudaMemsetAsync (P0, 0, blk, s) != cudaSuccess
+      || cudaMemsetAsync (P1, 0, blk, s) != cudaSuccess
+      || cudaMemsetAsync (R, 0, blk, s) != cudaSuccess
+      || cudaMemsetAsync (X, 0, blk, s) != cudaSuccess
+      || cudaMemsetAsync (sv->ws.ival.p, 0, sv->ws.ival.n * sizeof (int), s) != cudaSuccess
+      || cudaStreamSynchronize (s) != cudaSuccess) {
+    srv_fail (sv, set_error (LGH_ERR_GPU, "server: workspace clear"));
+    return;
+  }
+  std::vector<int> act (sv->cap);
   while (!sv->stop.load ()) {
-    /* 1. admission of new requests into free slots */
+    /* 1. admission into free slots */
     std::vector<SReq *> adm;
     srv_admit (sv, adm);
     for (SReq *r : adm) {
-      if (r->kind == 2) {
-        /* logdet at admission */
-        DBuf<double> cd;
-        double *dv = nullptr;
-        rc = cd.alloc (1);
-        if (!rc && kept > 0) {
-          dv = cd.p;
-          k_logdet1<<<1, 256, 0, s>>> (kept, g->lam_d.p, r->c, dv);
-        }
-        double hv = 0.;
-        if (!rc && kept > 0 && cudaMemcpyAsync (&hv, dv, 8, cudaMemcpyDeviceToHost, s) != cudaSuccess)
-          rc = set_error (LGH_ERR_GPU, "server: logdet copy");
-        if (!rc) cudaStreamSynchronize (s);
-        std::lock_guard<std::mutex> lk (sv->mu);
-        if (r->hout) *r->hout = hv;
-        r->status = rc ? -rc : 0;
-        r->t_done = wall ();
-        sv->lat.push_back (r->t_done - r->t_submit);
-        sv->completed++;
-        sv->done_cv.notify_all ();
-        continue;
-      }
-      /* stage the input columns and (sample) the U^T coefficients */
-      rc = r->din.alloc ((size_t) n * r->m);
-      if (!rc) rc = r->dout.alloc ((size_t) n * r->m);
-      if (!rc) rc = r->wcoef.alloc ((size_t) std::max (kept, 1) * r->m);
-      if (!rc) {
-        for (int j = 0; j < r->m; j++)
-          if (cudaMemcpyAsync (r->din.p + (size_t) j * n, r->hin + (size_t) j * r->ldin,
-                               n * 8, cudaMemcpyHostToDevice, s) != cudaSuccess)
-            rc = set_error (LGH_ERR_GPU, "server: input copy");
-      }
-      if (!rc && r->kind == 1 && kept > 0)
-        rc = launch_gemm_tn<double> (n, kept, r->m, g->U.p, g->ldu, r->din.p, 1,
-                                     r->wcoef.p, kept, 0, sv->gemmwork.p,
-                                     sv->gemmwork.n, s);
-      r->stage.assign (r->m, 1);
-      r->cols_left = r->m;
-      int j = 0;
-      for (int sl = 0; sl < sv->cap && j < r->m && !rc; sl++) {
-        if (sv->slots[sl].req) continue;
-        sv->slots[sl].req = r;
-        sv->slots[sl].col = j;
-        sv->slots[sl].stage = 1;
-        /* solve: stage-1 rhs r; sample: M^{1/2} xi */
-        rc = srv_place (sv, sl, r->din.p + (size_t) j * n,
-                        r->kind == 1 ? ms : nullptr, Pold);
-        j++;
-      }
+      rc = (r->kind == 2) ? srv_logdet (sv, r) : srv_start (sv, r, Pold);
       if (rc) break;
     }
     if (rc) { srv_fail (sv, rc); return; }
@@ -315,91 +478,30 @@ srv_loop (lgh_server_t *sv)
                        [&] { return sv->stop.load () || !sv->pending.empty (); });
       continue;
     }
-    /* 2. one tick: Z = PC(R) for fresh columns happens inside the tick order
-     *    pq -> upd -> PC -> dots; fresh columns were placed before PC */
-    rc = cudaMemcpyAsync (sv->fresh_d.p, sv->fresh_h.data (), sv->cap * sizeof (int),
-                          cudaMemcpyHostToDevice, s) == cudaSuccess ? 0
-         : set_error (LGH_ERR_GPU, "server: fresh flags");
+    /* 2. one PCG tick over the whole slot block: preconditioner, dots
+     *    (fresh columns start there), direction + Z product, update */
+    if (cudaMemcpyAsync (sv->fresh_d.p, sv->fresh_h.data (), sv->cap * sizeof (int),
+                         cudaMemcpyHostToDevice, s) != cudaSuccess)
+      rc = set_error (LGH_ERR_GPU, "server: fresh flags");
     if (!rc) {
-      if (p->mg) rc = mg_vcycle<double> (p->mg, R, Zb, ld, sv->cap, s);
+      if (p->mg) rc = mg_vcycle<double> (p->mg, R, Zb, ld, sv->cap, s, nullptr,
+                                         &sv->mgw);
       else rc = launch_rowscale<double> (n, ld, p->Z->csr.dinv, R, ld, Zb, ld, s);
     }
     if (!rc) rc = server_tick_dots<double> (p->Z->csr, R, Zb, ld, sv->cap,
                                             sv->fresh_d.p, p->zcfg.rtol, sv->ws, s);
-    std::fill (sv->fresh_h.begin (), sv->fresh_h.end (), 0);
     if (!rc) rc = server_tick_pq<double> (p->Z->csr, Zb, Pold, Pnew, Q, ld, sv->ws, s);
     if (!rc) rc = server_tick_upd<double> (n, ld, X, R, Pnew, Q, sv->ws, s);
     std::swap (Pold, Pnew);
+    std::fill (sv->fresh_h.begin (), sv->fresh_h.end (), 0);
     sv->ticks++;
     /* 3. harvest converged columns */
-    std::vector<int> act (sv->cap);
     if (!rc && cudaMemcpyAsync (act.data (), sv->ws.ival.p, sv->cap * sizeof (int),
                                 cudaMemcpyDeviceToHost, s) != cudaSuccess)
       rc = set_error (LGH_ERR_GPU, "server: mask copy");
     if (!rc && cudaStreamSynchronize (s) != cudaSuccess)
       rc = set_error (LGH_ERR_GPU, "server: tick");
-    if (rc) { srv_fail (sv, rc); return; }
-    for (int sl = 0; sl < sv->cap && !rc; sl++) {
-      Slot &S = sv->slots[sl];
-      if (!S.req || act[sl] || sv->fresh_h[sl]) continue;
-      SReq *r = S.req;
-      const int j = S.col;
-      double *ycol = r->dout.p + (size_t) j * n;
-      if (r->kind == 0 && S.stage == 1) {
-        /* y1 -> r2 = M^{1/2} y1 (kept in dout), w = U^T r2, stage-2 rhs M y1 */
-        k_col_out<<<cgrid (n), 256, 0, s>>> (n, X, ld, sl, ms, ycol);
-        if (kept > 0)
-          rc = launch_gemm_tn<double> (n, kept, 1, g->U.p, g->ldu, ycol, 1,
-                                       r->wcoef.p + (size_t) j * kept, kept, 0,
-                                       sv->gemmwork.p, sv->gemmwork.n, s);
-        if (!rc) {
-          /* the stage-2 right-hand side M^{1/2} r2 */
-          k_col_out<<<cgrid (n), 256, 0, s>>> (n, X, ld, sl, mass, sv->colbuf.p);
-          rc = srv_place (sv, sl, sv->colbuf.p, nullptr, Pold);
-          S.stage = 2;
-        }
-        continue;
-      }
-      /* final stage: y0 in X; x = a y0 + W diag(f - f_c) w */
-      const double a = (r->kind == 0) ? 1. / r->c : 1. / sqrt (r->c);
-      k_col_out<<<cgrid (n), 256, 0, s>>> (n, X, ld, sl, nullptr, sv->colbuf.p);
-      if (kept > 0) {
-        k_coef_col<<<1, 256, 0, s>>> (kept, g->lam_d.p, r->c, r->kind,
-                                      r->wcoef.p + (size_t) j * kept, sv->coefbuf.p);
-        rc = launch_gemm_nn<double> (n, kept, 1, 1.0, g->Wz.p, g->ldu,
-                                     sv->coefbuf.p, kept, a, sv->colbuf.p, 1,
-                                     ycol, 1, s);
-      } else {
-        rc = launch_vec_scale (n, sv->colbuf.p, nullptr, a, ycol, s);
-      }
-      if (rc) break;
-      if (cudaMemcpyAsync (r->hout + (size_t) j * r->ldout, ycol, n * 8,
-                           cudaMemcpyDeviceToHost, s) != cudaSuccess) {
-        rc = set_error (LGH_ERR_GPU, "server: output copy");
-        break;
-      }
-      S.req = nullptr;
-      S.col = -1;
-      S.stage = 0;
-      r->cols_left--;
-      sv->cols_done++;
-      if (r->cols_left == 0) {
-        if (cudaStreamSynchronize (s) != cudaSuccess) {
-          rc = set_error (LGH_ERR_GPU, "server: completion");
-          break;
-        }
-        std::lock_guard<std::mutex> lk (sv->mu);
-        r->status = 0;
-        r->t_done = wall ();
-        sv->lat.push_back (r->t_done - r->t_submit);
-        sv->completed++;
-        sv->t_last = r->t_done;
-        r->din.release ();
-        r->dout.release ();
-        r->wcoef.release ();
-        sv->done_cv.notify_all ();
-      }
-    }
+    if (!rc) rc = srv_harvest (sv, act, Pold);
     if (rc) { srv_fail (sv, rc); return; }
   }
 }
@@ -429,7 +531,7 @@ lgh_server_create (lgh_glr_t *glr, const lgh_server_opts_t *opts,
   LGH_CHECK (glr->prior->is_mat, LGH_ERR_SUP,
              "lgh_server_create: needs a Mat-path prior (device Z-solves)");
   lgh_server_opts_t o = opts ? *opts : lgh_server_opts_default ();
-  LGH_CHECK (o.slots >= 1 && o.slots <= 512, LGH_ERR_ARG_OUTOFRANGE,
+  LGH_CHECK (o.slots >= 1 && o.slots <= Harvest::MAXS, LGH_ERR_ARG_OUTOFRANGE,
              "lgh_server_create: slots %d", o.slots);
   lgh_server_t *sv = new lgh_server_t ();
   sv->g = glr;
@@ -440,25 +542,25 @@ lgh_server_create (lgh_glr_t *glr, const lgh_server_opts_t *opts,
   if (cudaStreamCreateWithFlags (&sv->s, cudaStreamNonBlocking) != cudaSuccess)
     rc = set_error (LGH_ERR_GPU, "lgh_server_create: stream");
   /* the shift-independent precompute W = Z^{-1} M^{1/2} U */
-  if (!rc && glr->kept > 0 && !glr->have_wz) {
-    rc = glr->Wz.alloc ((size_t) glr->n * glr->ldu);
-    if (!rc) cudaMemset (glr->Wz.p, 0, (size_t) glr->n * glr->ldu * 8);
-    if (!rc) rc = prior_solve_rows<double> (glr->prior, glr->kept, glr->U.p,
-                                            glr->ldu, glr->prior->msqrt.p,
-                                            glr->Wz.p, glr->ldu, nullptr);
-    if (!rc) glr->have_wz = 1;
-  }
+  if (!rc) rc = ensure_wz (glr);
+  const int kp = std::max (glr->kept, 1);
   if (!rc) rc = sv->ws.alloc (glr->n, sv->ld, 0);
   if (!rc) rc = sv->fresh_d.alloc (sv->ld);
-  if (!rc) rc = sv->colbuf.alloc (glr->n);
-  if (!rc) rc = sv->coefbuf.alloc (std::max (glr->kept, 1));
+  if (!rc) rc = sv->H.alloc ((size_t) glr->n * sv->ld);
+  if (!rc) rc = sv->coef.alloc ((size_t) kp * sv->cap);
   if (!rc) rc = sv->gemmwork.alloc (std::max<size_t> (
-             gemm_tn_work_elems (glr->n, std::max (glr->kept, 1), sv->cap), 64));
+             gemm_tn_work_elems (glr->n, kp, sv->cap), 64));
+  if (!rc) rc = sv->ldc.alloc (1);
+  if (!rc) rc = sv->ldo.alloc (1);
+  if (!rc) rc = sv->hv_d.alloc (sizeof (Harvest));
+  if (!rc) rc = cudaDeviceSynchronize () == cudaSuccess ? 0
+                : set_error (LGH_ERR_GPU, "lgh_server_create: set-up");
   if (rc) {
     if (sv->s) cudaStreamDestroy (sv->s);
     delete sv;
     return rc;
   }
+  sv->hv.reset (new Harvest ());
   sv->slots.assign (sv->cap, Slot ());
   sv->fresh_h.assign (sv->ld, 0);
   sv->t0 = wall ();

@@ -314,34 +314,69 @@ k_pcg_upd (ZK z, const T *__restrict__ dinv, T *__restrict__ X,
  *      x += d_new, r_new = r - Z d_new (zsolve_impl.h:108-141) ----------- */
 template <typename T, int CH>
 __global__ void __launch_bounds__ (ZS_THREADS, (CH * (16 / sizeof (T)) <= 8 ? 3 : 2))
-k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ dinv,
-        T *__restrict__ X,
+k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ vdv,
+        const T *__restrict__ dinv, T *__restrict__ X,
         const T *__restrict__ Rold, T *__restrict__ Rnew,
         const T *__restrict__ Dold, T *__restrict__ Dnew, int ld, int nvec,
-        int glog, T a, T b, int first)
+        int glog, T a, T b, int flags)
 {
+  /* r_new = r - Z d_new with d_new = a d + b D^{-1} r formed at each
+   * neighbour: sum_j (b vd_ij r_j + a v_ij d_j), vd_ij = v_ij / z_jj.
+   * Software pipeline over the group's rows: the next row's bounds and
+   * its first G (column, value, value/diagonal) triples are loaded while
+   * the current row's neighbour rows are gathered, so the only latency on
+   * a row's critical path is the gathers' own; the row's x is loaded
+   * ahead of the gathers. */
   ZS_GROUP_SETUP ();
-  for (int64_t i = (int64_t) blockIdx.x * ngroups + group; i < z.n;
-       i += (int64_t) gridDim.x * ngroups) {
+  const bool first = flags & CHEB_FIRST, zx = flags & CHEB_ZERO_X;
+  const bool wd = flags & CHEB_STORE_D;
+  const int64_t stride = (int64_t) gridDim.x * ngroups;
+  int64_t i = (int64_t) blockIdx.x * ngroups + group;
+  int64_t k0 = 0, k1 = 0;
+  int mc = 0;
+  T mv = T (0), mw = T (0);
+  if (i < z.n) {
+    k0 = z.rowptr[i];
+    k1 = z.rowptr[i + 1];
+    if (lane < k1 - k0) {
+      mc = z.col[k0 + lane];
+      mv = vals[k0 + lane];
+      mw = vdv[k0 + lane];
+    }
+  }
+  for (; i < z.n; i += stride) {
+    const int64_t inx = i + stride;
+    int64_t k0n = 0, k1n = 0;
+    if (inx < z.n) {
+      k0n = z.rowptr[inx];
+      k1n = z.rowptr[inx + 1];
+    }
+    Pack<T> xs[CH];
+#pragma unroll
+    for (int h = 0; h < CH; h++) {
+      const int vi = lane + h * G;
+      xs[h] = (zx || vi >= nvec) ? pzero<T> () : ldp (X + i * ld + vi * W);
+    }
     T acc[CH][W];
 #pragma unroll
     for (int h = 0; h < CH; h++)
 #pragma unroll
       for (int e = 0; e < W; e++) acc[h][e] = T (0);
-    const int64_t k0 = z.rowptr[i], k1 = z.rowptr[i + 1];
     for (int64_t kb = k0; kb < k1; kb += G) {
       const int cnt = (int) ((k1 - kb) < G ? (k1 - kb) : G);
-      int mc = 0;
-      T mv = T (0), md = T (0);
-      if (lane < cnt) {
-        mc = z.col[kb + lane];
-        mv = vals[kb + lane];
-        md = dinv[mc];
+      if (kb != k0) {   /* rows longer than G: later chunks load inline */
+        mc = 0;
+        mv = mw = T (0);
+        if (lane < cnt) {
+          mc = z.col[kb + lane];
+          mv = vals[kb + lane];
+          mw = vdv[kb + lane];
+        }
       }
       for (int t = 0; t < cnt; t++) {
         const int c = __shfl_sync (gmask, mc, t, G);
-        const T v = __shfl_sync (gmask, mv, t, G);
-        const T bdj = b * __shfl_sync (gmask, md, t, G);
+        const T av = a * __shfl_sync (gmask, mv, t, G);
+        const T bw = b * __shfl_sync (gmask, mw, t, G);
 #pragma unroll
         for (int h = 0; h < CH; h++) {
           const int vi = lane + h * G;
@@ -350,10 +385,18 @@ k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ dinv,
             Pack<T> dj = first ? pzero<T> () : ldp (Dold + (int64_t) c * ld + vi * W);
 #pragma unroll
             for (int e = 0; e < W; e++)
-              acc[h][e] = fma (v, fma (bdj, rj.v[e], a * dj.v[e]), acc[h][e]);
+              acc[h][e] = fma (bw, rj.v[e], fma (av, dj.v[e], acc[h][e]));
           }
         }
       }
+    }
+    /* the next row's first chunk, behind this row's gathers */
+    int mcn = 0;
+    T mvn = T (0), mwn = T (0);
+    if (inx < z.n && lane < k1n - k0n) {
+      mcn = z.col[k0n + lane];
+      mvn = vals[k0n + lane];
+      mwn = vdv[k0n + lane];
     }
     const T bdi = b * dinv[i];
 #pragma unroll
@@ -361,9 +404,9 @@ k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ dinv,
       const int vi = lane + h * G;
       if (vi < nvec) {
         const int64_t o = i * ld + vi * W;
-        Pack<T> ri = ldp (Rold + o), x = ldp (X + o);
+        Pack<T> ri = ldp (Rold + o);
         Pack<T> di = first ? pzero<T> () : ldp (Dold + o);
-        Pack<T> dn, rn;
+        Pack<T> dn, rn, x = xs[h];
 #pragma unroll
         for (int e = 0; e < W; e++) {
           dn.v[e] = fma (bdi, ri.v[e], a * di.v[e]);
@@ -371,10 +414,15 @@ k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ dinv,
           rn.v[e] = ri.v[e] - acc[h][e];
         }
         stp (X + o, x);
-        stp (Dnew + o, dn);
+        if (wd) stp (Dnew + o, dn);
         stp (Rnew + o, rn);
       }
     }
+    k0 = k0n;
+    k1 = k1n;
+    mc = mcn;
+    mv = mvn;
+    mw = mwn;
   }
 }
 
@@ -387,6 +435,8 @@ k_pcgx_pq (ZK z, const T *__restrict__ vals, const T *__restrict__ Zb,
            T *__restrict__ Qv, int ld, int nvec, int glog, int first,
            double *partA, unsigned *counter, double *scal, int *ival, int cap)
 {
+  /* the next row's bounds and first G (column, value) pairs are loaded
+   * while the current row's neighbours are gathered (software pipeline) */
   extern __shared__ double red[];
   ZS_GROUP_SETUP ();
   const double *beta = scal + S_BETA * cap;
@@ -403,21 +453,40 @@ k_pcgx_pq (ZK z, const T *__restrict__ vals, const T *__restrict__ Zb,
   for (int h = 0; h < CH; h++)
 #pragma unroll
     for (int e = 0; e < W; e++) aPQ[h][e] = 0.;
-  for (int64_t i = (int64_t) blockIdx.x * ngroups + group; i < z.n;
-       i += (int64_t) gridDim.x * ngroups) {
+  const int64_t stride = (int64_t) gridDim.x * ngroups;
+  int64_t i = (int64_t) blockIdx.x * ngroups + group;
+  int64_t k0 = 0, k1 = 0;
+  int mc = 0;
+  T mv = T (0);
+  if (i < z.n) {
+    k0 = z.rowptr[i];
+    k1 = z.rowptr[i + 1];
+    if (lane < k1 - k0) {
+      mc = z.col[k0 + lane];
+      mv = vals[k0 + lane];
+    }
+  }
+  for (; i < z.n; i += stride) {
+    const int64_t inx = i + stride;
+    int64_t k0n = 0, k1n = 0;
+    if (inx < z.n) {
+      k0n = z.rowptr[inx];
+      k1n = z.rowptr[inx + 1];
+    }
     T acc[CH][W];
 #pragma unroll
     for (int h = 0; h < CH; h++)
 #pragma unroll
       for (int e = 0; e < W; e++) acc[h][e] = T (0);
-    const int64_t k0 = z.rowptr[i], k1 = z.rowptr[i + 1];
     for (int64_t kb = k0; kb < k1; kb += G) {
       const int cnt = (int) ((k1 - kb) < G ? (k1 - kb) : G);
-      int mc = 0;
-      T mv = T (0);
-      if (lane < cnt) {
-        mc = z.col[kb + lane];
-        mv = vals[kb + lane];
+      if (kb != k0) {
+        mc = 0;
+        mv = T (0);
+        if (lane < cnt) {
+          mc = z.col[kb + lane];
+          mv = vals[kb + lane];
+        }
       }
       for (int t = 0; t < cnt; t++) {
         const int c = __shfl_sync (gmask, mc, t, G);
@@ -434,6 +503,12 @@ k_pcgx_pq (ZK z, const T *__restrict__ vals, const T *__restrict__ Zb,
           }
         }
       }
+    }
+    int mcn = 0;
+    T mvn = T (0);
+    if (inx < z.n && lane < k1n - k0n) {
+      mcn = z.col[k0n + lane];
+      mvn = vals[k0n + lane];
     }
 #pragma unroll
     for (int h = 0; h < CH; h++) {
@@ -452,6 +527,10 @@ k_pcgx_pq (ZK z, const T *__restrict__ vals, const T *__restrict__ Zb,
         stp (Qv + i * ld + vi * W, q);
       }
     }
+    k0 = k0n;
+    k1 = k1n;
+    mc = mcn;
+    mv = mvn;
   }
   block_colsum_store<T, CH> (aPQ, lane, group, G, nvec, ld, red, partA);
   const double *rz = scal + S_RZ * cap;
@@ -745,7 +824,7 @@ ZWork::alloc (int64_t n_, int cap_, int is32_)
   LGH_TRY (P1.alloc (blk));
   LGH_TRY (Q.alloc (blk));
   LGH_TRY (Zb.alloc (blk));
-  nblocks = num_sms () * 4;
+  nblocks = num_sms () * 8;
   LGH_TRY (partA.alloc ((size_t) cap * nblocks));
   LGH_TRY (partB.alloc ((size_t) cap * nblocks));
   LGH_TRY (scal.alloc ((size_t) cap * S_NSLOT));
@@ -771,6 +850,14 @@ zdinv (const Csr &Z)
 {
   if constexpr (std::is_same<T, double>::value) return Z.dinv;
   else return Z.dinv32;
+}
+
+template <typename T>
+static const T *
+zvd (const Csr &Z)
+{
+  if constexpr (std::is_same<T, double>::value) return Z.vd;
+  else return Z.vd32;
 }
 
 #define ZS_DISPATCH(CHV, ...)                                                \
@@ -836,7 +923,7 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
     ZS_DISPATCH (ch, {
       auto kf = k_pcg_init<T, CH_>;
       set_smem_attr (kf, smem);
-      kf<<<grid, ZS_THREADS, smem, s>>> (zk, dinv, Xin + c0, ldx, rs_in, bX,
+      kf<<<fit_grid (kf, grid, ZS_THREADS, smem), ZS_THREADS, smem, s>>> (zk, dinv, Xin + c0, ldx, rs_in, bX,
                                          bR, bP0, ldt, nvec, glog, wt,
                                          ws.partA.p, ws.partB.p,
                                          ws.counters.p, ws.scal.p, ws.ival.p,
@@ -858,7 +945,7 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
       ZS_DISPATCH (ch, {
         auto kd = k_pcgx_dots<T, CH_>;
         set_smem_attr (kd, smem);
-        kd<<<grid, ZS_THREADS, smem, s>>> (zk, bR, bZ, ldt, nvec, glog, wt, 1,
+        kd<<<fit_grid (kd, grid, ZS_THREADS, smem), ZS_THREADS, smem, s>>> (zk, bR, bZ, ldt, nvec, glog, wt, 1,
                                            ws.partA.p, ws.partB.p,
                                            ws.counters.p + 1, ws.scal.p,
                                            ws.ival.p, cap, cfg.rtol, 0, nullptr, nullptr);
@@ -871,7 +958,7 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
         ZS_DISPATCH (ch, {
           auto k1 = k_pcgx_pq<T, CH_>;
           set_smem_attr (k1, smem);
-          k1<<<grid, ZS_THREADS, smem, s>>> (zk, vals, bZ, Pold, Pnew, bQ, ldt,
+          k1<<<fit_grid (k1, grid, ZS_THREADS, smem), ZS_THREADS, smem, s>>> (zk, vals, bZ, Pold, Pnew, bQ, ldt,
                                              nvec, glog, it == 0, ws.partA.p,
                                              ws.counters.p, ws.scal.p,
                                              ws.ival.p, cap);
@@ -887,7 +974,7 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
         if (tr) LGH_TRY (tr->begin (K_PCGX_DOTS, 2. * bw, s));
         ZS_DISPATCH (ch, {
           auto kd = k_pcgx_dots<T, CH_>;
-          kd<<<grid, ZS_THREADS, smem, s>>> (zk, bR, bZ, ldt, nvec, glog, wt, 0,
+          kd<<<fit_grid (kd, grid, ZS_THREADS, smem), ZS_THREADS, smem, s>>> (zk, bR, bZ, ldt, nvec, glog, wt, 0,
                                              ws.partA.p, ws.partB.p,
                                              ws.counters.p + 1, ws.scal.p,
                                              ws.ival.p, cap, cfg.rtol, it,
@@ -944,9 +1031,12 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
         LGH_TRY (mg_vcycle<T> (mg, Ro, bZ, ldt, wt, s, tc));
         if (tc) LGH_TRY (tc->begin (K_CHEBX, zbytes + 7. * (double) n * wt * sizeof (T), s));
         ZS_DISPATCH (ch, {
-          k_chebx<T, CH_><<<grid, ZS_THREADS, 0, s>>> (zk, vals, bZ, bX, Ro, Rn,
+          k_chebx<T, CH_><<<fit_grid (k_chebx<T, CH_>, grid, ZS_THREADS, 0),
+                                           ZS_THREADS, 0, s>>> (zk, vals, bZ, bX, Ro, Rn,
                                                        Do, Dn, ldt, nvec, glog,
-                                                       (T) a, (T) b, k == 1);
+                                                       (T) a, (T) b,
+                                                      (k == 1 ? CHEB_FIRST : 0)
+                                                      | CHEB_STORE_D);
         });
         LGH_LAUNCH_CHECK ();
         if (tc) {
@@ -972,7 +1062,7 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
         ZS_DISPATCH (ch, {
           auto k1 = k_pcg_pq<T, CH_>;
           set_smem_attr (k1, smem);
-          k1<<<grid, ZS_THREADS, smem, s>>> (zk, vals, dinv, bR, Pold, Pnew,
+          k1<<<fit_grid (k1, grid, ZS_THREADS, smem), ZS_THREADS, smem, s>>> (zk, vals, dinv, bR, Pold, Pnew,
                                              bQ, ldt, nvec, glog, it == 0,
                                              ws.partA.p, ws.counters.p,
                                              ws.scal.p, ws.ival.p, cap);
@@ -983,7 +1073,7 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
           }
           auto k2 = k_pcg_upd<T, CH_>;
           set_smem_attr (k2, smem);
-          k2<<<grid, ZS_THREADS, smem, s>>> (zk, dinv, bX, bR, Pnew, bQ, ldt,
+          k2<<<fit_grid (k2, grid, ZS_THREADS, smem), ZS_THREADS, smem, s>>> (zk, dinv, bX, bR, Pnew, bQ, ldt,
                                              nvec, glog, ws.partA.p,
                                              ws.partB.p, ws.counters.p + 1,
                                              ws.scal.p, ws.ival.p, cap,
@@ -1051,9 +1141,12 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
           tbytes.push_back (zbytes + 6. * (double) n * wt * sizeof (T));
         }
         ZS_DISPATCH (ch, {
-          k_cheb<T, CH_><<<grid, ZS_THREADS, 0, s>>> (zk, vals, dinv, bX, Ro, Rn,
+          k_cheb<T, CH_><<<fit_grid (k_cheb<T, CH_>, grid, ZS_THREADS, 0),
+                                          ZS_THREADS, 0, s>>> (zk, vals, zvd<T> (Z), dinv, bX, Ro, Rn,
                                                       Do, Dn, ldt, nvec, glog,
-                                                      (T) a, (T) b, k == 1);
+                                                      (T) a, (T) b,
+                                                      (k == 1 ? CHEB_FIRST : 0)
+                                                      | CHEB_STORE_D);
         });
         LGH_LAUNCH_CHECK ();
         if (tk) {
@@ -1111,7 +1204,7 @@ server_tick_pq (const Csr &Z, const T *Zb, const T *Pold, T *Pnew, T *Q, int ld,
   ZS_DISPATCH (ch, {
     auto k1 = k_pcgx_pq<T, CH_>;
     set_smem_attr (k1, smem);
-    k1<<<grid, ZS_THREADS, smem, s>>> (zk, zvals<T> (Z), Zb, Pold, Pnew, Q, ld,
+    k1<<<fit_grid (k1, grid, ZS_THREADS, smem), ZS_THREADS, smem, s>>> (zk, zvals<T> (Z), Zb, Pold, Pnew, Q, ld,
                                        nvec, glog, 0, ws.partA.p,
                                        ws.counters.p, ws.scal.p, ws.ival.p,
                                        ws.cap);
@@ -1149,7 +1242,7 @@ server_tick_dots (const Csr &Z, const T *R, const T *Zb, int ld, int w,
   ZS_DISPATCH (ch, {
     auto kd = k_pcgx_dots<T, CH_>;
     set_smem_attr (kd, smem);
-    kd<<<grid, ZS_THREADS, smem, s>>> (zk, R, Zb, ld, nvec, glog, w, 0,
+    kd<<<fit_grid (kd, grid, ZS_THREADS, smem), ZS_THREADS, smem, s>>> (zk, R, Zb, ld, nvec, glog, w, 0,
                                        ws.partA.p, ws.partB.p,
                                        ws.counters.p + 1, ws.scal.p, ws.ival.p,
                                        ws.cap, rtol, 0, nullptr, fresh);
@@ -1172,7 +1265,7 @@ template int server_tick_dots<double> (const Csr &, const double *,
 template <typename T>
 int
 launch_cheb_step (const Csr &A, T *X, const T *Ro, T *Rn, const T *Do, T *Dn,
-                  int ld, double a, double b, int first, cudaStream_t s)
+                  int ld, double a, double b, int flags, cudaStream_t s)
 {
   constexpr int W = Pack<T>::W;
   const int nvec = ld / W;
@@ -1183,13 +1276,60 @@ launch_cheb_step (const Csr &A, T *X, const T *Ro, T *Rn, const T *Do, T *Dn,
   const T *vals = zvals<T> (A);
   const T *dinv = zdinv<T> (A);
   ZS_DISPATCH (ch, {
-    k_cheb<T, CH_><<<grid, ZS_THREADS, 0, s>>> (zk, vals, dinv, X, Ro, Rn, Do,
+    k_cheb<T, CH_><<<fit_grid (k_cheb<T, CH_>, grid, ZS_THREADS, 0),
+                                          ZS_THREADS, 0, s>>> (zk, vals, zvd<T> (A), dinv, X, Ro, Rn, Do,
                                                 Dn, ld, nvec, glog, (T) a,
-                                                (T) b, first);
+                                                (T) b, flags);
   });
   LGH_LAUNCH_CHECK ();
   return 0;
 }
+
+/* the last Chebyshev step of a smoothing sequence whose residual is not
+ * needed afterwards: x += a d + b D^{-1} r, elementwise (no Z product) */
+template <typename T>
+__global__ void
+k_cheb_tail (int64_t n, int ld, const T *__restrict__ dinv, T *__restrict__ X,
+             const T *__restrict__ R, const T *__restrict__ D, T a, T b,
+             int first)
+{
+  constexpr int W = Pack<T>::W;
+  const int nvec = ld / W;
+  const int64_t total = n * nvec;
+  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t) gridDim.x * blockDim.x) {
+    const int64_t i = e / nvec;
+    const int64_t o = i * ld + (e - i * nvec) * W;
+    const T bdi = b * dinv[i];
+    Pack<T> x = ldp (X + o), r = ldp (R + o);
+    Pack<T> d = first ? pzero<T> () : ldp (D + o);
+#pragma unroll
+    for (int k = 0; k < W; k++) x.v[k] += fma (bdi, r.v[k], a * d.v[k]);
+    stp (X + o, x);
+  }
+}
+
+template <typename T>
+int
+launch_cheb_tail (const Csr &A, T *X, const T *R, const T *D, int ld, double a,
+                  double b, int first, cudaStream_t s)
+{
+  constexpr int W = Pack<T>::W;
+  const int64_t total = A.n * (int64_t) (ld / W);
+  const int grid = (int) std::max<int64_t> (1, std::min<int64_t> (
+      (int64_t) num_sms () * 8, (total + 255) / 256));
+  k_cheb_tail<T><<<grid, 256, 0, s>>> (A.n, ld, zdinv<T> (A), X, R, D, (T) a,
+                                       (T) b, first);
+  LGH_LAUNCH_CHECK ();
+  return 0;
+}
+
+template int launch_cheb_tail<double> (const Csr &, double *, const double *,
+                                       const double *, int, double, double,
+                                       int, cudaStream_t);
+template int launch_cheb_tail<float> (const Csr &, float *, const float *,
+                                      const float *, int, double, double, int,
+                                      cudaStream_t);
 
 template int launch_cheb_step<double> (const Csr &, double *, const double *,
                                        double *, const double *, double *,
@@ -1216,7 +1356,7 @@ zresid_launch (const Csr &Z, int64_t n, int w, const double *Bm, int ldb,
   ZS_DISPATCH (ch, {
     auto kf = k_zresid<TO, CH_>;
     set_smem_attr (kf, smem);
-    kf<<<grid, ZS_THREADS, smem, s>>> (zk, Z.vals, Z.dinv, Bm, ldb, rs_in, X,
+    kf<<<fit_grid (kf, grid, ZS_THREADS, smem), ZS_THREADS, smem, s>>> (zk, Z.vals, Z.dinv, Bm, ldb, rs_in, X,
                                        ldx, Rout, ldr, nvec, glog, w, partA,
                                        partB, counter, out_r, out_b);
   });
@@ -1242,7 +1382,7 @@ zsolve_residual_norms (const Csr &Z, int64_t n, int w, const double *Bm,
   const int ld = round_ld (w);
   DBuf<double> pa, pb;
   DBuf<unsigned> cnt;
-  const int nb = num_sms () * 4;
+  const int nb = num_sms () * 8;
   LGH_TRY (pa.alloc ((size_t) ld * nb));
   LGH_TRY (pb.alloc ((size_t) ld * nb));
   LGH_TRY (cnt.alloc (4));
@@ -1251,6 +1391,90 @@ zsolve_residual_norms (const Csr &Z, int64_t n, int w, const double *Bm,
                                   (double *) nullptr, 0, out, nullptr, pa.p,
                                   pb.p, cnt.p, nb, s));
   LGH_CUDA (cudaStreamSynchronize (s));
+  return 0;
+}
+
+
+/* Y += D (FP32 correction into the FP64 iterate), row-major, w columns */
+__global__ void
+k_add_f32 (int64_t n, int w, double *Y, int ldy, const float *D, int ldd)
+{
+  const int64_t total = n * w;
+  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t) gridDim.x * blockDim.x) {
+    const int64_t i = e / w;
+    const int c = (int) (e - i * w);
+    Y[i * ldy + c] += (double) D[i * ldd + c];
+  }
+}
+
+/* Z Y = S X to FP64 accuracy with FP32 sweeps: mixed-precision iterative
+ * refinement.  Y = 0; repeat { R = fp32(S X - Z Y) with the per-column
+ * Jacobi-scaled norms ||D^{-1} R||, ||D^{-1} S X||; stop when every column
+ * has ||D^{-1} R|| <= rtol ||D^{-1} S X||; solve Z D = R in FP32 to
+ * inner_rtol (the blocked solver of the prior, same preconditioner); Y +=
+ * D }.  The residual is formed in FP64 from the FP64 iterate, so the
+ * attainable accuracy is FP64's; each step gains about inner_rtol.
+ * Returns LGH_ERR_NOT_CONVERGED after max_steps corrections. */
+int
+zsolve_refined (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws32,
+                int64_t n, int w, const double *X, int ldx,
+                const double *rowscale_in, double *Y, int ldy,
+                const double *rowscale_out, double inner_rtol, int max_steps,
+                ZsolveStats *st, int *steps_out, cudaStream_t s)
+{
+  if (w == 0) return 0;
+  LGH_CHECK (ldy >= round_ld (w) && ldy % 2 == 0, LGH_ERR_ARG_SIZ,
+             "zsolve_refined: ldy %d", ldy);
+  const int ld32 = round_ld (w);
+  DBuf<float> R32, D32;
+  DBuf<double> pa, pb, nrm;
+  DBuf<unsigned> cnt;
+  const int nb = num_sms () * 8;
+  LGH_TRY (R32.alloc ((size_t) n * ld32));
+  LGH_TRY (D32.alloc ((size_t) n * ld32));
+  LGH_TRY (pa.alloc ((size_t) ld32 * nb));
+  LGH_TRY (pb.alloc ((size_t) ld32 * nb));
+  LGH_TRY (nrm.alloc (2 * (size_t) ld32));
+  LGH_TRY (cnt.alloc (4));
+  LGH_CUDA (cudaMemsetAsync (cnt.p, 0, 4 * sizeof (unsigned), s));
+  LGH_CUDA (cudaMemset2DAsync (Y, (size_t) ldy * sizeof (double), 0,
+                               (size_t) ld32 * sizeof (double), n, s));
+  ZsolveCfg icfg = cfg;
+  icfg.rtol = inner_rtol;
+  std::vector<double> hn (2 * (size_t) ld32);
+  const int egrid = (int) std::max<int64_t> (1, std::min<int64_t> (
+      (int64_t) num_sms () * 8, (n * w + 255) / 256));
+  int step = 0;
+  for (;; step++) {
+    LGH_TRY (zresid_launch<float> (Z, n, w, X, ldx, rowscale_in, Y, ldy, R32.p,
+                                   ld32, nrm.p, nrm.p + ld32, pa.p, pb.p, cnt.p,
+                                   nb, s));
+    LGH_CUDA (cudaMemcpyAsync (hn.data (), nrm.p, hn.size () * sizeof (double),
+                               cudaMemcpyDeviceToHost, s));
+    LGH_CUDA (cudaStreamSynchronize (s));
+    bool done = true;
+    for (int c = 0; c < w; c++)
+      if (hn[c] > cfg.rtol * hn[ld32 + c]) done = false;
+    if (done || step >= max_steps) break;
+    LGH_TRY (zsolve_block<float> (Z, icfg, mg, ws32, n, w, R32.p, ld32, nullptr,
+                                  D32.p, ld32, nullptr, st, 0, s));
+    k_add_f32<<<egrid, 256, 0, s>>> (n, w, Y, ldy, D32.p, ld32);
+    LGH_LAUNCH_CHECK ();
+  }
+  if (steps_out) *steps_out = step;
+  if (rowscale_out)
+    LGH_TRY (launch_rowscale<double> (n, w, rowscale_out, Y, ldy, Y, ldy, s));
+  LGH_CUDA (cudaStreamSynchronize (s));
+  if (step >= max_steps) {
+    bool done = true;
+    for (int c = 0; c < w; c++)
+      if (hn[c] > cfg.rtol * hn[ld32 + c]) done = false;
+    if (!done)
+      return set_error (LGH_ERR_NOT_CONVERGED,
+                        "zsolve_refined: %d refinement steps did not reach "
+                        "rtol %g", max_steps, cfg.rtol);
+  }
   return 0;
 }
 

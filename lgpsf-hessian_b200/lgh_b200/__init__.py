@@ -206,6 +206,7 @@ SIGNATURES = {
     "lgh_server_get_stats": (ctypes.c_int, [P, ctypes.POINTER(ServerStats)]),
     "lgh_server_destroy": (None, [P]),
     "lgh_launch_count": (ctypes.c_long, []),
+    "lgh_runtime_counters": (ctypes.c_int, [c_dbl_p]),
     "lgh_kernel_timing": (ctypes.c_int, [ctypes.c_int]),
     "lgh_kernel_timing_get": (ctypes.c_char_p, [ctypes.c_int, c_dbl_p,
                                                 ctypes.POINTER(ctypes.c_long),
@@ -413,14 +414,15 @@ class Prior:
                      "lgh_prior_create_mat_pc")
 
     def info(self):
-        out = np.zeros(12)
+        out = np.zeros(14)
         _chk(load().lgh_prior_get_info(self.h, out.ctypes.data_as(c_dbl_p)),
              "lgh_prior_get_info")
         return dict(emin=out[0], emax=out[1], lmin=out[2], lmax=out[3],
                     nit=int(out[4]), bound_its=int(out[5]),
                     mean_col_iters=out[6], calls=int(out[7]),
                     mg_levels=int(out[8]), mg_coarse=int(out[9]),
-                    mg_setup_s=out[10], pc=int(out[11]))
+                    mg_setup_s=out[10], pc=int(out[11]),
+                    refine_calls=int(out[12]), refine_steps=int(out[13]))
 
     def apply(self, x):
         vx, vy = Vec(data=x), Vec(self.n)
@@ -576,6 +578,15 @@ def kernel_timing_get():
             return out
         out[name.decode()] = (ms.value, n.value, by.value)
         i += 1
+
+
+def runtime_counters():
+    """Host-side runtime counters (lgh_runtime_counters)."""
+    out = np.zeros(5)
+    _chk(load().lgh_runtime_counters(out.ctypes.data_as(c_dbl_p)),
+         "lgh_runtime_counters")
+    return dict(allocs=int(out[0]), alloc_s=out[1], frees=int(out[2]),
+                free_s=out[3], launches=int(out[4]))
 
 
 class Server:

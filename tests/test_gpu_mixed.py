@@ -1,0 +1,97 @@
+"""Mixed precision (LGH_PREC_MIXED: FP32 sketch blocks, F-applies and
+CholQR2 sweeps with FP64 accumulation; FP64 small dense work, eigenvectors
+and the downstream operations) against the plain FP64 build on the same
+inputs and the same hashed sketch.  The reference computes in FP64 only;
+the mixed form is an extension whose accuracy is reported against FP64:
+eigenvalue error relative to the largest eigenvalue, the largest principal
+angle between the leading eigenvector subspaces, and solve / logdet
+agreement.
+"""
+
+import numpy as np
+import pytest
+
+import lgh_b200 as L
+import lgh_b200.problems as P
+
+pytestmark = pytest.mark.gpu
+
+MIXED = 1
+
+
+@pytest.fixture(scope="module")
+def c1(cuda_device):
+    cfg = P.grid_problem("c1")
+    B, Z = L.Mat(cfg["B"]), L.Mat(cfg["Z"])
+    pr = L.Prior(Z=Z, mass=cfg["mass"], opts=L.prior_opts(ksp_rtol=1e-12))
+    return cfg, B, Z, pr
+
+
+def _sin_max(U1, U2):
+    s = np.linalg.svd(U2.T @ U1, compute_uv=False)
+    return float(np.sqrt(max(0.0, 1.0 - np.min(s) ** 2)))
+
+
+def test_mixed_spectrum_matches_fp64(c1):
+    cfg, B, Z, pr = c1
+    o = L.glr_opts(ell=60, seed=0, trunc_rel=1e-3)
+    g64 = L.Glr(B, pr, o)
+    g32 = L.Glr(B, pr, o, exec=L.exec_opts(precision=MIXED))
+    assert g32.stats()["precision"] == MIXED
+    l64, l32 = g64.eigs(), g32.eigs()
+    k = min(len(l64), len(l32)) - 1
+    assert k >= 20
+    assert abs(len(l64) - len(l32)) <= 1
+    err = np.max(np.abs(l32[:k] - l64[:k])) / l64[0]
+    assert err < 1e-5, err
+    # leading, well separated eigenvectors span the same subspace
+    U64, U32 = g64.U()[:, :10], g32.U()[:, :10]
+    assert _sin_max(U64, U32) < 1e-3
+    # downstream operations run in FP64 on the mixed model
+    rhs = np.random.default_rng(4).standard_normal(cfg["N"])
+    x64, x32 = g64.solve(1.0, rhs), g32.solve(1.0, rhs)
+    assert np.linalg.norm(x32 - x64) / np.linalg.norm(x64) < 1e-4
+    ld64, ld32 = g64.logdet(1.0), g32.logdet(1.0)
+    assert abs(ld32 - ld64) < 1e-4 * abs(ld64)
+
+
+def test_mixed_extend_equals_one_shot(c1):
+    """Incremental extension in mixed precision (FP32 BCGS2 against the old
+    basis) reaches the one-shot mixed spectrum at the extended width."""
+    cfg, B, Z, pr = c1
+    ex = L.exec_opts(precision=MIXED)
+    ga = L.Glr(B, pr, L.glr_opts(ell=40, seed=0, trunc_rel=1e-3), exec=ex)
+    ga.extend(20)
+    gb = L.Glr(B, pr, L.glr_opts(ell=60, seed=0, trunc_rel=1e-3), exec=ex)
+    la, lb = ga.eigs(), gb.eigs()
+    k = min(len(la), len(lb)) - 1
+    assert k >= 20
+    assert np.max(np.abs(la[:k] - lb[:k])) / lb[0] < 1e-5
+
+
+def test_mixed_batch_solves_are_refined_to_fp64(c1):
+    """The batched solves of a mixed object run their Z-solves as FP32
+    sweeps refined in FP64 to the prior's tolerance (1e-12 here), so they
+    agree with the FP64 single-vector solve of the same model to FP64
+    solver accuracy."""
+    cfg, B, Z, pr = c1
+    g = L.Glr(B, pr, L.glr_opts(ell=40, seed=0, check=0),
+              exec=L.exec_opts(precision=MIXED))
+    before = pr.info()
+    R = np.random.default_rng(9).standard_normal((cfg["N"], 2))
+    cs = [0.1, 3.0]
+    X = g.solve_batch(cs, R)
+    after = pr.info()
+    assert after["refine_calls"] >= before["refine_calls"] + 3  # W, y1, y0
+    steps = after["refine_steps"] - before["refine_steps"]
+    calls = after["refine_calls"] - before["refine_calls"]
+    assert 1 <= steps / calls <= 4
+    for si, c in enumerate(cs):
+        for j in range(2):
+            ref = g.solve(c, R[:, j])
+            assert np.linalg.norm(X[si][:, j] - ref) \
+                < 1e-8 * np.linalg.norm(ref)
+    S = g.sample_batch(cs, R)
+    for si, c in enumerate(cs):
+        ref = g.sample(c, R[:, 0])
+        assert np.linalg.norm(S[si][:, 0] - ref) < 1e-8 * np.linalg.norm(ref)
