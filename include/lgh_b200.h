@@ -185,7 +185,7 @@ int lgh_prior_solve_block (lgh_prior_t *prior, int m, const double *X,
  * emax, margined lmin, lmax, Chebyshev nit, probe iterations, mean
  * per-column CG iterations so far, number of solve calls, multigrid
  * levels, coarse size, multigrid setup seconds, preconditioner type,
- * mixed-precision refined solves, and their refinement steps.          */
+ * number of block solves run with the FP32 V-cycle (mixed form), 0.     */
 int lgh_prior_get_info (const lgh_prior_t *prior, double *out);
 
 /* ---- glr.h --------------------------------------------------------------- */
@@ -275,15 +275,19 @@ int lgh_glr_eigs (const lgh_glr_t *glr, int *nkept, const double **lam);
 
 /* ---- extensions --------------------------------------------------------- */
 
+/* Mixed precision: the tall blocks (sketch, F-applies, CholQR2 sweeps)
+ * are FP32 with FP64 accumulation; every ell x ell operation is FP64; the
+ * Z-solves keep FP64 Krylov vectors with an FP32 multigrid V-cycle as the
+ * preconditioner (FP32 Krylov vectors would stop at eps_32 kappa(Z),
+ * 1e-3 on a 512^2 grid), so they reach the prior's tolerance.           */
 #define LGH_PREC_FP64  0   /* everything FP64 (the plain form)             */
-#define LGH_PREC_MIXED 1   /* FP32 sweeps/blocks, FP64 small dense + core  */
+#define LGH_PREC_MIXED 1   /* FP32 blocks and V-cycles, FP64 Krylov + core */
 
 typedef struct lgh_exec_opts
 {
   int    precision;    /* LGH_PREC_FP64 (default) | LGH_PREC_MIXED       */
-  double inner_rtol;   /* mixed: FP32 Z-solve tolerance of the build
-                          (default 1e-6)                                 */
-  int    max_refine;   /* mixed: FP64 refinement steps per solve (4)     */
+  double inner_rtol;   /* mixed: Z-solve tolerance on FP32 blocks; 0
+                          (default) = the prior's own                    */
   int    verbose;
   int    rank_cap;     /* keep at most rank_cap modes ("rank r,
                           oversample p" = ell r + p, rank_cap r); 0 = off */

@@ -522,6 +522,17 @@ prior_solve_rows (lgh_prior_t *p, int w, const T *X, int ldx,
     ZsolveCfg cfg;
     prior_zcfg (p, cfg);
     if (rtol_override > 0.) cfg.rtol = rtol_override;
+    if (std::is_same<T, float>::value && p->mg != nullptr && cfg.mode <= 1) {
+      /* FP32 blocks (mixed form): FP64 PCG iterates, FP32 V-cycle, FP32 in
+       * and out -- FP32 Krylov vectors would stop at eps_32 kappa(Z) */
+      const int64_t n = p->n;
+      const int ld = round_ld (w);
+      LGH_TRY (p->mix_in.alloc ((size_t) n * ld));
+      LGH_TRY (launch_f32_to_f64 (n, w, (const float *) X, ldx, p->mix_in.p, ld, s));
+      LGH_TRY (prior_solve_pc32 (p, w, p->mix_in.p, ld, s_in, p->mix_in.p, ld,
+                                 s_out, rtol_override));
+      return launch_f64_to_f32 (n, w, p->mix_in.p, ld, (float *) Y, ldy, s);
+    }
     int cap = std::min (w, std::is_same<T, double>::value ? 512 : 1024);
     ZWork &ws = std::is_same<T, double>::value ? p->ws64 : p->ws32;
     LGH_TRY (ws.alloc (p->n, cap, std::is_same<T, float>::value));
@@ -559,29 +570,6 @@ prior_solve_rows (lgh_prior_t *p, int w, const T *X, int ldx,
   }
 }
 
-/* the same FP64 solve to the prior's tolerance through FP32 sweeps and FP64
- * iterative refinement (Mat priors; callback priors solve in FP64).  X and
- * Y must not overlap. */
-int
-prior_solve_refined (lgh_prior_t *p, int w, const double *X, int ldx,
-                     const double *s_in, double *Y, int ldy,
-                     const double *s_out, double inner_rtol, int max_steps)
-{
-  if (w == 0) return 0;
-  if (!p->is_mat)
-    return prior_solve_rows<double> (p, w, X, ldx, s_in, Y, ldy, s_out);
-  ZsolveCfg cfg;
-  prior_zcfg (p, cfg);
-  LGH_TRY (p->ws32.alloc (p->n, std::min (w, 1024), 1));
-  int steps = 0;
-  const int rc = zsolve_refined (p->Z->csr, cfg, p->mg, p->ws32, p->n, w, X, ldx,
-                                 s_in, Y, ldy, s_out, inner_rtol, max_steps,
-                                 &p->stats, &steps, stream ());
-  p->refine_calls++;
-  p->refine_steps += steps;
-  return rc;
-}
-
 int
 resident_ctas (const void *fn, int threads, int smem)
 {
@@ -601,6 +589,28 @@ resident_ctas (const void *fn, int threads, int smem)
   const int r = per_sm > 0 ? per_sm * num_sms () : 0;
   cache[key] = r;
   return r;
+}
+
+/* FP64 block solve to the prior's tolerance with an FP32 V-cycle inside
+ * FP64 PCG (the mixed form's Z-solves; Jacobi or callback priors solve in
+ * FP64).  X and Y may be the same block. */
+int
+prior_solve_pc32 (lgh_prior_t *p, int w, const double *X, int ldx,
+                  const double *s_in, double *Y, int ldy, const double *s_out,
+                  double rtol_override)
+{
+  if (w == 0) return 0;
+  if (!p->is_mat || p->mg == nullptr || p->zcfg.mode > 1)
+    return prior_solve_rows<double> (p, w, X, ldx, s_in, Y, ldy, s_out,
+                                     rtol_override);
+  ZsolveCfg cfg;
+  prior_zcfg (p, cfg);
+  if (rtol_override > 0.) cfg.rtol = rtol_override;
+  cfg.pc32 = 1;
+  LGH_TRY (p->ws64.alloc (p->n, std::min (w, 512), 0));
+  p->pc32_calls++;
+  return zsolve_block<double> (p->Z->csr, cfg, p->mg, p->ws64, p->n, w, X, ldx,
+                               s_in, Y, ldy, s_out, &p->stats, 0, stream ());
 }
 
 template int prior_solve_rows<double> (lgh_prior_t *, int, const double *, int,
@@ -867,8 +877,8 @@ lgh_prior_get_info (const lgh_prior_t *p, double *out)
   out[9] = p->mg ? (double) p->mg->n0 : 0.;
   out[10] = p->mg ? p->mg->setup_s : 0.;
   out[11] = p->pc_type;
-  out[12] = (double) p->refine_calls;
-  out[13] = (double) p->refine_steps;
+  out[12] = (double) p->pc32_calls;
+  out[13] = 0.;
   return 0;
 }
 

@@ -199,8 +199,9 @@ apply_F (lgh_glr_t *g, int w, const T *X, int ldx, T *Y, int ldy, T *W,
 {
   cudaStream_t s = stream ();
   const double *ms = g->prior->msqrt.p;
-  /* FP32 Z-solves run at the mixed form's inner tolerance */
-  const double rt = std::is_same<T, float>::value
+  /* FP32 blocks: the prior's tolerance unless inner_rtol asks for a looser
+   * one (inner_rtol <= 0: the prior's) */
+  const double rt = std::is_same<T, float>::value && g->exec.inner_rtol > 0.
                     ? std::max (g->exec.inner_rtol, g->prior->zcfg.rtol) : 0.;
   double t0 = wall ();
   LGH_TRY (prior_solve_rows<T> (g->prior, w, X, ldx, ms, W, ldw, nullptr, rt));
@@ -607,16 +608,15 @@ check_vecs (lgh_glr_t *g, lgh_Vec a, lgh_Vec b, const char *who)
   return 0;
 }
 
-/* the FP64 Z-solves of the downstream block operations: FP64 sweeps, or
- * for a mixed-precision object FP32 sweeps refined in FP64 to the prior's
- * tolerance.  X and Y must not overlap. */
+/* the FP64 Z-solves of the downstream block operations: FP64 PCG with an
+ * FP64 V-cycle, or for a mixed-precision object with an FP32 V-cycle;
+ * both to the prior's tolerance.  X and Y must not overlap. */
 static int
 glr_zsolve (lgh_glr_t *g, int w, const double *X, int ldx, const double *s_in,
             double *Y, int ldy, const double *s_out)
 {
   if (g->exec.precision == LGH_PREC_MIXED)
-    return prior_solve_refined (g->prior, w, X, ldx, s_in, Y, ldy, s_out,
-                                g->exec.inner_rtol, g->exec.max_refine);
+    return prior_solve_pc32 (g->prior, w, X, ldx, s_in, Y, ldy, s_out);
   return prior_solve_rows<double> (g->prior, w, X, ldx, s_in, Y, ldy, s_out);
 }
 
@@ -719,8 +719,7 @@ lgh_exec_opts_default (void)
 {
   lgh_exec_opts_t e;
   e.precision = LGH_PREC_FP64;
-  e.inner_rtol = 1e-6;
-  e.max_refine = 4;
+  e.inner_rtol = 0.;
   e.verbose = 0;
   e.rank_cap = 0;
   return e;

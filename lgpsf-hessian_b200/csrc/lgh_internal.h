@@ -259,6 +259,7 @@ struct ZsolveCfg
   double lmin = 0, lmax = 0; /* margined interval (mode 2/3) */
   int nit = 0;
   int check_every = 16;
+  int pc32 = 0;          /* FP64 PCG with an FP32 V-cycle (mixed form)  */
 };
 
 struct Hierarchy; /* aggregation multigrid (mode 3) */
@@ -277,6 +278,7 @@ struct ZWork
   int64_t n = 0;
   int is32 = 0;
   DBuf<char> X, R, P0, P1, Q, Zb;
+  DBuf<char> R32, Z32;         /* FP32 V-cycle input / output (pc32) */
   DBuf<double> partA, partB;   /* [nblocks][ld] */
   DBuf<double> scal;           /* per-column scalars */
   DBuf<int> ival;              /* active flags / counts */
@@ -297,22 +299,11 @@ int zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg,
                   const double *rowscale_out, ZsolveStats *st,
                   int record_hist, cudaStream_t s);
 
-/* residual-norm helper used by refinement and tests:
+/* residual-norm helper used by the tests:
  * out[c] = || D^{-1}(B - Z X) ||_2 per column (FP64) */
 int zsolve_residual_norms (const Csr &Z, int64_t n, int w, const double *Bm,
                            int ldb, const double *X, int ldx, double *out,
                            cudaStream_t s);
-
-/* Z Y = S X to FP64 accuracy (per-column Jacobi-scaled residual <= rtol of
- * cfg) by mixed-precision iterative refinement with FP32 inner solves to
- * inner_rtol; FP64 X, Y (ldy >= round_ld (w)).  steps_out (nullable):
- * corrections taken. */
-int zsolve_refined (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg,
-                    ZWork &ws32, int64_t n, int w, const double *X, int ldx,
-                    const double *rowscale_in, double *Y, int ldy,
-                    const double *rowscale_out, double inner_rtol,
-                    int max_steps, ZsolveStats *st, int *steps_out,
-                    cudaStream_t s);
 
 /* mode 3: build / destroy the hierarchy from Z (device), CSR on host */
 int mg_build (const Csr &Z, int tile, double smoother_top, int nu,

@@ -48,7 +48,8 @@ struct lgh_prior
   double emin = 0., emax = 0.;
   int bound_its = 0;
   lgh::ZsolveStats stats;
-  long refine_calls = 0, refine_steps = 0;   /* mixed-precision refinement */
+  long pc32_calls = 0;          /* Z-solves with the FP32 V-cycle (mixed) */
+  lgh::DBuf<double> mix_in;     /* FP64 copy of an FP32 block (mixed) */
 };
 
 /* struct lgh_glr (glr_common_impl.h:252-278), device resident */
@@ -99,10 +100,9 @@ template <typename T>
 int prior_solve_rows (lgh_prior_t *p, int w, const T *X, int ldx,
                       const double *s_in, T *Y, int ldy, const double *s_out,
                       double rtol_override = 0.);
-int prior_solve_refined (lgh_prior_t *p, int w, const double *X, int ldx,
-                         const double *s_in, double *Y, int ldy,
-                         const double *s_out, double inner_rtol,
-                         int max_steps);
+int prior_solve_pc32 (lgh_prior_t *p, int w, const double *X, int ldx,
+                      const double *s_in, double *Y, int ldy,
+                      const double *s_out, double rtol_override = 0.);
 int launch_vec_div (int64_t n, const double *x, const double *d, double *y,
                     cudaStream_t s);
 }

@@ -712,7 +712,7 @@ k_chebx (ZK z, const T *__restrict__ vals, const T *__restrict__ Zb,
 }
 
 /* ---- FP64 residual, R = S B - Z X (pads zero), per-column ||D^{-1} R|| and
- * ||D^{-1} S B|| (refinement and tests) ---------------------------------- */
+ * ||D^{-1} S B|| (tests) ------------------------------------------------- */
 template <typename TO, int CH>
 __global__ void __launch_bounds__ (ZS_THREADS)
 k_zresid (ZK z, const double *__restrict__ vals,
@@ -874,6 +874,35 @@ zvd (const Csr &Z)
     return set_error (LGH_ERR_SUP, "zsolve: chunking %d unsupported", CHV);  \
   }
 
+/* flat conversion of a row-major block (same leading dimension on both
+ * sides), four elements per thread */
+template <typename TI, typename TO>
+__global__ void
+k_cvt_flat (int64_t count, const TI *__restrict__ X, TO *__restrict__ Y)
+{
+  const int64_t q = count / 4;
+  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < q;
+       e += (int64_t) gridDim.x * blockDim.x) {
+    const int64_t o = e * 4;
+#pragma unroll
+    for (int k = 0; k < 4; k++) Y[o + k] = (TO) X[o + k];
+  }
+  for (int64_t o = q * 4 + (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+       o < count; o += (int64_t) gridDim.x * blockDim.x)
+    Y[o] = (TO) X[o];
+}
+
+template <typename TI, typename TO>
+static int
+cvt_flat (int64_t count, const TI *X, TO *Y, cudaStream_t s)
+{
+  const int grid = (int) std::max<int64_t> (1, std::min<int64_t> (
+      (int64_t) num_sms () * 8, (count / 4 + 255) / 256));
+  k_cvt_flat<TI, TO><<<grid, 256, 0, s>>> (count, X, Y);
+  LGH_LAUNCH_CHECK ();
+  return 0;
+}
+
 template <typename T>
 int
 zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
@@ -941,7 +970,25 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
       static thread_local KTrace ktr;
       KTrace *tr = timing ? &ktr : nullptr;
       const double bw = (double) n * wt * sizeof (T);
-      LGH_TRY (mg_vcycle<T> (mg, bR, bZ, ldt, wt, s, tr));
+      /* z = V(r): in T, or (cfg.pc32, FP64 iterates) an FP32 V-cycle
+       * between two conversions: the Krylov vectors and so the attainable
+       * accuracy stay FP64, the V-cycle's traffic is halved */
+      const bool pc32 = cfg.pc32 && std::is_same<T, double>::value;
+      float *R32 = nullptr, *Z32 = nullptr;
+      if (pc32) {
+        LGH_TRY (ws.R32.alloc ((size_t) n * ws.cap * sizeof (float)));
+        LGH_TRY (ws.Z32.alloc ((size_t) n * ws.cap * sizeof (float)));
+        R32 = (float *) ws.R32.p;
+        Z32 = (float *) ws.Z32.p;
+      }
+      auto precond = [&] () -> int {
+        if (!pc32) return mg_vcycle<T> (mg, bR, bZ, ldt, wt, s, tr);
+        const int64_t cnt = n * (int64_t) ldt;
+        LGH_TRY ((cvt_flat<T, float> (cnt, bR, R32, s)));
+        LGH_TRY (mg_vcycle<float> (mg, R32, Z32, ldt, wt, s, nullptr));
+        return cvt_flat<float, T> (cnt, Z32, bZ, s);
+      };
+      LGH_TRY (precond ());
       ZS_DISPATCH (ch, {
         auto kd = k_pcgx_dots<T, CH_>;
         set_smem_attr (kd, smem);
@@ -970,7 +1017,7 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
                                             ws.scal.p + S_ALPHA * cap);
         LGH_LAUNCH_CHECK ();
         if (tr) LGH_TRY (tr->end (s));
-        LGH_TRY (mg_vcycle<T> (mg, bR, bZ, ldt, wt, s, tr));
+        LGH_TRY (precond ());
         if (tr) LGH_TRY (tr->begin (K_PCGX_DOTS, 2. * bw, s));
         ZS_DISPATCH (ch, {
           auto kd = k_pcgx_dots<T, CH_>;
@@ -1394,88 +1441,5 @@ zsolve_residual_norms (const Csr &Z, int64_t n, int w, const double *Bm,
   return 0;
 }
 
-
-/* Y += D (FP32 correction into the FP64 iterate), row-major, w columns */
-__global__ void
-k_add_f32 (int64_t n, int w, double *Y, int ldy, const float *D, int ldd)
-{
-  const int64_t total = n * w;
-  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (int64_t) gridDim.x * blockDim.x) {
-    const int64_t i = e / w;
-    const int c = (int) (e - i * w);
-    Y[i * ldy + c] += (double) D[i * ldd + c];
-  }
-}
-
-/* Z Y = S X to FP64 accuracy with FP32 sweeps: mixed-precision iterative
- * refinement.  Y = 0; repeat { R = fp32(S X - Z Y) with the per-column
- * Jacobi-scaled norms ||D^{-1} R||, ||D^{-1} S X||; stop when every column
- * has ||D^{-1} R|| <= rtol ||D^{-1} S X||; solve Z D = R in FP32 to
- * inner_rtol (the blocked solver of the prior, same preconditioner); Y +=
- * D }.  The residual is formed in FP64 from the FP64 iterate, so the
- * attainable accuracy is FP64's; each step gains about inner_rtol.
- * Returns LGH_ERR_NOT_CONVERGED after max_steps corrections. */
-int
-zsolve_refined (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws32,
-                int64_t n, int w, const double *X, int ldx,
-                const double *rowscale_in, double *Y, int ldy,
-                const double *rowscale_out, double inner_rtol, int max_steps,
-                ZsolveStats *st, int *steps_out, cudaStream_t s)
-{
-  if (w == 0) return 0;
-  LGH_CHECK (ldy >= round_ld (w) && ldy % 2 == 0, LGH_ERR_ARG_SIZ,
-             "zsolve_refined: ldy %d", ldy);
-  const int ld32 = round_ld (w);
-  DBuf<float> R32, D32;
-  DBuf<double> pa, pb, nrm;
-  DBuf<unsigned> cnt;
-  const int nb = num_sms () * 8;
-  LGH_TRY (R32.alloc ((size_t) n * ld32));
-  LGH_TRY (D32.alloc ((size_t) n * ld32));
-  LGH_TRY (pa.alloc ((size_t) ld32 * nb));
-  LGH_TRY (pb.alloc ((size_t) ld32 * nb));
-  LGH_TRY (nrm.alloc (2 * (size_t) ld32));
-  LGH_TRY (cnt.alloc (4));
-  LGH_CUDA (cudaMemsetAsync (cnt.p, 0, 4 * sizeof (unsigned), s));
-  LGH_CUDA (cudaMemset2DAsync (Y, (size_t) ldy * sizeof (double), 0,
-                               (size_t) ld32 * sizeof (double), n, s));
-  ZsolveCfg icfg = cfg;
-  icfg.rtol = inner_rtol;
-  std::vector<double> hn (2 * (size_t) ld32);
-  const int egrid = (int) std::max<int64_t> (1, std::min<int64_t> (
-      (int64_t) num_sms () * 8, (n * w + 255) / 256));
-  int step = 0;
-  for (;; step++) {
-    LGH_TRY (zresid_launch<float> (Z, n, w, X, ldx, rowscale_in, Y, ldy, R32.p,
-                                   ld32, nrm.p, nrm.p + ld32, pa.p, pb.p, cnt.p,
-                                   nb, s));
-    LGH_CUDA (cudaMemcpyAsync (hn.data (), nrm.p, hn.size () * sizeof (double),
-                               cudaMemcpyDeviceToHost, s));
-    LGH_CUDA (cudaStreamSynchronize (s));
-    bool done = true;
-    for (int c = 0; c < w; c++)
-      if (hn[c] > cfg.rtol * hn[ld32 + c]) done = false;
-    if (done || step >= max_steps) break;
-    LGH_TRY (zsolve_block<float> (Z, icfg, mg, ws32, n, w, R32.p, ld32, nullptr,
-                                  D32.p, ld32, nullptr, st, 0, s));
-    k_add_f32<<<egrid, 256, 0, s>>> (n, w, Y, ldy, D32.p, ld32);
-    LGH_LAUNCH_CHECK ();
-  }
-  if (steps_out) *steps_out = step;
-  if (rowscale_out)
-    LGH_TRY (launch_rowscale<double> (n, w, rowscale_out, Y, ldy, Y, ldy, s));
-  LGH_CUDA (cudaStreamSynchronize (s));
-  if (step >= max_steps) {
-    bool done = true;
-    for (int c = 0; c < w; c++)
-      if (hn[c] > cfg.rtol * hn[ld32 + c]) done = false;
-    if (!done)
-      return set_error (LGH_ERR_NOT_CONVERGED,
-                        "zsolve_refined: %d refinement steps did not reach "
-                        "rtol %g", max_steps, cfg.rtol);
-  }
-  return 0;
-}
 
 } /* namespace lgh */

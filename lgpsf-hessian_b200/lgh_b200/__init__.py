@@ -77,8 +77,7 @@ class PriorMatOpts(ctypes.Structure):
 class ExecOpts(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int),
                 ("inner_rtol", ctypes.c_double),
-                ("max_refine", ctypes.c_int), ("verbose", ctypes.c_int),
-                ("rank_cap", ctypes.c_int)]
+                ("verbose", ctypes.c_int), ("rank_cap", ctypes.c_int)]
 
 
 class ServerOpts(ctypes.Structure):
@@ -422,7 +421,7 @@ class Prior:
                     mean_col_iters=out[6], calls=int(out[7]),
                     mg_levels=int(out[8]), mg_coarse=int(out[9]),
                     mg_setup_s=out[10], pc=int(out[11]),
-                    refine_calls=int(out[12]), refine_steps=int(out[13]))
+                    pc32_calls=int(out[12]))
 
     def apply(self, x):
         vx, vy = Vec(data=x), Vec(self.n)

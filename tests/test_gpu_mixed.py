@@ -1,7 +1,8 @@
 """Mixed precision (LGH_PREC_MIXED: FP32 sketch blocks, F-applies and
-CholQR2 sweeps with FP64 accumulation; FP64 small dense work, eigenvectors
-and the downstream operations) against the plain FP64 build on the same
-inputs and the same hashed sketch.  The reference computes in FP64 only;
+CholQR2 sweeps with FP64 accumulation; Z-solves with FP64 Krylov vectors
+and an FP32 V-cycle; FP64 small dense work, eigenvectors and downstream
+operations) against the plain FP64 build on the same inputs and the same
+hashed sketch.  The reference computes in FP64 only;
 the mixed form is an extension whose accuracy is reported against FP64:
 eigenvalue error relative to the largest eigenvalue, the largest principal
 angle between the leading eigenvector subspaces, and solve / logdet
@@ -43,7 +44,7 @@ def test_mixed_spectrum_matches_fp64(c1):
     assert k >= 20
     assert abs(len(l64) - len(l32)) <= 1
     err = np.max(np.abs(l32[:k] - l64[:k])) / l64[0]
-    assert err < 1e-5, err
+    assert err < 1e-6, err
     # leading, well separated eigenvectors span the same subspace
     U64, U32 = g64.U()[:, :10], g32.U()[:, :10]
     assert _sin_max(U64, U32) < 1e-3
@@ -66,13 +67,13 @@ def test_mixed_extend_equals_one_shot(c1):
     la, lb = ga.eigs(), gb.eigs()
     k = min(len(la), len(lb)) - 1
     assert k >= 20
-    assert np.max(np.abs(la[:k] - lb[:k])) / lb[0] < 1e-5
+    assert np.max(np.abs(la[:k] - lb[:k])) / lb[0] < 1e-6
 
 
-def test_mixed_batch_solves_are_refined_to_fp64(c1):
-    """The batched solves of a mixed object run their Z-solves as FP32
-    sweeps refined in FP64 to the prior's tolerance (1e-12 here), so they
-    agree with the FP64 single-vector solve of the same model to FP64
+def test_mixed_batch_solves_reach_fp64_accuracy(c1):
+    """The batched solves of a mixed object run FP64 PCG with the FP32
+    V-cycle as preconditioner to the prior's tolerance (1e-12 here), so
+    they agree with the FP64 single-vector solve of the same model to FP64
     solver accuracy."""
     cfg, B, Z, pr = c1
     g = L.Glr(B, pr, L.glr_opts(ell=40, seed=0, check=0),
@@ -82,10 +83,7 @@ def test_mixed_batch_solves_are_refined_to_fp64(c1):
     cs = [0.1, 3.0]
     X = g.solve_batch(cs, R)
     after = pr.info()
-    assert after["refine_calls"] >= before["refine_calls"] + 3  # W, y1, y0
-    steps = after["refine_steps"] - before["refine_steps"]
-    calls = after["refine_calls"] - before["refine_calls"]
-    assert 1 <= steps / calls <= 4
+    assert after["pc32_calls"] >= before["pc32_calls"] + 3  # W, y1, y0
     for si, c in enumerate(cs):
         for j in range(2):
             ref = g.solve(c, R[:, j])
