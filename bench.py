@@ -72,6 +72,18 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(seconds, world, device):
+    """The slowest rank's device-timed seconds (every rank calls this at
+    the same point; one all-reduce of one double)."""
+    if world <= 1:
+        return seconds
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([seconds], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def workload(cfg):
     return {"workload": "c2: 512^2 2D grid (N=%d), B Gaussian x Wendland "
                         "(%.1f nnz/row), Z = L + 25 M (5-point), ell=%d "
@@ -307,11 +319,8 @@ def run_ours(args):
     runtime = {k: (rt1[k] - rt0[k]) / args.steps
                for k in ("allocs", "alloc_s", "frees", "free_s")}
     clk = clocks.stop()
-    elapsed = t_start.elapsed_time(t_end) / 1e3
-    if world > 1:
-        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = max_over_ranks(t_start.elapsed_time(t_end) / 1e3, world,
+                             "cuda")
     build_s = [ev[0].elapsed_time(ev[1]) / 1e3 for ev, _ in timers]
     solve_s = [ev[1].elapsed_time(ev[2]) / 1e3 for ev, _ in timers]
     g_last = timers[-1][1]
@@ -626,11 +635,7 @@ def run_e2e(args, cfg, L, torch, world, dist):
         step()
     e1.record()
     torch.cuda.synchronize()
-    el = e0.elapsed_time(e1) / 1e3
-    if world > 1:
-        t = torch.tensor([el], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        el = float(t.item())
+    el = max_over_ranks(e0.elapsed_time(e1) / 1e3, world, "cuda")
     return {"value": world * args.steps / el, "unit": UNIT,
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
 

@@ -393,6 +393,54 @@ void lgh_server_destroy (lgh_server_t *server);
 int lgh_gram_noalloc (int64_t n, int w, const double *X, int64_t ldx,
                       double *G, int64_t ldg);
 
+/* ---- row-sharded operators (more than one GPU) -------------------------
+ * The reference distributes vectors and operators over MPI ranks in
+ * contiguous row slabs (MPIAIJ; docs/glr-woodbury-formulas.tex:76-98).  A
+ * shard plan is one rank's view of a symmetric CSR operator: its owned rows
+ * [row0, row1) (the even split r N / P), the remote rows its nonzeros
+ * reference (ghosts, ascending, counted per owner rank), and local column
+ * indices over an extended row-major block [owned rows; ghost rows].  The
+ * caller exchanges the ghost lists (an all-to-all) and registers each
+ * peer's requests with lgh_shard_set_sends; per application it packs each
+ * peer's rows, sends and receives the contiguous buffers with its own
+ * collective (NCCL / gloo) and unpacks them into the ghost rows.  Gram-type
+ * products are local products plus an all-reduce; the sketch of rows
+ * [i0, i0 + n) is lgh_sketch_rows, identical to those rows of the global
+ * sketch (partition-independent, glr_common_impl.h:55-58).             */
+typedef struct lgh_shard lgh_shard_t;
+
+void lgh_shard_range (int64_t N, int nranks, int rank, int64_t *row0,
+                      int64_t *row1);
+/* rowptr (row1 - row0 + 1 entries, rowptr[0] = 0) and colidx (global
+ * column indices) of this rank's rows; host arrays, copied.             */
+int lgh_shard_create (int64_t N, int nranks, int rank, const int64_t *rowptr,
+                      const int32_t *colidx, lgh_shard_t **shard);
+int lgh_shard_info (const lgh_shard_t *shard, int64_t *row0, int64_t *row1,
+                    int64_t *nghost);
+/* borrowed: ghost rows (nghost, ascending) and counts[nranks] per owner   */
+int lgh_shard_ghosts (const lgh_shard_t *shard, const int64_t **rows,
+                      const int64_t **counts);
+/* borrowed: local column indices (one per local nonzero)                 */
+int lgh_shard_local_colidx (const lgh_shard_t *shard, const int32_t **colidx);
+/* rows (global, owned here) that peer requested as its ghosts            */
+int lgh_shard_set_sends (lgh_shard_t *shard, int peer, int64_t count,
+                         const int64_t *rows);
+/* borrowed: the registered send rows for peer, as local row indices      */
+int lgh_shard_sends (const lgh_shard_t *shard, int peer, int64_t *count,
+                     const int64_t **local_rows);
+/* device: buf (count x w, contiguous) = the send rows of X for peer       */
+int lgh_shard_pack (lgh_shard_t *shard, int peer, int w, const double *X,
+                    int64_t ldx, double *buf);
+/* device: write peer's rows into the ghost rows of Xext (the rows after
+ * the nloc owned rows, in ghost order)                                    */
+int lgh_shard_unpack (const lgh_shard_t *shard, int peer, int w,
+                      const double *buf, double *Xext, int64_t ld);
+void lgh_shard_destroy (lgh_shard_t *shard);
+/* device: Y[i][j] = randn_at (seed, i0 + i, j0 + j), j < k; zero for
+ * k <= j < ld (row-major, leading dimension ld)                          */
+int lgh_sketch_rows (uint64_t seed, int64_t i0, int64_t n, int64_t j0, int k,
+                     double *Y, int64_t ld);
+
 /* Per-kernel CUDA-event timing of the hot kernels: switch on (1) / off (0)
  * (either resets the figures); read accumulated device milliseconds,
  * launches and algorithmic bytes of kernel id 0 k_pcg_pq, 1 k_pcg_upd,

@@ -204,6 +204,27 @@ SIGNATURES = {
                                        ctypes.POINTER(ctypes.c_double)]),
     "lgh_server_get_stats": (ctypes.c_int, [P, ctypes.POINTER(ServerStats)]),
     "lgh_server_destroy": (None, [P]),
+    "lgh_shard_range": (None, [I64, ctypes.c_int, ctypes.c_int,
+                               ctypes.POINTER(I64), ctypes.POINTER(I64)]),
+    "lgh_shard_create": (ctypes.c_int, [I64, ctypes.c_int, ctypes.c_int, P, P,
+                                        ctypes.POINTER(P)]),
+    "lgh_shard_info": (ctypes.c_int, [P, ctypes.POINTER(I64),
+                                      ctypes.POINTER(I64),
+                                      ctypes.POINTER(I64)]),
+    "lgh_shard_ghosts": (ctypes.c_int, [P, ctypes.POINTER(ctypes.POINTER(I64)),
+                                        ctypes.POINTER(ctypes.POINTER(I64))]),
+    "lgh_shard_local_colidx": (ctypes.c_int, [
+        P, ctypes.POINTER(ctypes.POINTER(ctypes.c_int32))]),
+    "lgh_shard_set_sends": (ctypes.c_int, [P, ctypes.c_int, I64, P]),
+    "lgh_shard_sends": (ctypes.c_int, [P, ctypes.c_int, ctypes.POINTER(I64),
+                                       ctypes.POINTER(ctypes.POINTER(I64))]),
+    "lgh_shard_pack": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, P, I64,
+                                      P]),
+    "lgh_shard_unpack": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, P, P,
+                                        I64]),
+    "lgh_shard_destroy": (None, [P]),
+    "lgh_sketch_rows": (ctypes.c_int, [ctypes.c_uint64, I64, I64, I64,
+                                       ctypes.c_int, P, I64]),
     "lgh_launch_count": (ctypes.c_long, []),
     "lgh_runtime_counters": (ctypes.c_int, [c_dbl_p]),
     "lgh_kernel_timing": (ctypes.c_int, [ctypes.c_int]),
@@ -586,6 +607,83 @@ def runtime_counters():
          "lgh_runtime_counters")
     return dict(allocs=int(out[0]), alloc_s=out[1], frees=int(out[2]),
                 free_s=out[3], launches=int(out[4]))
+
+
+def shard_range(N, nranks, rank):
+    a, b = I64(), I64()
+    load().lgh_shard_range(N, nranks, rank, ctypes.byref(a), ctypes.byref(b))
+    return a.value, b.value
+
+
+class Shard:
+    """One rank's row slab of a symmetric CSR operator (lgh_shard_*): the
+    host-side partition and halo plan.  csr: the global CSR dict
+    (rowptr, colidx[, vals]); only this rank's rows are handed over."""
+
+    def __init__(self, csr, nranks, rank):
+        L = load()
+        N = len(csr["rowptr"]) - 1
+        self.N, self.nranks, self.rank = N, nranks, rank
+        self.row0, self.row1 = shard_range(N, nranks, rank)
+        rp = np.ascontiguousarray(csr["rowptr"][self.row0:self.row1 + 1],
+                                  dtype=np.int64)
+        k0, k1 = int(rp[0]), int(rp[-1])
+        self.rowptr = rp - k0
+        self.colidx = np.ascontiguousarray(csr["colidx"][k0:k1],
+                                           dtype=np.int32)
+        self.vals = (np.ascontiguousarray(csr["vals"][k0:k1])
+                     if "vals" in csr else None)
+        self.h = P()
+        _chk(L.lgh_shard_create(N, nranks, rank, self.rowptr.ctypes.data,
+                                self.colidx.ctypes.data, ctypes.byref(self.h)),
+             "lgh_shard_create")
+
+    @property
+    def nloc(self):
+        return self.row1 - self.row0
+
+    def ghosts(self):
+        """(ghost rows ascending, counts per owner rank)"""
+        rows, counts = ctypes.POINTER(I64)(), ctypes.POINTER(I64)()
+        nl = I64()
+        _chk(load().lgh_shard_info(self.h, None, None, ctypes.byref(nl)),
+             "lgh_shard_info")
+        _chk(load().lgh_shard_ghosts(self.h, ctypes.byref(rows),
+                                     ctypes.byref(counts)), "lgh_shard_ghosts")
+        g = (np.ctypeslib.as_array(rows, shape=(nl.value,)).copy()
+             if nl.value else np.zeros(0, np.int64))
+        c = np.ctypeslib.as_array(counts, shape=(self.nranks,)).copy()
+        return g, c
+
+    def local_colidx(self):
+        p = ctypes.POINTER(ctypes.c_int32)()
+        _chk(load().lgh_shard_local_colidx(self.h, ctypes.byref(p)),
+             "lgh_shard_local_colidx")
+        n = len(self.colidx)
+        return (np.ctypeslib.as_array(p, shape=(n,)).copy() if n
+                else np.zeros(0, np.int32))
+
+    def set_sends(self, peer, rows):
+        rows = np.ascontiguousarray(rows, dtype=np.int64)
+        _chk(load().lgh_shard_set_sends(self.h, peer, len(rows),
+                                        rows.ctypes.data if len(rows) else None),
+             "lgh_shard_set_sends")
+
+    def sends(self, peer):
+        cnt = I64()
+        p = ctypes.POINTER(I64)()
+        _chk(load().lgh_shard_sends(self.h, peer, ctypes.byref(cnt),
+                                    ctypes.byref(p)), "lgh_shard_sends")
+        return (np.ctypeslib.as_array(p, shape=(cnt.value,)).copy()
+                if cnt.value else np.zeros(0, np.int64))
+
+    def close(self):
+        if _L is not None and getattr(self, "h", None):
+            _L.lgh_shard_destroy(self.h)
+            self.h = P()
+
+    def __del__(self):
+        self.close()
 
 
 class Server:
