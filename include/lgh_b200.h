@@ -49,6 +49,7 @@
 #define LGH_ERR_ARG_OUTOFRANGE   63  /* PETSC_ERR_ARG_OUTOFRANGE             */
 #define LGH_ERR_ARG_WRONGSTATE   73  /* PETSC_ERR_ARG_WRONGSTATE             */
 #define LGH_ERR_LIB              76  /* PETSC_ERR_LIB: factorisation failed  */
+#define LGH_ERR_CONV_FAILED      82  /* PETSC_ERR_CONV_FAILED                */
 #define LGH_ERR_ARG_NULL         85  /* PETSC_ERR_ARG_NULL                   */
 #define LGH_ERR_NOT_CONVERGED    91  /* PETSC_ERR_NOT_CONVERGED              */
 #define LGH_ERR_GPU              97  /* PETSC_ERR_GPU: CUDA runtime error    */
@@ -392,6 +393,80 @@ void lgh_server_destroy (lgh_server_t *server);
  * synchronises before returning.                                          */
 int lgh_gram_noalloc (int64_t n, int w, const double *X, int64_t ldx,
                       double *G, int64_t ldg);
+
+/* ---- stage 2.5: deflation correction against the true Hessian
+ * (glr.h:171-270).  The GLR object approximates the misfit Hessian; the
+ * correction measures the dominant modes of the whitened error operator
+ *   E_w = S^- (F_true + c0 I) S^- - I,  S^- = (U lam U^T + c0 I)^{-1/2},
+ *   F_true = M^{1/2} Z^{-1} H_d Z^{-T} M^{1/2},
+ * with the user's true-Hessian applies, and grafts a rank-r correction into
+ * (U, lam).  The corrected spectrum is SIGNED (never flipped); shift-taking
+ * operations then need c > floor = max(0, -min lam'); lgh_glr_apply serves
+ * the corrected low-rank action; lgh_glr_extend is refused afterwards.    */
+typedef struct lgh_glr_correct_opts
+{
+  double        c0;        /* reference shift of the error metric (1.0)   */
+  int           rank;      /* max correction rank; -1 (default) = all     */
+  int           applies;   /* true-Hessian apply budget (default 30)      */
+  int           n_qc;      /* probes path: trailing probes held out (0)   */
+  int           q_power;   /* fresh path: extra power passes (0)          */
+  double        clamp_eps; /* d clamped to >= -1 + clamp_eps (0.05)       */
+  double        d_keep_min;/* drop priced modes with |d| below this (0)   */
+  double        drop_tol;  /* relative basis drop tolerance (1e-12)       */
+  unsigned long seed;      /* fresh-path hashed sketch seed (424242)      */
+  int           verbose;
+}
+lgh_glr_correct_opts_t;
+
+lgh_glr_correct_opts_t lgh_glr_correct_opts_default (void);
+
+typedef struct lgh_glr_correct_report
+{
+  int    kept;             /* correction modes grafted                    */
+  int    basis;            /* error-basis dimension available             */
+  int    clamped;          /* Rayleigh values clamped at -1 + clamp_eps   */
+  int    hd_applies;       /* true-Hessian applies spent                  */
+  double d_min, d_max;     /* correction eigenvalues, post-clamp          */
+  double floor;            /* shift validity: ops need c > floor          */
+  double qc_before, qc_after;  /* whitened energy ratio on held-out
+                                  probes (n_qc > 0); -1 when unavailable  */
+  double t_operator, t_dense;
+}
+lgh_glr_correct_report_t;
+
+/* y = H_d x on HOST arrays of the N dofs (the reference's local arrays on
+ * one rank); the library copies each column to and from the device.     */
+#ifndef LGH_HESSIAN_FN_DEFINED
+#define LGH_HESSIAN_FN_DEFINED
+typedef void (*lgh_hessian_fn) (const double *in_local, double *out_local,
+                                void *ctx);
+#endif
+
+/* Value-pass correction from k probe pairs (host, column-major: V[j*N + i]
+ * entry i of probe j, HV the true-Hessian responses); the apply budget
+ * prices the top error-basis directions exactly.                         */
+int lgh_glr_correct_probes (lgh_glr_t *glr, int k, const double *V,
+                            const double *HV, lgh_hessian_fn hessian_apply,
+                            void *ctx, const lgh_glr_correct_opts_t *opts,
+                            lgh_glr_correct_report_t *report);
+/* Fresh randomized correction: a hashed Gaussian sketch of E_w.          */
+int lgh_glr_correct (lgh_glr_t *glr, lgh_hessian_fn hessian_apply, void *ctx,
+                     const lgh_glr_correct_opts_t *opts,
+                     lgh_glr_correct_report_t *report);
+
+/* ---- persistence ---------------------------------------------------------
+ * Save a built object's spectrum and U (and, with with_extension = 1, the
+ * sketch basis and raw projection that lgh_glr_extend continues from) to a
+ * file, and restore it against the same B and prior without a rebuild: a
+ * restarted serving process, or another process, serves the same model.
+ * The reference keeps this state in memory only; the file format is this
+ * library's (little-endian, checksummed).  lgh_glr_load checks the size
+ * and the checksum (LGH_ERR_ARG_SIZ / LGH_ERR_ARG_WRONG); an object loaded
+ * without extension state returns LGH_ERR_ARG_WRONGSTATE from an
+ * incremental extend.                                                     */
+int lgh_glr_save (const lgh_glr_t *glr, const char *path, int with_extension);
+int lgh_glr_load (lgh_Mat B, lgh_prior_t *prior, const char *path,
+                  lgh_glr_t **glr);
 
 /* ---- row-sharded operators (more than one GPU) -------------------------
  * The reference distributes vectors and operators over MPI ranks in

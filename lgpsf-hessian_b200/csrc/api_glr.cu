@@ -825,9 +825,10 @@ lgh_glr_solve (lgh_glr_t *glr, double c, lgh_Vec rhs, lgh_Vec x)
 int
 lgh_glr_apply (lgh_glr_t *glr, double c, lgh_Vec v, lgh_Vec y)
 {
-  /* exact y = B v + c R v (glr_common_impl.h:1026-1048); the corrected
-   * low-rank branch needs lgh_glr_correct, which this library omits */
+  /* exact y = B v + c R v (glr_common_impl.h:1026-1048); after a
+   * correction the corrected low-rank action (correct.cu) */
   LGH_TRY (check_vecs (glr, v, y, "lgh_glr_apply"));
+  if (glr->corrected) return glr_apply_corrected (glr, c, v->d, y->d);
   LGH_TRY (glr_scratch (glr));
   lgh_prior_t *p = glr->prior;
   cudaStream_t s = stream ();

@@ -72,8 +72,8 @@ struct lgh_glr
   lgh::DBuf<double> Q, A;
   lgh::DBuf<float> Q32;
   int ldq = 4, ell = 0;
-  /* deflation-correction state of the reference (never set here: the
-   * correction stage is not part of this library) */
+  /* deflation-correction state (correct.cu): U, lam are the corrected,
+   * signed model; shifts need c > floor */
   int corrected = 0;
   double floor = 0.;
   /* scratch */
@@ -103,6 +103,7 @@ int prior_solve_rows (lgh_prior_t *p, int w, const T *X, int ldx,
 int prior_solve_pc32 (lgh_prior_t *p, int w, const double *X, int ldx,
                       const double *s_in, double *Y, int ldy,
                       const double *s_out, double rtol_override = 0.);
+int glr_apply_corrected (lgh_glr_t *g, double c, const double *v, double *y);
 int launch_vec_div (int64_t n, const double *x, const double *d, double *y,
                     cudaStream_t s);
 }

@@ -25,7 +25,8 @@ PC_AMG, PC_JACOBI = 0, 1
 ERR_NAMES = {0: "SUCCESS", 55: "ERR_MEM", 56: "ERR_SUP", 58: "ERR_ORDER",
              60: "ERR_ARG_SIZ", 62: "ERR_ARG_WRONG",
              63: "ERR_ARG_OUTOFRANGE", 73: "ERR_ARG_WRONGSTATE",
-             76: "ERR_LIB", 85: "ERR_ARG_NULL", 91: "ERR_NOT_CONVERGED",
+             76: "ERR_LIB", 82: "ERR_CONV_FAILED", 85: "ERR_ARG_NULL",
+             91: "ERR_NOT_CONVERGED",
              97: "ERR_GPU"}
 
 
@@ -110,6 +111,33 @@ class GlrStats(ctypes.Structure):
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
+
+class CorrectOpts(ctypes.Structure):
+    """lgh_glr_correct_opts_t (include/lgpsf_hessian/glr.h:200-225)."""
+
+    _fields_ = [("c0", ctypes.c_double), ("rank", ctypes.c_int),
+                ("applies", ctypes.c_int), ("n_qc", ctypes.c_int),
+                ("q_power", ctypes.c_int), ("clamp_eps", ctypes.c_double),
+                ("d_keep_min", ctypes.c_double), ("drop_tol", ctypes.c_double),
+                ("seed", ctypes.c_ulong), ("verbose", ctypes.c_int)]
+
+
+class CorrectReport(ctypes.Structure):
+    """lgh_glr_correct_report_t (include/lgpsf_hessian/glr.h:229-242)."""
+
+    _fields_ = [("kept", ctypes.c_int), ("basis", ctypes.c_int),
+                ("clamped", ctypes.c_int), ("hd_applies", ctypes.c_int),
+                ("d_min", ctypes.c_double), ("d_max", ctypes.c_double),
+                ("floor", ctypes.c_double), ("qc_before", ctypes.c_double),
+                ("qc_after", ctypes.c_double), ("t_operator", ctypes.c_double),
+                ("t_dense", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+HESS_FN = ctypes.CFUNCTYPE(None, ctypes.POINTER(ctypes.c_double),
+                           ctypes.POINTER(ctypes.c_double), P)
 
 VEC_FN = ctypes.CFUNCTYPE(None, P, P, P)
 MAT_FN = ctypes.CFUNCTYPE(None, P, P, P)
@@ -204,6 +232,15 @@ SIGNATURES = {
                                        ctypes.POINTER(ctypes.c_double)]),
     "lgh_server_get_stats": (ctypes.c_int, [P, ctypes.POINTER(ServerStats)]),
     "lgh_server_destroy": (None, [P]),
+    "lgh_glr_correct_opts_default": (CorrectOpts, []),
+    "lgh_glr_correct_probes": (ctypes.c_int, [P, ctypes.c_int, P, P, HESS_FN,
+                                              P, ctypes.POINTER(CorrectOpts),
+                                              ctypes.POINTER(CorrectReport)]),
+    "lgh_glr_correct": (ctypes.c_int, [P, HESS_FN, P,
+                                       ctypes.POINTER(CorrectOpts),
+                                       ctypes.POINTER(CorrectReport)]),
+    "lgh_glr_save": (ctypes.c_int, [P, ctypes.c_char_p, ctypes.c_int]),
+    "lgh_glr_load": (ctypes.c_int, [P, P, ctypes.c_char_p, ctypes.POINTER(P)]),
     "lgh_shard_range": (None, [I64, ctypes.c_int, ctypes.c_int,
                                ctypes.POINTER(I64), ctypes.POINTER(I64)]),
     "lgh_shard_create": (ctypes.c_int, [I64, ctypes.c_int, ctypes.c_int, P, P,
@@ -489,6 +526,55 @@ class Glr:
         self.report = rep.as_dict()
         self.n = prior.n
 
+    @staticmethod
+    def _hess(fn, n):
+        def cb(xin, xout, ctx):
+            x = np.ctypeslib.as_array(xin, shape=(n,))
+            y = np.ctypeslib.as_array(xout, shape=(n,))
+            y[:] = fn(x.copy())
+        return HESS_FN(cb)
+
+    def correct_probes(self, V, HV, hessian, opts=None):
+        """Value-pass deflation correction from probe pairs (N x k host
+        arrays) and a true-Hessian callable x -> H_d x (host arrays)."""
+        L = load()
+        o = opts if opts is not None else L.lgh_glr_correct_opts_default()
+        Vf = np.asfortranarray(V, dtype=np.float64)
+        HVf = np.asfortranarray(HV, dtype=np.float64)
+        cb = self._hess(hessian, self.n)
+        rep = CorrectReport()
+        _chk(L.lgh_glr_correct_probes(self.h, Vf.shape[1], Vf.ctypes.data,
+                                      HVf.ctypes.data, cb, None,
+                                      ctypes.byref(o), ctypes.byref(rep)),
+             "lgh_glr_correct_probes")
+        return rep.as_dict()
+
+    def correct(self, hessian, opts=None):
+        """Fresh randomized deflation correction."""
+        L = load()
+        o = opts if opts is not None else L.lgh_glr_correct_opts_default()
+        cb = self._hess(hessian, self.n)
+        rep = CorrectReport()
+        _chk(L.lgh_glr_correct(self.h, cb, None, ctypes.byref(o),
+                               ctypes.byref(rep)), "lgh_glr_correct")
+        return rep.as_dict()
+
+    def save(self, path, with_extension=False):
+        _chk(load().lgh_glr_save(self.h, str(path).encode(),
+                                 1 if with_extension else 0), "lgh_glr_save")
+
+    @classmethod
+    def load(cls, B, prior, path):
+        """Restore a saved object against the same B and prior."""
+        g = cls.__new__(cls)
+        g.h = P()
+        g.B, g.prior = B, prior
+        _chk(load().lgh_glr_load(B.h, prior.h, str(path).encode(),
+                                 ctypes.byref(g.h)), "lgh_glr_load")
+        g.report = {}
+        g.n = prior.n
+        return g
+
     def extend(self, k):
         rep = GlrReport()
         _chk(load().lgh_glr_extend(self.h, int(k), ctypes.byref(rep)),
@@ -607,6 +693,13 @@ def runtime_counters():
          "lgh_runtime_counters")
     return dict(allocs=int(out[0]), alloc_s=out[1], frees=int(out[2]),
                 free_s=out[3], launches=int(out[4]))
+
+
+def correct_opts(**kw):
+    o = load().lgh_glr_correct_opts_default()
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
 
 
 def shard_range(N, nranks, rank):

@@ -90,6 +90,50 @@ def test_prior_mat_problem(grid_m=24, rank=6):
 # CSR helpers
 
 
+def test_deflate_problem(err_scale=1.0, n=120, rank_b=10, rank_c=4):
+    """The closed-form problem of the reference's deflation gates
+    (tests/test_deflate.cpp:43-100): B SPD of exact rank 10, diagonal Z and
+    mass, a true Hessian H_d = B + DH with a planted signed error of exact
+    rank 4 (err_scale blows up the leading negative mode), deterministic
+    probes, and the dense oracle of F_true = whiten(H_d), signed,
+    |lambda|-descending."""
+    i = np.arange(n)
+
+    def factor(k):
+        return np.sin(0.1 * (i + 1) * (k + 3)) + 0.2 * np.cos(0.37 * i * k + k)
+
+    def perr(k):
+        return np.cos(0.21 * (i + 2) * (k + 1)) + 0.3 * np.sin(0.4 * i - k)
+
+    def terr(k):
+        t = 0.08 / (k + 1.0) * (-1.0 if k % 2 else 1.0)
+        return t * err_scale if k == 1 else t
+
+    Bd = np.zeros((n, n))
+    for k in range(rank_b):
+        a = factor(k)
+        Bd += 2.0 / (k + 1.0) * np.outer(a, a)
+    Hd = Bd.copy()
+    for k in range(rank_c):
+        p = perr(k)
+        Hd += terr(k) * np.outer(p, p)
+    z = 1.0 + 0.01 * i
+    m = 0.5 + 0.1 * (i % 7)
+    w = np.sqrt(m) / z
+    F = w[:, None] * Hd * w[None, :]
+    ev = np.linalg.eigvalsh(F)
+    ev = ev[np.argsort(-np.abs(ev), kind="stable")]
+
+    def probes(k):
+        jj = np.arange(k)
+        return (np.sin(0.03 * (i[:, None] + 1) * (jj[None, :] + 2))
+                + 0.1 * np.cos(0.7 * i[:, None] - 1.3 * jj[None, :]))
+
+    return dict(n=n, B_dense=Bd, Hd=Hd, zdiag=z, mass=m, oracle=ev,
+                probe_vec=np.cos(0.05 * i + 1.0), probes=probes,
+                rank_b=rank_b, rank_c=rank_c)
+
+
 def coo_to_csr(n, rows, cols, vals):
     order = np.lexsort((cols, rows))
     rows, cols, vals = rows[order], cols[order], vals[order]

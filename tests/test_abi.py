@@ -49,7 +49,11 @@ def test_struct_layouts_match_c_compiler(tmp_path):
                "lgh_prior_mat_opts_t": lgh_b200.PriorMatOpts,
                "lgh_exec_opts_t": lgh_b200.ExecOpts,
                "lgh_glr_stats_t": lgh_b200.GlrStats,
-               "lgh_prior_callbacks_t": lgh_b200.PriorCallbacks}
+               "lgh_prior_callbacks_t": lgh_b200.PriorCallbacks,
+               "lgh_glr_correct_opts_t": lgh_b200.CorrectOpts,
+               "lgh_glr_correct_report_t": lgh_b200.CorrectReport,
+               "lgh_server_opts_t": lgh_b200.ServerOpts,
+               "lgh_server_stats_t": lgh_b200.ServerStats}
     lines = ['#include <stdio.h>', '#include <stddef.h>',
              '#include "lgh_b200.h"', 'int main(void){']
     for cname, py in structs.items():
