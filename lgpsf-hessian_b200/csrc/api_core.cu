@@ -101,11 +101,88 @@ rt_add (double &sec, long &cnt, double dt)
   cnt++;
 }
 
+/* ---- device memory: a caching allocator -----------------------------------
+ * cudaFree synchronises the whole device and, for the build's 0.5 GB
+ * blocks, took up to 50 ms apiece on some hosts; a job frees ~30 blocks.
+ * Freed blocks therefore go to a cache keyed by size, with an event
+ * recorded on the library stream after the free; an allocation takes the
+ * smallest cached block of at least its size (and at most twice it), after
+ * the host has waited for that block's event, so no work still using the
+ * block can overlap its next owner on any stream.  The cache keeps at most
+ * a third of the device's memory; when cudaMalloc runs out, the cache is
+ * released and the allocation retried.  Sizes are rounded up to 2 MiB
+ * above 4 MiB (256 B below) so that repeated shapes reuse blocks. */
+
+namespace
+{
+struct CachedBlock
+{
+  void *p;
+  size_t bytes;
+  cudaEvent_t ev;
+};
+std::mutex g_pool_mu;
+std::multimap<size_t, CachedBlock> g_pool;
+std::map<void *, size_t> g_live;     /* allocated block -> rounded size */
+size_t g_pool_bytes = 0, g_pool_cap = 0;
+
+size_t
+pool_round (size_t b)
+{
+  if (b == 0) b = 256;
+  if (b > ((size_t) 4 << 20)) return (b + ((size_t) 2 << 20) - 1) & ~(((size_t) 2 << 20) - 1);
+  return (b + 255) & ~(size_t) 255;
+}
+
+void
+pool_release_all ()
+{
+  /* caller holds g_pool_mu */
+  for (auto &kv : g_pool) {
+    cudaEventSynchronize (kv.second.ev);
+    cudaEventDestroy (kv.second.ev);
+    cudaFree (kv.second.p);
+  }
+  g_pool.clear ();
+  g_pool_bytes = 0;
+}
+} /* namespace */
+
 int
 dalloc (void **p, size_t bytes)
 {
   const double t0 = wall ();
-  cudaError_t e = cudaMalloc (p, bytes ? bytes : 256);
+  const size_t rb = pool_round (bytes);
+  *p = nullptr;
+  {
+    std::lock_guard<std::mutex> lk (g_pool_mu);
+    auto it = g_pool.lower_bound (rb);
+    if (it != g_pool.end () && it->first <= 2 * rb) {
+      CachedBlock b = it->second;
+      g_pool.erase (it);
+      g_pool_bytes -= b.bytes;
+      cudaEventSynchronize (b.ev);
+      cudaEventDestroy (b.ev);
+      g_live[b.p] = b.bytes;
+      *p = b.p;
+    }
+  }
+  cudaError_t e = cudaSuccess;
+  if (*p == nullptr) {
+    e = cudaMalloc (p, rb);
+    if (e == cudaErrorMemoryAllocation) {
+      cudaGetLastError ();
+      {
+        std::lock_guard<std::mutex> lk (g_pool_mu);
+        pool_release_all ();
+      }
+      e = cudaMalloc (p, rb);
+    }
+    if (e == cudaSuccess) {
+      std::lock_guard<std::mutex> lk (g_pool_mu);
+      g_live[*p] = rb;
+    }
+  }
   rt_add (g_rt.alloc_s, g_rt.allocs, wall () - t0);
   if (e != cudaSuccess) {
     *p = nullptr;
@@ -121,7 +198,29 @@ dfree (void *p)
 {
   if (!p) return;
   const double t0 = wall ();
-  cudaFree (p);
+  std::lock_guard<std::mutex> lk (g_pool_mu);
+  auto it = g_live.find (p);
+  size_t bytes = 0;
+  if (it != g_live.end ()) {
+    bytes = it->second;
+    g_live.erase (it);
+  }
+  if (g_pool_cap == 0) {
+    size_t fb = 0, tb = 0;
+    if (cudaMemGetInfo (&fb, &tb) == cudaSuccess) g_pool_cap = tb / 3;
+    else cudaGetLastError ();
+  }
+  cudaEvent_t ev = nullptr;
+  if (bytes == 0 || g_pool_bytes + bytes > g_pool_cap
+      || cudaEventCreateWithFlags (&ev, cudaEventDisableTiming) != cudaSuccess
+      || cudaEventRecord (ev, stream ()) != cudaSuccess) {
+    if (ev) cudaEventDestroy (ev);
+    cudaGetLastError ();
+    cudaFree (p);
+  } else {
+    g_pool.insert ({ bytes, CachedBlock{ p, bytes, ev } });
+    g_pool_bytes += bytes;
+  }
   rt_add (g_rt.free_s, g_rt.frees, wall () - t0);
 }
 
