@@ -65,7 +65,9 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=20.0)
     ap.add_argument("--serve-s", type=float, default=5.0)
     ap.add_argument("--no-mixed", action="store_true")
-    ap.add_argument("--config", default="c2", choices=["c2", "c3", "c4"],
+    ap.add_argument("--serve-rates", default="",
+                    help="comma-separated request rates for --config c5")
+    ap.add_argument("--config", default="c2", choices=["c2", "c3", "c4", "c5"],
                     help="c2: the headline job (default); c3 / c4: the "
                          "mixed-precision 3D extend and the batched-shift "
                          "workloads, one JSON line each")
@@ -516,14 +518,15 @@ def run_mixed_job(args, B, pr, opts, N, g64, rhs, xout, L, torch):
     return out
 
 
-def run_serving(args, g, N, L):
+def run_serving(args, g, N, L, rate=None, window=None, slots=64):
     """Continuous batching through the request loop (lgh_server_*) on the
     built object: a seeded Poisson stream at --serve-rate requests/s for
     --serve-s seconds, 60/30/10 solve/sample/logdet, m ~ U{1..64} columns,
     shifts log-uniform in [1e-3, 1e3]; submit-to-done latency per request
     and completed columns per second (first submit to last completion)."""
     rng = np.random.default_rng(2024)
-    rate, window = args.serve_rate, args.serve_s
+    rate = args.serve_rate if rate is None else rate
+    window = args.serve_s if window is None else window
     t, arrivals = 0.0, []
     while True:
         t += rng.exponential(1.0 / rate)
@@ -536,7 +539,7 @@ def run_serving(args, g, N, L):
         arrivals.append((t, kind, m, c))
     mmax = max(m for _, k, m, _ in arrivals if k != 2)
     pool = np.asfortranarray(rng.standard_normal((N, mmax)))
-    sv = L.Server(g, slots=64)
+    sv = L.Server(g, slots=slots)
     ids = []
     t0 = time.perf_counter()
     for ta, kind, m, c in arrivals:
@@ -553,7 +556,7 @@ def run_serving(args, g, N, L):
     lat.sort()
     cols = sum(m for _, k, m, _ in arrivals if k != 2)
     return {"requests": len(arrivals), "offered_per_s": rate,
-            "window_s": window, "slots": 64, "columns": cols,
+            "window_s": window, "slots": slots, "columns": cols,
             "columns_per_s": cols / (t1 - t0),
             "p50_ms": 1e3 * lat[len(lat) // 2],
             "p99_ms": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))],
@@ -760,6 +763,50 @@ def run_c4(args):
     return 0
 
 
+def run_c5(args):
+    """Config 5: 128^3 3D grid (N = 2097152), Z = h L + 16 M, B Gaussian
+    (0.01) x Wendland (0.02); GLR rank 500 (ell 520, rank cap 500) built in
+    mixed precision and kept resident; then seeded Poisson request streams
+    (60/30/10 solve/sample/logdet, m ~ U{1..64}, c log-uniform in
+    [1e-3, 1e3]) through the request loop at each rate of --serve-rates;
+    p50 / p99 latency and completed columns per second.  One JSON line."""
+    import torch
+    import lgh_b200 as L
+    from lgh_b200 import problems as P
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    cfg = P.grid_problem("c5")
+    t_gen = time.perf_counter() - t0
+    N = cfg["N"]
+    B, Z = L.Mat(cfg["B"]), L.Mat(cfg["Z"])
+    pr = L.Prior(Z=Z, mass=cfg["mass"], opts=L.prior_opts(ksp_rtol=ZRTOL))
+    ex = L.exec_opts(precision=L.PREC_MIXED, rank_cap=500)
+    ev = _events(torch, 2)
+    ev[0].record()
+    g = L.Glr(B, pr, L.glr_opts(ell=520, q_power=1, seed=SEED,
+                                trunc_rel=0.0, check=0), exec=ex)
+    ev[1].record()
+    torch.cuda.synchronize()
+    build_s = ev[0].elapsed_time(ev[1]) / 1e3
+    rates = [float(r) for r in (args.serve_rates or "2,5,10").split(",")]
+    sweep = [run_serving(args, g, N, L, rate=r, window=args.serve_s)
+             for r in rates]
+    line = {"metric": "served columns/s and p50/p99 request latency",
+            "value": max(x["columns_per_s"] for x in sweep),
+            "unit": "columns/s", "higher_is_better": True, "n_gpus": 1,
+            "dtype": "f32 blocks / f64 core (mixed)",
+            "data": "synthetic (config formulas)",
+            "config": {"workload": "c5: 128^3 3D grid (N=%d), B %.1f nnz/row, "
+                                   "ell 520 (rank 500), Poisson request "
+                                   "streams at %s requests/s" % (
+                                       N, cfg["nnz_B"] / N, rates),
+                       "N": N, "nnz_B": cfg["nnz_B"]},
+            "generate_s": t_gen, "build_s": build_s,
+            "kept": int(len(g.eigs())), "sweep": sweep}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.warmup < 3:
@@ -770,6 +817,8 @@ def main():
         return run_c3(args)
     if args.config == "c4":
         return run_c4(args)
+    if args.config == "c5":
+        return run_c5(args)
     return run_ours(args)
 
 

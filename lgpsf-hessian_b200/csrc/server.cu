@@ -227,6 +227,7 @@ struct lgh_server
   std::vector<lgh::Slot> slots;
   lgh::DBuf<int> fresh_d;
   std::vector<int> fresh_h;
+  int *fresh_pin = nullptr, *act_pin = nullptr;   /* pinned per-tick copies */
   lgh::DBuf<double> H, coef, gemmwork, ldc, ldo;
   lgh::DBuf<char> hv_d;
   std::unique_ptr<lgh::Harvest> hv;
@@ -461,6 +462,27 @@ srv_loop (lgh_server_t *sv)
     return;
   }
   std::vector<int> act (sv->cap);
+  /* one PCG tick over the slot block for a given pair of direction
+   * buffers; after two eager ticks (which set up the V-cycle buffers and
+   * the launch-shape caches) each parity is captured into a CUDA graph
+   * once and replayed, so a tick costs one graph launch on the host */
+  auto tick = [&] (double *Po, double *Pn) -> int {
+    if (p->mg)
+      LGH_TRY (mg_vcycle<double> (p->mg, R, Zb, ld, sv->cap, s, nullptr, &sv->mgw));
+    else
+      LGH_TRY (launch_rowscale<double> (n, ld, p->Z->csr.dinv, R, ld, Zb, ld, s));
+    LGH_TRY (server_tick_dots<double> (p->Z->csr, R, Zb, ld, sv->cap, sv->fresh_d.p,
+                                       p->zcfg.rtol, sv->ws, s));
+    LGH_TRY (server_tick_pq<double> (p->Z->csr, Zb, Po, Pn, Q, ld, sv->ws, s));
+    return server_tick_upd<double> (n, ld, X, R, Pn, Q, sv->ws, s);
+  };
+  cudaGraphExec_t gexec[2] = { nullptr, nullptr };
+  bool graphs_off = false;
+  int parity = 0;   /* 0: the old direction is in P0 */
+  auto release_graphs = [&] () {
+    for (auto &ge : gexec)
+      if (ge) { cudaGraphExecDestroy (ge); ge = nullptr; }
+  };
   while (!sv->stop.load ()) {
     /* 1. admission into free slots */
     std::vector<SReq *> adm;
@@ -469,7 +491,7 @@ srv_loop (lgh_server_t *sv)
       rc = (r->kind == 2) ? srv_logdet (sv, r) : srv_start (sv, r, Pold);
       if (rc) break;
     }
-    if (rc) { srv_fail (sv, rc); return; }
+    if (rc) { release_graphs (); srv_fail (sv, rc); return; }
     bool any = false;
     for (auto &sl : sv->slots) any |= sl.req != nullptr;
     if (!any) {
@@ -480,30 +502,52 @@ srv_loop (lgh_server_t *sv)
     }
     /* 2. one PCG tick over the whole slot block: preconditioner, dots
      *    (fresh columns start there), direction + Z product, update */
-    if (cudaMemcpyAsync (sv->fresh_d.p, sv->fresh_h.data (), sv->cap * sizeof (int),
+    memcpy (sv->fresh_pin, sv->fresh_h.data (), sv->cap * sizeof (int));
+    if (cudaMemcpyAsync (sv->fresh_d.p, sv->fresh_pin, sv->cap * sizeof (int),
                          cudaMemcpyHostToDevice, s) != cudaSuccess)
       rc = set_error (LGH_ERR_GPU, "server: fresh flags");
-    if (!rc) {
-      if (p->mg) rc = mg_vcycle<double> (p->mg, R, Zb, ld, sv->cap, s, nullptr,
-                                         &sv->mgw);
-      else rc = launch_rowscale<double> (n, ld, p->Z->csr.dinv, R, ld, Zb, ld, s);
+    if (!rc && !graphs_off && sv->ticks >= 2 && gexec[parity] == nullptr) {
+      cudaGraph_t gr = nullptr;
+      if (cudaStreamBeginCapture (s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        const int crc = tick (Pold, Pnew);
+        const cudaError_t ce = cudaStreamEndCapture (s, &gr);
+        if (crc != 0 || ce != cudaSuccess || gr == nullptr
+            || cudaGraphInstantiate (&gexec[parity], gr, 0) != cudaSuccess) {
+          gexec[parity] = nullptr;
+          graphs_off = true;     /* keep ticking eagerly */
+        }
+        if (gr) cudaGraphDestroy (gr);
+      } else {
+        graphs_off = true;
+      }
+      cudaGetLastError ();
+      clear_error ();
     }
-    if (!rc) rc = server_tick_dots<double> (p->Z->csr, R, Zb, ld, sv->cap,
-                                            sv->fresh_d.p, p->zcfg.rtol, sv->ws, s);
-    if (!rc) rc = server_tick_pq<double> (p->Z->csr, Zb, Pold, Pnew, Q, ld, sv->ws, s);
-    if (!rc) rc = server_tick_upd<double> (n, ld, X, R, Pnew, Q, sv->ws, s);
+    if (!rc) {
+      if (gexec[parity]) {
+        if (cudaGraphLaunch (gexec[parity], s) != cudaSuccess)
+          rc = set_error (LGH_ERR_GPU, "server: tick graph launch");
+      } else {
+        rc = tick (Pold, Pnew);
+      }
+    }
     std::swap (Pold, Pnew);
+    parity ^= 1;
     std::fill (sv->fresh_h.begin (), sv->fresh_h.end (), 0);
     sv->ticks++;
     /* 3. harvest converged columns */
-    if (!rc && cudaMemcpyAsync (act.data (), sv->ws.ival.p, sv->cap * sizeof (int),
+    if (!rc && cudaMemcpyAsync (sv->act_pin, sv->ws.ival.p, sv->cap * sizeof (int),
                                 cudaMemcpyDeviceToHost, s) != cudaSuccess)
       rc = set_error (LGH_ERR_GPU, "server: mask copy");
     if (!rc && cudaStreamSynchronize (s) != cudaSuccess)
       rc = set_error (LGH_ERR_GPU, "server: tick");
-    if (!rc) rc = srv_harvest (sv, act, Pold);
-    if (rc) { srv_fail (sv, rc); return; }
+    if (!rc) {
+      memcpy (act.data (), sv->act_pin, sv->cap * sizeof (int));
+      rc = srv_harvest (sv, act, Pold);
+    }
+    if (rc) { release_graphs (); srv_fail (sv, rc); return; }
   }
+  release_graphs ();
 }
 
 } /* namespace lgh */
@@ -553,10 +597,15 @@ lgh_server_create (lgh_glr_t *glr, const lgh_server_opts_t *opts,
   if (!rc) rc = sv->ldc.alloc (1);
   if (!rc) rc = sv->ldo.alloc (1);
   if (!rc) rc = sv->hv_d.alloc (sizeof (Harvest));
+  if (!rc && (cudaMallocHost ((void **) &sv->fresh_pin, sv->ld * sizeof (int)) != cudaSuccess
+              || cudaMallocHost ((void **) &sv->act_pin, sv->ld * sizeof (int)) != cudaSuccess))
+    rc = set_error (LGH_ERR_MEM, "lgh_server_create: pinned buffers");
   if (!rc) rc = cudaDeviceSynchronize () == cudaSuccess ? 0
                 : set_error (LGH_ERR_GPU, "lgh_server_create: set-up");
   if (rc) {
     if (sv->s) cudaStreamDestroy (sv->s);
+    if (sv->fresh_pin) cudaFreeHost (sv->fresh_pin);
+    if (sv->act_pin) cudaFreeHost (sv->act_pin);
     delete sv;
     return rc;
   }
@@ -656,6 +705,8 @@ lgh_server_destroy (lgh_server_t *sv)
   sv->cv.notify_all ();
   if (sv->worker.joinable ()) sv->worker.join ();
   if (sv->s) cudaStreamDestroy (sv->s);
+  if (sv->fresh_pin) cudaFreeHost (sv->fresh_pin);
+  if (sv->act_pin) cudaFreeHost (sv->act_pin);
   delete sv;
 }
 
