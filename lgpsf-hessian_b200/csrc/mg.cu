@@ -24,6 +24,8 @@
 #include <math.h>
 #include <string.h>
 
+#include <omp.h>
+
 #include <algorithm>
 #include <type_traits>
 #include <vector>
@@ -54,15 +56,38 @@ hcsr_diag (const HCsr &A, int64_t i)
   return 0.;
 }
 
+/* The host set-up runs its row loops on all host threads (OpenMP); every
+ * reduction sums fixed row blocks in a fixed order, so the hierarchy is
+ * the same bits whatever the thread count. */
 static void
 hcsr_mult (const HCsr &A, const std::vector<double> &x, std::vector<double> &y)
 {
   y.assign (A.n, 0.);
+#pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < A.n; i++) {
     double s = 0.;
     for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++) s += A.v[k] * x[A.ci[k]];
     y[i] = s;
   }
+}
+
+/* sum_i a_i b_i over 256 fixed row blocks, combined in order */
+static double
+hdot (const std::vector<double> &a, const std::vector<double> &b)
+{
+  const int64_t n = (int64_t) a.size ();
+  constexpr int NB = 256;
+  double part[NB];
+#pragma omp parallel for schedule(static)
+  for (int blk = 0; blk < NB; blk++) {
+    const int64_t i0 = n * blk / NB, i1 = n * (blk + 1) / NB;
+    double s = 0.;
+    for (int64_t i = i0; i < i1; i++) s += a[i] * b[i];
+    part[blk] = s;
+  }
+  double s = 0.;
+  for (int blk = 0; blk < NB; blk++) s += part[blk];
+  return s;
 }
 
 static HCsr
@@ -86,7 +111,8 @@ hcsr_transpose (const HCsr &A)
   return T;
 }
 
-/* C = A B (Gustavson, dense accumulator), columns sorted per row */
+/* C = A B (Gustavson, dense accumulator), columns sorted per row; row
+ * chunks in parallel, each with its own accumulator, then concatenated */
 static HCsr
 hcsr_gemm (const HCsr &A, const HCsr &B)
 {
@@ -94,29 +120,51 @@ hcsr_gemm (const HCsr &A, const HCsr &B)
   C.n = A.n;
   C.m = B.m;
   C.rp.assign (C.n + 1, 0);
-  std::vector<double> acc (B.m, 0.);
-  std::vector<int32_t> mark (B.m, -1), cols;
-  for (int64_t i = 0; i < A.n; i++) {
-    cols.clear ();
-    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++) {
-      const int64_t j = A.ci[k];
-      const double a = A.v[k];
-      for (int64_t q = B.rp[j]; q < B.rp[j + 1]; q++) {
-        const int32_t c = B.ci[q];
-        if (mark[c] != (int32_t) i) {
-          mark[c] = (int32_t) i;
-          acc[c] = 0.;
-          cols.push_back (c);
+  const int nt = std::max (1, std::min (omp_get_max_threads (), 64));
+  const int nchunk = (int) std::min<int64_t> (std::max<int64_t> (A.n, 1), 4 * nt);
+  std::vector<std::vector<int32_t>> cci (nchunk);
+  std::vector<std::vector<double>> cv (nchunk);
+  std::vector<std::vector<int64_t>> crn (nchunk);
+#pragma omp parallel num_threads(nt)
+  {
+    std::vector<double> acc (B.m, 0.);
+    std::vector<int64_t> mark (B.m, -1);
+    std::vector<int32_t> cols;
+#pragma omp for schedule(dynamic, 1)
+    for (int ch = 0; ch < nchunk; ch++) {
+      const int64_t r0 = A.n * ch / nchunk, r1 = A.n * (ch + 1) / nchunk;
+      for (int64_t i = r0; i < r1; i++) {
+        cols.clear ();
+        for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++) {
+          const int64_t j = A.ci[k];
+          const double a = A.v[k];
+          for (int64_t q = B.rp[j]; q < B.rp[j + 1]; q++) {
+            const int32_t c = B.ci[q];
+            if (mark[c] != i) {
+              mark[c] = i;
+              acc[c] = 0.;
+              cols.push_back (c);
+            }
+            acc[c] += a * B.v[q];
+          }
         }
-        acc[c] += a * B.v[q];
+        std::sort (cols.begin (), cols.end ());
+        for (int32_t c : cols) {
+          cci[ch].push_back (c);
+          cv[ch].push_back (acc[c]);
+        }
+        crn[ch].push_back ((int64_t) cols.size ());
       }
     }
-    std::sort (cols.begin (), cols.end ());
-    for (int32_t c : cols) {
-      C.ci.push_back (c);
-      C.v.push_back (acc[c]);
+  }
+  int64_t i = 0;
+  for (int ch = 0; ch < nchunk; ch++) {
+    for (int64_t cnt : crn[ch]) {
+      C.rp[i + 1] = C.rp[i] + cnt;
+      i++;
     }
-    C.rp[i + 1] = (int64_t) C.ci.size ();
+    C.ci.insert (C.ci.end (), cci[ch].begin (), cci[ch].end ());
+    C.v.insert (C.v.end (), cv[ch].begin (), cv[ch].end ());
   }
   return C;
 }
@@ -136,22 +184,27 @@ lanczos_lmax (const HCsr &A, int its, uint64_t seed)
   }
   std::vector<double> al, be;
   double rz = 0., rzold = 0.;
-  for (int64_t i = 0; i < n; i++) { z[i] = dinv[i] * r[i]; rz += r[i] * z[i]; }
+  for (int64_t i = 0; i < n; i++) z[i] = dinv[i] * r[i];
+  rz = hdot (r, z);
   p = z;
   for (int k = 0; k < its; k++) {
     hcsr_mult (A, p, q);
-    double pq = 0.;
-    for (int64_t i = 0; i < n; i++) pq += p[i] * q[i];
+    const double pq = hdot (p, q);
     if (!(pq > 0.)) break;
     const double a = rz / pq;
     al.push_back (a);
-    for (int64_t i = 0; i < n; i++) { x[i] += a * p[i]; r[i] -= a * q[i]; }
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) {
+      x[i] += a * p[i];
+      r[i] -= a * q[i];
+      z[i] = dinv[i] * r[i];
+    }
     rzold = rz;
-    rz = 0.;
-    for (int64_t i = 0; i < n; i++) { z[i] = dinv[i] * r[i]; rz += r[i] * z[i]; }
+    rz = hdot (r, z);
     if (rz <= 1e-300) break;
     const double b = rz / rzold;
     be.push_back (b);
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < n; i++) p[i] = z[i] + b * p[i];
   }
   const int m = (int) al.size ();
@@ -184,7 +237,7 @@ lanczos_lmax (const HCsr &A, int its, uint64_t seed)
 
 /* one smoothed-aggregation coarsening step */
 static void
-sa_coarsen (const HCsr &A, double theta, HCsr &P, int64_t &nc)
+sa_coarsen (const HCsr &A, double theta, double lmax, HCsr &P, int64_t &nc)
 {
   const int64_t n = A.n;
   std::vector<double> diag (n);
@@ -226,8 +279,7 @@ sa_coarsen (const HCsr &A, double theta, HCsr &P, int64_t &nc)
   for (int64_t i = 0; i < n; i++) sz[agg[i]] += 1.;
   std::vector<double> p0 (n);
   for (int64_t i = 0; i < n; i++) p0[i] = 1. / sqrt (sz[agg[i]]);
-  /* omega = 4/3 / lambda_max(D^{-1}A) */
-  const double lmax = lanczos_lmax (A, 40, 20260813ULL);
+  /* omega = 4/3 / lambda_max(D^{-1}A) (the level's own estimate) */
   const double omega = (4.0 / 3.0) / lmax;
   /* P = (I - omega D^{-1} A) P0, row by row */
   P.n = n;
@@ -382,6 +434,9 @@ mg_build (const Csr &Z, int tile, double smoother_top, int nu, Hierarchy **out)
     lv.n = A.n;
     lv.nu = nu > 0 ? nu : 2;
     lv.smax = lanczos_lmax (A, 40, 20260813ULL + (uint64_t) l);
+    /* the prolongator damping used the seed of level 0 on every level;
+     * keep that estimate (identical on level 0, one Lanczos run fewer) */
+    const double lmax_own = (l == 0) ? lv.smax : lanczos_lmax (A, 40, 20260813ULL);
     lv.slo = 0.1 * lv.smax;
     lv.shi = smoother_top * lv.smax;
     if (l == 0) {
@@ -430,7 +485,7 @@ mg_build (const Csr &Z, int tile, double smoother_top, int nu, Hierarchy **out)
     }
     HCsr P;
     int64_t nc = 0;
-    sa_coarsen (A, theta, P, nc);
+    sa_coarsen (A, theta, lmax_own, P, nc);
     if (nc >= A.n) {
       /* no coarsening progress: stop here with a dense coarse level is
        * impossible at this size */
