@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-rate", type=float, default=20.0)
     ap.add_argument("--serve-s", type=float, default=5.0)
+    ap.add_argument("--serve-slots", type=int, default=64,
+                    help="Z-solve columns in flight in the request loop")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--serve-rates", default="",
                     help="comma-separated request rates for --config c5")
@@ -518,7 +520,7 @@ def run_mixed_job(args, B, pr, opts, N, g64, rhs, xout, L, torch):
     return out
 
 
-def run_serving(args, g, N, L, rate=None, window=None, slots=64):
+def run_serving(args, g, N, L, rate=None, window=None, slots=None):
     """Continuous batching through the request loop (lgh_server_*) on the
     built object: a seeded Poisson stream at --serve-rate requests/s for
     --serve-s seconds, 60/30/10 solve/sample/logdet, m ~ U{1..64} columns,
@@ -527,6 +529,7 @@ def run_serving(args, g, N, L, rate=None, window=None, slots=64):
     rng = np.random.default_rng(2024)
     rate = args.serve_rate if rate is None else rate
     window = args.serve_s if window is None else window
+    slots = args.serve_slots if slots is None else slots
     t, arrivals = 0.0, []
     while True:
         t += rng.exponential(1.0 / rate)
@@ -541,12 +544,16 @@ def run_serving(args, g, N, L, rate=None, window=None, slots=64):
     pool = np.asfortranarray(rng.standard_normal((N, mmax)))
     sv = L.Server(g, slots=slots)
     ids = []
+    t_sub, late = 0.0, 0.0
     t0 = time.perf_counter()
     for ta, kind, m, c in arrivals:
         dt = ta - (time.perf_counter() - t0)
         if dt > 0:
             time.sleep(dt)
+        late = max(late, -dt)
+        ts = time.perf_counter()
         ids.append(sv.submit(kind, c, None if kind == 2 else pool[:, :m]))
+        t_sub += time.perf_counter() - ts
     lat = []
     for i in ids:
         lat.append(sv.wait(i, timeout=600.0)[1])
@@ -561,6 +568,13 @@ def run_serving(args, g, N, L, rate=None, window=None, slots=64):
             "p50_ms": 1e3 * lat[len(lat) // 2],
             "p99_ms": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))],
             "max_ms": 1e3 * lat[-1], "ticks": st["ticks"],
+            "loop_s": {k: round(st[k], 4) for k in (
+                "t_admit_s", "t_tick_s", "t_harvest_s", "t_up_s",
+                "t_down_s")},
+            "client": {"span_s": round(t1 - t0, 3),
+                       "submit_s": round(t_sub, 4),
+                       "max_late_s": round(late, 4)},
+            "harvests": st["harvests"],
             "mix": "60/30/10 solve/sample/logdet, m~U{1..64}, "
                    "c log-uniform [1e-3, 1e3]"}
 

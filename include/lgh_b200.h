@@ -336,9 +336,12 @@ int lgh_glr_logdet_batch (lgh_glr_t *glr, int nshift, const double *c,
  * object: a worker thread owns a block of `slots` Z-solve columns; each
  * column carries its own CG state, so requests that arrive while others run
  * join the same launches as columns free up, and a request's result does not
- * depend on what it was batched with.  Admission needs free slots for all of
- * a request's columns and free device memory for its staging buffers above
- * hbm_reserve of the total.  The loop has its own stream and work
+ * depend on what it was batched with.  Requests are admitted in arrival
+ * order column by column (a request wider than the slot block runs in
+ * parts); a second thread copies inputs to the device ahead of admission,
+ * while the device keeps hbm_reserve of its memory free, and copies results
+ * back.  A mixed-precision object (LGH_PREC_MIXED) runs its V-cycles in
+ * FP32 here too.  The loop has its own streams and work
  * buffers and only reads the GLR object and its prior, so the read-only
  * operations (solve, sample, logdet and their batched forms) may be
  * called beside it; lgh_glr_extend and the destroy calls must wait until
@@ -362,15 +365,24 @@ typedef struct lgh_server_stats
   long   completed, columns, ticks, pending;
   double p50_s, p99_s, max_s;   /* request latency, submit to done        */
   double columns_per_s;
+  /* the loop thread's seconds in admission (staging the admitted columns),
+   * in ticks (launch to the convergence mask on the host) and in harvests,
+   * and the harvest count                                                  */
+  double t_admit_s, t_tick_s, t_harvest_s;
+  long   harvests;
+  /* the copier thread's seconds moving inputs up and results down        */
+  double t_up_s, t_down_s;
 }
 lgh_server_stats_t;
 
 lgh_server_opts_t lgh_server_opts_default (void);
 int lgh_server_create (lgh_glr_t *glr, const lgh_server_opts_t *opts,
                        lgh_server_t **server);
-/* in / out: host column-major blocks (n x m, leading dims ldin / ldout)
- * that stay valid until the request completes; LGH_REQ_LOGDET writes one
- * double to out.                                                          */
+/* in / out: host column-major blocks (n x m, any m >= 1, leading dims
+ * ldin / ldout) that stay valid until the request completes;
+ * LGH_REQ_LOGDET writes one double to out.  A request that cannot get
+ * device memory for its staging while nothing else holds any completes
+ * with LGH_ERR_MEM (reported by lgh_server_wait); the loop carries on.    */
 int lgh_server_submit (lgh_server_t *server, int kind, double c, int m,
                        const double *in, int64_t ldin, double *out,
                        int64_t ldout, int64_t *id);
@@ -545,6 +557,13 @@ int lgh_test_rng_state (uint64_t seed, int64_t n, int64_t j0, int k,
 int lgh_test_spmm (lgh_Mat A, int w, const double *X, double *Y, int fp32);
 int lgh_test_zsolve (lgh_prior_t *prior, int w, const double *X, double *Y,
                      int fp32);
+/* one Chebyshev-Jacobi smoothing step of a square CSR Mat (n x w row-major
+ * host blocks) with the smoother's kernel: X in place, Rout = Ro - A d_new,
+ * Dout = d_new (flags & 4), d_new = a Do + b D^{-1} Ro (flags & 1: a Do
+ * left out; flags & 2: X taken as zero).                                  */
+int lgh_test_cheb_step (lgh_Mat A, int w, double a, double b, int flags,
+                        int fp32, double *X, const double *Ro,
+                        const double *Do, double *Rout, double *Dout);
 int lgh_test_gram (int64_t n, int w, const double *X, double *G);
 int lgh_test_gemm_nn (int64_t n, int k, int m, const double *X,
                       const double *M, double *Y);

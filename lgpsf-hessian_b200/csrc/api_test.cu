@@ -13,6 +13,7 @@
 
 #include "lgh_device.cuh"
 #include "lgh_internal.h"
+#include "lgh_mg.h"
 #include "lgh_objects.h"
 
 using namespace lgh;
@@ -31,6 +32,48 @@ static int
 down (T *h, const DBuf<T> &d, size_t n)
 {
   LGH_CUDA (cudaMemcpy (h, d.p, n * sizeof (T), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+/* one Chebyshev-Jacobi step of a square CSR Mat on n x w row-major host
+ * blocks (the smoother's kernel k_cheb): X is updated in place; Rout = Ro - A d_new and, with
+ * CHEB_STORE_D (4) in flags, Dout = d_new.  flags as the smoother's
+ * (1 first step: Do not read; 2 x is zero: X not read). */
+template <typename T>
+static int
+test_cheb (lgh_Mat A, int w, double a, double b, int flags, double *X, const double *Ro, const double *Do, double *Rout,
+           double *Dout)
+{
+  const int64_t n = A->csr.n;
+  const int ld = round_ld (w);
+  const size_t cnt = (size_t) n * ld;
+  std::vector<T> hx (cnt, T (0)), hr (cnt, T (0)), hd (cnt, T (0));
+  for (int64_t i = 0; i < n; i++)
+    for (int j = 0; j < w; j++) {
+      hx[i * ld + j] = (T) X[i * w + j];
+      hr[i * ld + j] = (T) Ro[i * w + j];
+      hd[i * ld + j] = Do ? (T) Do[i * w + j] : T (0);
+    }
+  DBuf<T> dx, dro, ddo, drn, ddn;
+  LGH_TRY (up (dx, hx.data (), cnt));
+  LGH_TRY (up (dro, hr.data (), cnt));
+  LGH_TRY (up (ddo, hd.data (), cnt));
+  LGH_TRY (drn.alloc (cnt));
+  LGH_TRY (ddn.alloc (cnt));
+  LGH_CUDA (cudaMemset (drn.p, 0, cnt * sizeof (T)));
+  LGH_CUDA (cudaMemset (ddn.p, 0, cnt * sizeof (T)));
+  LGH_TRY (launch_cheb_step<T> (A->csr, dx.p, dro.p, drn.p, ddo.p, ddn.p, ld, a, b,
+                                flags, stream ()));
+  LGH_CUDA (cudaStreamSynchronize (stream ()));
+  LGH_TRY (down (hx.data (), dx, cnt));
+  LGH_TRY (down (hr.data (), drn, cnt));
+  LGH_TRY (down (hd.data (), ddn, cnt));
+  for (int64_t i = 0; i < n; i++)
+    for (int j = 0; j < w; j++) {
+      X[i * w + j] = (double) hx[i * ld + j];
+      Rout[i * w + j] = (double) hr[i * ld + j];
+      if (Dout) Dout[i * w + j] = (double) hd[i * ld + j];
+    }
   return 0;
 }
 
@@ -91,6 +134,21 @@ lgh_test_spmm (lgh_Mat A, int w, const double *X, double *Y, int fp32)
   }
   for (int64_t i = 0; i < n; i++) memcpy (Y + i * w, hy.data () + i * ld, w * sizeof (double));
   return 0;
+}
+
+int
+lgh_test_cheb_step (lgh_Mat A, int w, double a, double b, int flags,
+                    int fp32, double *X, const double *Ro,
+                    const double *Do, double *Rout, double *Dout)
+{
+  LGH_TRY (ensure_init ());
+  LGH_CHECK (A && A->kind == 0 && X && Ro && Rout, LGH_ERR_ARG_NULL,
+             "lgh_test_cheb_step: NULL");
+  LGH_CHECK (A->csr.ncols == 0 || A->csr.ncols == A->csr.n, LGH_ERR_ARG_WRONG,
+             "lgh_test_cheb_step: square CSR Mat");
+  LGH_CHECK (w >= 1, LGH_ERR_ARG_OUTOFRANGE, "lgh_test_cheb_step: w");
+  return fp32 ? test_cheb<float> (A, w, a, b, flags, X, Ro, Do, Rout, Dout)
+              : test_cheb<double> (A, w, a, b, flags, X, Ro, Do, Rout, Dout);
 }
 
 /* Y = Z^{-1} X through the prior's blocked solve, n x w row-major */

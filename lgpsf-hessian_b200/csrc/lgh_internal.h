@@ -180,6 +180,10 @@ template <typename T>
 int launch_spmm_mode (const Csr &A, const T *X, int ldx, T *Y, int ldy, int w,
                       int mode, const T *Bm, int ldb, cudaStream_t s);
 
+/* Y = (TO) X over count elements of two blocks with the same layout */
+template <typename TI, typename TO>
+int cvt_flat (int64_t count, const TI *X, TO *Y, cudaStream_t s);
+
 /* elementwise / block helpers (k_vec.cu) */
 template <typename T>
 int launch_rowscale (int64_t n, int w, const double *scale, const T *X,

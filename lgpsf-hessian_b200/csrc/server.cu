@@ -177,8 +177,11 @@ struct SReq
   int64_t ldout = 0;
   /* device staging: input columns, output columns, U^T coefficients */
   DBuf<double> din, dout, wcoef;
-  int cols_left = 0;
-  int status = 1;   /* 1 pending/active, 0 done, < 0 error */
+  int staged = 0;     /* din holds the input (set by the copier)          */
+  int placed = 0;     /* columns handed to slots so far                   */
+  int cols_left = 0;  /* columns not yet through their last stage         */
+  cudaEvent_t ev_out = nullptr;   /* recorded after the last scatter      */
+  int status = 1;     /* 1 pending/active, 0 done, < 0 error              */
   double t_submit = 0., t_done = 0.;
 };
 
@@ -189,7 +192,7 @@ struct Slot
   int stage = 0;  /* 1: first Z-solve, 2: second (solve only) */
 };
 
-/* per-tick description of the harvested columns, copied to the device */
+/* per-harvest description of the harvested columns, copied to the device */
 struct Harvest
 {
   static constexpr int MAXS = 512;
@@ -204,21 +207,34 @@ struct Harvest
   double *out_b[MAXS];       /* request output columns */
 };
 
+/* a run of one request's columns admitted into slots this round */
+struct Adm
+{
+  SReq *r;
+  int j0, take;
+};
+
 } /* namespace lgh */
 
 struct lgh_server
 {
   lgh_glr_t *g = nullptr;
   int cap = 64, ld = 64;
+  int pc32 = 0;                 /* FP32 V-cycle (mixed-precision object) */
   double reserve = 0.1;
-  cudaStream_t s = nullptr;
-  std::thread worker;
+  cudaStream_t s = nullptr;     /* the loop's stream */
+  cudaStream_t sc = nullptr;    /* the copier's stream */
+  std::thread worker, copier;
   std::mutex mu;
-  std::condition_variable cv, done_cv;
-  std::deque<lgh::SReq *> pending;
+  std::condition_variable cv, ccv, done_cv;
+  std::deque<lgh::SReq *> pending;      /* arrival order, until placed */
+  std::deque<lgh::SReq *> up_q, dl_q;   /* copier: inputs in, results out */
   std::map<int64_t, std::unique_ptr<lgh::SReq>> reqs;
   std::atomic<bool> stop{ false };
+  std::atomic<int> failed{ 0 };
   int64_t next_id = 1;
+  long staged_cols = 0;   /* uploaded columns not yet placed */
+  long inflight = 0;      /* requests holding device staging */
   int err = 0;
   std::string errmsg;
   /* slot block and per-tick staging */
@@ -228,11 +244,20 @@ struct lgh_server
   lgh::DBuf<int> fresh_d;
   std::vector<int> fresh_h;
   int *fresh_pin = nullptr, *act_pin = nullptr;   /* pinned per-tick copies */
+  /* the copier's pinned staging, two halves of stg_half bytes: host
+   * columns are packed into one half by memcpy while the other half's
+   * DMA runs, so no pageable copy (which the driver stages itself,
+   * holding up other threads' calls) is ever made */
+  char *stg = nullptr;
+  size_t stg_half = 0;
+  cudaEvent_t stg_ev[2] = { nullptr, nullptr };
   lgh::DBuf<double> H, coef, gemmwork, ldc, ldo;
   lgh::DBuf<char> hv_d;
   std::unique_ptr<lgh::Harvest> hv;
   /* statistics */
-  long completed = 0, ticks = 0, cols_done = 0;
+  long completed = 0;
+  std::atomic<long> ticks{ 0 }, cols_done{ 0 }, harvests{ 0 };   /* loop-written */
+  double t_admit = 0., t_tick = 0., t_harvest = 0., t_up = 0., t_down = 0.;
   std::vector<double> lat;
   double t0 = 0., t_last = 0.;
 };
@@ -244,51 +269,231 @@ static int
 srv_fail (lgh_server_t *sv, int rc)
 {
   std::lock_guard<std::mutex> lk (sv->mu);
-  sv->err = rc;
-  sv->errmsg = lgh_last_error ();
+  if (sv->err == 0) {
+    sv->err = rc;
+    sv->errmsg = lgh_last_error ();
+  }
+  sv->failed.store (rc);
   for (auto &kv : sv->reqs)
     if (kv.second->status == 1) kv.second->status = -rc;
+  sv->cv.notify_all ();
+  sv->ccv.notify_all ();
   sv->done_cv.notify_all ();
   return rc;
 }
 
-/* admit pending requests in arrival order while slots and memory allow */
+/* a request leaves the loop: its staging is released (every use of it on
+ * either stream has completed: the copier synchronised its stream after
+ * the result copy, which waited for the loop's last scatter) */
 static void
-srv_admit (lgh_server_t *sv, std::vector<SReq *> &admitted)
+srv_finish (lgh_server_t *sv, SReq *r, int rc)
+{
+  const bool held = r->din.p != nullptr;
+  r->din.release ();
+  r->dout.release ();
+  r->wcoef.release ();
+  if (r->ev_out) {
+    cudaEventDestroy (r->ev_out);
+    r->ev_out = nullptr;
+  }
+  std::lock_guard<std::mutex> lk (sv->mu);
+  r->status = rc ? -rc : 0;
+  r->t_done = wall ();
+  if (held) sv->inflight--;
+  if (!rc) {
+    sv->lat.push_back (r->t_done - r->t_submit);
+    sv->completed++;
+    sv->t_last = r->t_done;
+  }
+  sv->done_cv.notify_all ();
+  sv->ccv.notify_all ();
+}
+
+/* room on the device for a request's staging above the reserve */
+static bool
+srv_room (lgh_server_t *sv, const SReq *r)
+{
+  size_t fb = 0, tb = 0;
+  if (cudaMemGetInfo (&fb, &tb) != cudaSuccess) {
+    cudaGetLastError ();
+    return true;
+  }
+  const double need = (double) sv->g->n * r->m * 16.
+                      + (double) std::max (sv->g->kept, 1) * r->m * 8.;
+  return (double) fb - need >= sv->reserve * (double) tb;
+}
+
+/* a request's input columns to the device through the pinned halves */
+static int
+srv_put (lgh_server_t *sv, SReq *r)
+{
+  const int64_t n = sv->g->n;
+  const size_t colb = (size_t) n * 8;
+  const int per = (int) std::max<size_t> (1, sv->stg_half / colb);
+  int b = 0;
+  for (int j0 = 0; j0 < r->m; j0 += per, b ^= 1) {
+    const int mc = std::min (per, r->m - j0);
+    char *h = sv->stg + (size_t) b * sv->stg_half;
+    LGH_CUDA (cudaEventSynchronize (sv->stg_ev[b]));   /* the half is free */
+    /* host memory bandwidth takes several threads */
+#pragma omp parallel for num_threads (std::min (mc, 8)) schedule (static)
+    for (int j = 0; j < mc; j++)
+      memcpy (h + (size_t) j * colb, r->hin + (size_t) (j0 + j) * r->ldin, colb);
+    LGH_CUDA (cudaMemcpyAsync (r->din.p + (size_t) j0 * n, h, mc * colb,
+                               cudaMemcpyHostToDevice, sv->sc));
+    LGH_CUDA (cudaEventRecord (sv->stg_ev[b], sv->sc));
+  }
+  LGH_CUDA (cudaStreamSynchronize (sv->sc));
+  return 0;
+}
+
+/* a finished request's output columns to the host through the pinned
+ * halves: chunk k + 1's DMA runs while chunk k is copied out */
+static int
+srv_get (lgh_server_t *sv, SReq *r)
+{
+  const int64_t n = sv->g->n;
+  const size_t colb = (size_t) n * 8;
+  const int per = (int) std::max<size_t> (1, sv->stg_half / colb);
+  const int nch = (r->m + per - 1) / per;
+  LGH_CUDA (cudaStreamWaitEvent (sv->sc, r->ev_out, 0));
+  auto issue = [&] (int k) -> int {
+    const int b = k & 1, j0 = k * per, mc = std::min (per, r->m - j0);
+    LGH_CUDA (cudaMemcpyAsync (sv->stg + (size_t) b * sv->stg_half,
+                               r->dout.p + (size_t) j0 * n, mc * colb,
+                               cudaMemcpyDeviceToHost, sv->sc));
+    LGH_CUDA (cudaEventRecord (sv->stg_ev[b], sv->sc));
+    return 0;
+  };
+  LGH_TRY (issue (0));
+  for (int k = 0; k < nch; k++) {
+    if (k + 1 < nch) LGH_TRY (issue (k + 1));
+    const int b = k & 1, j0 = k * per, mc = std::min (per, r->m - j0);
+    LGH_CUDA (cudaEventSynchronize (sv->stg_ev[b]));
+    const char *h = sv->stg + (size_t) b * sv->stg_half;
+#pragma omp parallel for num_threads (std::min (mc, 8)) schedule (static)
+    for (int j = 0; j < mc; j++)
+      memcpy (r->hout + (size_t) (j0 + j) * r->ldout, h + (size_t) j * colb, colb);
+  }
+  return 0;
+}
+
+/* the copier thread: host transfers off the loop's critical path.  Inputs
+ * go up in arrival order, at most two slot blocks of columns ahead of
+ * placement and while the device keeps hbm_reserve free (or nothing else
+ * holds staging); results come down as soon as the loop's last scatter
+ * of a request has run, and the request completes when they have landed. */
+static void
+srv_copier (lgh_server_t *sv)
+{
+  const int64_t n = sv->g->n;
+  const long ahead = 2L * sv->cap;
+  for (;;) {
+    SReq *dl = nullptr, *up = nullptr;
+    bool room_wait = false;
+    {
+      std::unique_lock<std::mutex> lk (sv->mu);
+      auto may_up = [&] {
+        return !sv->up_q.empty ()
+               && (sv->staged_cols == 0
+                   || sv->staged_cols + sv->up_q.front ()->m <= ahead);
+      };
+      sv->ccv.wait_for (lk, std::chrono::milliseconds (5), [&] {
+        return sv->stop.load () || sv->failed.load () || !sv->dl_q.empty ()
+               || may_up ();
+      });
+      if (sv->stop.load () || sv->failed.load ()) return;
+      if (!sv->dl_q.empty ()) {
+        dl = sv->dl_q.front ();
+        sv->dl_q.pop_front ();
+      } else if (may_up ()) {
+        SReq *r = sv->up_q.front ();
+        if (r->status != 1) {
+          sv->up_q.pop_front ();
+        } else if (sv->inflight > 0 && !srv_room (sv, r)) {
+          room_wait = true;
+        } else {
+          sv->up_q.pop_front ();
+          up = r;
+        }
+      }
+    }
+    if (room_wait) {
+      std::this_thread::sleep_for (std::chrono::milliseconds (1));
+      continue;
+    }
+    if (dl) {
+      const double w0 = wall ();
+      const int rc = srv_get (sv, dl);
+      {
+        std::lock_guard<std::mutex> lk (sv->mu);
+        sv->t_down += wall () - w0;
+      }
+      srv_finish (sv, dl, rc);
+      if (rc) { srv_fail (sv, rc); return; }
+    } else if (up) {
+      /* all of the request's device staging, so that the loop thread
+       * never allocates */
+      int rc = up->din.alloc ((size_t) n * up->m);
+      if (!rc) rc = up->dout.alloc ((size_t) n * up->m);
+      if (!rc) rc = up->wcoef.alloc ((size_t) std::max (sv->g->kept, 1) * up->m);
+      if (rc == 0) {
+        std::lock_guard<std::mutex> lk (sv->mu);
+        sv->inflight++;
+      }
+      if (rc == LGH_ERR_MEM) {
+        /* this request alone fails: nothing else held staging memory */
+        up->din.release ();
+        up->dout.release ();
+        up->wcoef.release ();
+        srv_finish (sv, up, rc);
+        clear_error ();
+        continue;
+      }
+      const double w0 = wall ();
+      if (!rc) rc = srv_put (sv, up);
+      if (rc) { srv_fail (sv, rc); return; }
+      std::lock_guard<std::mutex> lk (sv->mu);
+      sv->t_up += wall () - w0;
+      up->staged = 1;
+      sv->staged_cols += up->m;
+      sv->cv.notify_all ();
+    }
+  }
+}
+
+/* admit staged requests in arrival order, column by column, into the free
+ * slots: a request wider than what is free starts with the columns that
+ * fit and keeps the head of the queue until all of its columns are in */
+static void
+srv_admit (lgh_server_t *sv, std::vector<Adm> &adm)
 {
   std::lock_guard<std::mutex> lk (sv->mu);
   int free_slots = 0;
   for (auto &sl : sv->slots) free_slots += sl.req == nullptr;
   while (!sv->pending.empty ()) {
     SReq *r = sv->pending.front ();
-    if (r->kind != 2) {
-      if (r->m > free_slots) break;
-      size_t fb = 0, tb = 0;
-      if (cudaMemGetInfo (&fb, &tb) == cudaSuccess) {
-        const double need = (double) sv->g->n * r->m * 16.
-                            + (double) std::max (sv->g->kept, 1) * r->m * 8.;
-        if ((double) fb - need < sv->reserve * (double) tb) break;
-      }
-      free_slots -= r->m;
+    if (r->status != 1) {           /* failed while staging */
+      sv->pending.pop_front ();
+      continue;
     }
-    sv->pending.pop_front ();
-    admitted.push_back (r);
+    if (!r->staged) break;
+    if (r->kind == 2) {
+      sv->pending.pop_front ();
+      adm.push_back ({ r, 0, 0 });
+      continue;
+    }
+    const int take = std::min (free_slots, r->m - r->placed);
+    if (take <= 0) break;
+    adm.push_back ({ r, r->placed, take });
+    r->placed += take;
+    free_slots -= take;
+    if (r->placed == r->m) {
+      sv->pending.pop_front ();
+      sv->staged_cols -= r->m;
+      sv->ccv.notify_all ();
+    }
   }
-}
-
-static void
-srv_finish (lgh_server_t *sv, SReq *r, int rc)
-{
-  std::lock_guard<std::mutex> lk (sv->mu);
-  r->status = rc ? -rc : 0;
-  r->t_done = wall ();
-  sv->lat.push_back (r->t_done - r->t_submit);
-  sv->completed++;
-  sv->t_last = r->t_done;
-  r->din.release ();
-  r->dout.release ();
-  r->wcoef.release ();
-  sv->done_cv.notify_all ();
 }
 
 /* logdet requests complete at admission with the kernel of lgh_glr_logdet */
@@ -308,32 +513,34 @@ srv_logdet (lgh_server_t *sv, SReq *r)
   return 0;
 }
 
-/* stage a solve / sample request's columns into free slots */
+/* columns j0 .. j0 + take - 1 of a solve / sample request into free slots;
+ * its first run also forms, for a sample, w = U^T xi for all of its
+ * columns (the copier allocated the request's staging) */
 static int
-srv_start (lgh_server_t *sv, SReq *r, double *Pold)
+srv_start (lgh_server_t *sv, const Adm &a, double *Pold)
 {
   lgh_glr_t *g = sv->g;
+  SReq *r = a.r;
   const int64_t n = g->n;
-  const int kept = g->kept;
+  const int kept = g->kept, ldh = sv->ld;
   cudaStream_t s = sv->s;
   double *X = (double *) sv->ws.X.p, *R = (double *) sv->ws.R.p;
-  LGH_TRY (r->din.alloc ((size_t) n * r->m));
-  LGH_TRY (r->dout.alloc ((size_t) n * r->m));
-  LGH_TRY (r->wcoef.alloc ((size_t) std::max (kept, 1) * r->m));
-  LGH_CUDA (cudaMemcpy2DAsync (r->din.p, n * 8, r->hin, r->ldin * 8, n * 8, r->m,
-                               cudaMemcpyHostToDevice, s));
-  if (r->kind == 1 && kept > 0) {
-    /* sample: w = U^T xi before any Z-solve */
-    const int ldh = sv->ld;
-    LGH_TRY (launch_colmajor_to_rowmajor (n, r->m, r->din.p, n, sv->H.p, ldh,
-                                          nullptr, s));
-    LGH_TRY (launch_gemm_tn<double> (n, kept, r->m, g->U.p, g->ldu, sv->H.p, ldh,
-                                     r->wcoef.p, kept, 0, sv->gemmwork.p,
-                                     sv->gemmwork.n, s));
+  if (a.j0 == 0) {
+    r->cols_left = r->m;
+    if (r->kind == 1 && kept > 0) {
+      for (int c0 = 0; c0 < r->m; c0 += sv->cap) {
+        const int mc = std::min (sv->cap, r->m - c0);
+        LGH_TRY (launch_colmajor_to_rowmajor (n, mc, r->din.p + (size_t) c0 * n, n,
+                                              sv->H.p, ldh, nullptr, s));
+        LGH_TRY (launch_gemm_tn<double> (n, kept, mc, g->U.p, g->ldu, sv->H.p, ldh,
+                                         r->wcoef.p + (size_t) c0 * kept, kept, 0,
+                                         sv->gemmwork.p, sv->gemmwork.n, s));
+      }
+    }
   }
-  r->cols_left = r->m;
-  int j = 0;
-  for (int sl = 0; sl < sv->cap && j < r->m; sl++) {
+  int j = a.j0;
+  const int jend = a.j0 + a.take;
+  for (int sl = 0; sl < sv->cap && j < jend; sl++) {
     Slot &S = sv->slots[sl];
     if (S.req) continue;
     S.req = r;
@@ -347,13 +554,14 @@ srv_start (lgh_server_t *sv, SReq *r, double *Pold)
     sv->fresh_h[sl] = 1;
     j++;
   }
-  LGH_CHECK (j == r->m, LGH_ERR_ARG_WRONG, "server: admitted without free slots");
+  LGH_CHECK (j == jend, LGH_ERR_ARG_WRONG, "server: admitted without free slots");
   return 0;
 }
 
-/* columns whose Z-solve converged this tick move on: solve stage 1 ->
- * U^T coefficients and the second Z-solve; last stage -> the Woodbury
- * combination, the output column, and request completion */
+/* columns whose Z-solve has converged move on: solve stage 1 -> U^T
+ * coefficients and the second Z-solve; last stage -> the Woodbury
+ * combination and the output column.  A request whose last column left
+ * goes to the copier behind an event on the loop's stream. */
 static int
 srv_harvest (lgh_server_t *sv, const std::vector<int> &act, double *Pold)
 {
@@ -391,6 +599,7 @@ srv_harvest (lgh_server_t *sv, const std::vector<int> &act, double *Pold)
     }
   }
   if (ka == 0 && kb == 0) return 0;
+  sv->harvests++;
   Harvest *hd = (Harvest *) sv->hv_d.p;
   LGH_CUDA (cudaMemcpyAsync (hd, &h, sizeof (Harvest), cudaMemcpyHostToDevice, s));
   if (ka > 0) {
@@ -428,12 +637,13 @@ srv_harvest (lgh_server_t *sv, const std::vector<int> &act, double *Pold)
     sv->cols_done += kb;
   }
   for (SReq *r : fin) {
-    LGH_CUDA (cudaMemcpy2DAsync (r->hout, r->ldout * 8, r->dout.p, n * 8, n * 8, r->m,
-                                 cudaMemcpyDeviceToHost, s));
+    LGH_CUDA (cudaEventCreateWithFlags (&r->ev_out, cudaEventDisableTiming));
+    LGH_CUDA (cudaEventRecord (r->ev_out, s));
   }
   if (!fin.empty ()) {
-    LGH_CUDA (cudaStreamSynchronize (s));
-    for (SReq *r : fin) srv_finish (sv, r, 0);
+    std::lock_guard<std::mutex> lk (sv->mu);
+    for (SReq *r : fin) sv->dl_q.push_back (r);
+    sv->ccv.notify_all ();
   }
   return 0;
 }
@@ -449,6 +659,7 @@ srv_loop (lgh_server_t *sv)
   double *X = (double *) sv->ws.X.p, *R = (double *) sv->ws.R.p;
   double *P0 = (double *) sv->ws.P0.p, *P1 = (double *) sv->ws.P1.p;
   double *Q = (double *) sv->ws.Q.p, *Zb = (double *) sv->ws.Zb.p;
+  float *R32 = (float *) sv->ws.R32.p, *Z32 = (float *) sv->ws.Z32.p;
   double *Pold = P0, *Pnew = P1;
   int rc = 0;
   const size_t blk = (size_t) n * ld * sizeof (double);
@@ -465,12 +676,19 @@ srv_loop (lgh_server_t *sv)
   /* one PCG tick over the slot block for a given pair of direction
    * buffers; after two eager ticks (which set up the V-cycle buffers and
    * the launch-shape caches) each parity is captured into a CUDA graph
-   * once and replayed, so a tick costs one graph launch on the host */
+   * once and replayed, so a tick costs one graph launch on the host.  A
+   * mixed-precision object's V-cycle runs in FP32 on rounded copies of the
+   * residuals (the FP64 CG scalars and iterates are unchanged). */
   auto tick = [&] (double *Po, double *Pn) -> int {
-    if (p->mg)
+    if (p->mg && sv->pc32) {
+      LGH_TRY ((cvt_flat<double, float> (n * ld, R, R32, s)));
+      LGH_TRY (mg_vcycle<float> (p->mg, R32, Z32, ld, sv->cap, s, nullptr, &sv->mgw));
+      LGH_TRY ((cvt_flat<float, double> (n * ld, Z32, Zb, s)));
+    } else if (p->mg) {
       LGH_TRY (mg_vcycle<double> (p->mg, R, Zb, ld, sv->cap, s, nullptr, &sv->mgw));
-    else
+    } else {
       LGH_TRY (launch_rowscale<double> (n, ld, p->Z->csr.dinv, R, ld, Zb, ld, s));
+    }
     LGH_TRY (server_tick_dots<double> (p->Z->csr, R, Zb, ld, sv->cap, sv->fresh_d.p,
                                        p->zcfg.rtol, sv->ws, s));
     LGH_TRY (server_tick_pq<double> (p->Z->csr, Zb, Po, Pn, Q, ld, sv->ws, s));
@@ -479,29 +697,37 @@ srv_loop (lgh_server_t *sv)
   cudaGraphExec_t gexec[2] = { nullptr, nullptr };
   bool graphs_off = false;
   int parity = 0;   /* 0: the old direction is in P0 */
+  int hold = 0;     /* ticks that converged columns have waited */
+  const int batch = std::max (1, sv->cap / 8);
   auto release_graphs = [&] () {
     for (auto &ge : gexec)
       if (ge) { cudaGraphExecDestroy (ge); ge = nullptr; }
   };
-  while (!sv->stop.load ()) {
+  double ta = 0., tt = 0., th = 0.;   /* phase seconds, published per tick */
+  while (!sv->stop.load () && !sv->failed.load ()) {
     /* 1. admission into free slots */
-    std::vector<SReq *> adm;
+    double w0 = wall ();
+    std::vector<Adm> adm;
     srv_admit (sv, adm);
-    for (SReq *r : adm) {
-      rc = (r->kind == 2) ? srv_logdet (sv, r) : srv_start (sv, r, Pold);
+    for (const Adm &a : adm) {
+      rc = (a.r->kind == 2) ? srv_logdet (sv, a.r) : srv_start (sv, a, Pold);
       if (rc) break;
     }
+    if (!adm.empty ()) ta += wall () - w0;
     if (rc) { release_graphs (); srv_fail (sv, rc); return; }
     bool any = false;
     for (auto &sl : sv->slots) any |= sl.req != nullptr;
     if (!any) {
       std::unique_lock<std::mutex> lk (sv->mu);
-      sv->cv.wait_for (lk, std::chrono::milliseconds (2),
-                       [&] { return sv->stop.load () || !sv->pending.empty (); });
+      sv->cv.wait_for (lk, std::chrono::milliseconds (2), [&] {
+        return sv->stop.load () || sv->failed.load ()
+               || (!sv->pending.empty () && sv->pending.front ()->staged);
+      });
       continue;
     }
     /* 2. one PCG tick over the whole slot block: preconditioner, dots
      *    (fresh columns start there), direction + Z product, update */
+    w0 = wall ();
     memcpy (sv->fresh_pin, sv->fresh_h.data (), sv->cap * sizeof (int));
     if (cudaMemcpyAsync (sv->fresh_d.p, sv->fresh_pin, sv->cap * sizeof (int),
                          cudaMemcpyHostToDevice, s) != cudaSuccess)
@@ -535,15 +761,39 @@ srv_loop (lgh_server_t *sv)
     parity ^= 1;
     std::fill (sv->fresh_h.begin (), sv->fresh_h.end (), 0);
     sv->ticks++;
-    /* 3. harvest converged columns */
+    /* 3. the convergence mask; converged columns are harvested in
+     *    batches (a harvest reads all of U and W once, whatever its
+     *    width): at cap/8 columns, when every occupied slot has
+     *    converged, or after three ticks of waiting.  A converged column
+     *    is frozen (its step lengths are zero), so waiting changes no bit
+     *    of its result. */
     if (!rc && cudaMemcpyAsync (sv->act_pin, sv->ws.ival.p, sv->cap * sizeof (int),
                                 cudaMemcpyDeviceToHost, s) != cudaSuccess)
       rc = set_error (LGH_ERR_GPU, "server: mask copy");
     if (!rc && cudaStreamSynchronize (s) != cudaSuccess)
       rc = set_error (LGH_ERR_GPU, "server: tick");
+    tt += wall () - w0;
     if (!rc) {
       memcpy (act.data (), sv->act_pin, sv->cap * sizeof (int));
-      rc = srv_harvest (sv, act, Pold);
+      int occ = 0, conv = 0;
+      for (int sl = 0; sl < sv->cap; sl++)
+        if (sv->slots[sl].req) {
+          occ++;
+          conv += act[sl] == 0;
+        }
+      if (conv > 0) hold++;
+      if (conv > 0 && (conv >= batch || conv == occ || hold >= 3)) {
+        w0 = wall ();
+        rc = srv_harvest (sv, act, Pold);
+        th += wall () - w0;
+        hold = 0;
+      }
+    }
+    {
+      std::lock_guard<std::mutex> lk (sv->mu);
+      sv->t_admit = ta;
+      sv->t_tick = tt;
+      sv->t_harvest = th;
     }
     if (rc) { release_graphs (); srv_fail (sv, rc); return; }
   }
@@ -566,6 +816,27 @@ lgh_server_opts_default (void)
   return o;
 }
 
+static void
+srv_release (lgh_server_t *sv)
+{
+  if (sv->s) {
+    cudaStreamSynchronize (sv->s);
+    cudaStreamDestroy (sv->s);
+  }
+  if (sv->sc) {
+    cudaStreamSynchronize (sv->sc);
+    cudaStreamDestroy (sv->sc);
+  }
+  for (auto &kv : sv->reqs)
+    if (kv.second->ev_out) cudaEventDestroy (kv.second->ev_out);
+  for (auto &e : sv->stg_ev)
+    if (e) cudaEventDestroy (e);
+  if (sv->stg) cudaFreeHost (sv->stg);
+  if (sv->fresh_pin) cudaFreeHost (sv->fresh_pin);
+  if (sv->act_pin) cudaFreeHost (sv->act_pin);
+  delete sv;
+}
+
 int
 lgh_server_create (lgh_glr_t *glr, const lgh_server_opts_t *opts,
                    lgh_server_t **out)
@@ -582,13 +853,22 @@ lgh_server_create (lgh_glr_t *glr, const lgh_server_opts_t *opts,
   sv->cap = o.slots;
   sv->ld = round_ld (o.slots);
   sv->reserve = o.hbm_reserve;
+  sv->pc32 = glr->exec.precision == LGH_PREC_MIXED && glr->prior->mg != nullptr;
   int rc = 0;
-  if (cudaStreamCreateWithFlags (&sv->s, cudaStreamNonBlocking) != cudaSuccess)
-    rc = set_error (LGH_ERR_GPU, "lgh_server_create: stream");
+  if (cudaStreamCreateWithFlags (&sv->s, cudaStreamNonBlocking) != cudaSuccess
+      || cudaStreamCreateWithFlags (&sv->sc, cudaStreamNonBlocking) != cudaSuccess)
+    rc = set_error (LGH_ERR_GPU, "lgh_server_create: streams");
   /* the shift-independent precompute W = Z^{-1} M^{1/2} U */
   if (!rc) rc = ensure_wz (glr);
   const int kp = std::max (glr->kept, 1);
   if (!rc) rc = sv->ws.alloc (glr->n, sv->ld, 0);
+  if (!rc && sv->pc32) {
+    rc = sv->ws.R32.alloc ((size_t) glr->n * sv->ld * sizeof (float));
+    if (!rc) rc = sv->ws.Z32.alloc ((size_t) glr->n * sv->ld * sizeof (float));
+    if (!rc && cudaMemsetAsync (sv->ws.Z32.p, 0, (size_t) glr->n * sv->ld * sizeof (float),
+                                sv->s) != cudaSuccess)
+      rc = set_error (LGH_ERR_GPU, "lgh_server_create: clear");
+  }
   if (!rc) rc = sv->fresh_d.alloc (sv->ld);
   if (!rc) rc = sv->H.alloc ((size_t) glr->n * sv->ld);
   if (!rc) rc = sv->coef.alloc ((size_t) kp * sv->cap);
@@ -600,13 +880,18 @@ lgh_server_create (lgh_glr_t *glr, const lgh_server_opts_t *opts,
   if (!rc && (cudaMallocHost ((void **) &sv->fresh_pin, sv->ld * sizeof (int)) != cudaSuccess
               || cudaMallocHost ((void **) &sv->act_pin, sv->ld * sizeof (int)) != cudaSuccess))
     rc = set_error (LGH_ERR_MEM, "lgh_server_create: pinned buffers");
+  /* staging halves of at least one column and 32 MiB */
+  sv->stg_half = std::max<size_t> ((size_t) 32 << 20, (size_t) glr->n * 8);
+  if (!rc && cudaMallocHost ((void **) &sv->stg, 2 * sv->stg_half) != cudaSuccess)
+    rc = set_error (LGH_ERR_MEM, "lgh_server_create: staging buffers");
+  for (auto &e : sv->stg_ev)
+    if (!rc && (cudaEventCreateWithFlags (&e, cudaEventDisableTiming) != cudaSuccess
+                || cudaEventRecord (e, sv->sc) != cudaSuccess))
+      rc = set_error (LGH_ERR_GPU, "lgh_server_create: staging events");
   if (!rc) rc = cudaDeviceSynchronize () == cudaSuccess ? 0
                 : set_error (LGH_ERR_GPU, "lgh_server_create: set-up");
   if (rc) {
-    if (sv->s) cudaStreamDestroy (sv->s);
-    if (sv->fresh_pin) cudaFreeHost (sv->fresh_pin);
-    if (sv->act_pin) cudaFreeHost (sv->act_pin);
-    delete sv;
+    srv_release (sv);
     return rc;
   }
   sv->hv.reset (new Harvest ());
@@ -618,6 +903,10 @@ lgh_server_create (lgh_glr_t *glr, const lgh_server_opts_t *opts,
   sv->worker = std::thread ([sv, dev] {
     cudaSetDevice (dev);
     srv_loop (sv);
+  });
+  sv->copier = std::thread ([sv, dev] {
+    cudaSetDevice (dev);
+    srv_copier (sv);
   });
   *out = sv;
   return 0;
@@ -634,9 +923,8 @@ lgh_server_submit (lgh_server_t *sv, int kind, double c, int m,
              "lgh_server_submit: shift c must exceed the spectrum floor %g",
              sv->g->floor);
   if (kind != 2) {
-    LGH_CHECK (in && out && m >= 1 && m <= sv->cap && ldin >= sv->g->n
-               && ldout >= sv->g->n, LGH_ERR_ARG_SIZ,
-               "lgh_server_submit: need 1 <= m <= slots and ld >= n");
+    LGH_CHECK (in && out && m >= 1 && ldin >= sv->g->n && ldout >= sv->g->n,
+               LGH_ERR_ARG_SIZ, "lgh_server_submit: need m >= 1 and ld >= n");
   }
   std::unique_ptr<SReq> r (new SReq ());
   r->kind = kind;
@@ -646,6 +934,7 @@ lgh_server_submit (lgh_server_t *sv, int kind, double c, int m,
   r->ldin = ldin;
   r->hout = out;
   r->ldout = ldout;
+  r->staged = kind == 2;
   r->t_submit = wall ();
   std::lock_guard<std::mutex> lk (sv->mu);
   LGH_CHECK (sv->err == 0, sv->err, "lgh_server_submit: server failed: %s",
@@ -653,8 +942,10 @@ lgh_server_submit (lgh_server_t *sv, int kind, double c, int m,
   r->id = sv->next_id++;
   *id = r->id;
   sv->pending.push_back (r.get ());
+  if (kind != 2) sv->up_q.push_back (r.get ());
   sv->reqs[r->id] = std::move (r);
   sv->cv.notify_all ();
+  sv->ccv.notify_all ();
   return 0;
 }
 
@@ -669,7 +960,12 @@ lgh_server_wait (lgh_server_t *sv, int64_t id, double timeout_s, double *latency
   const bool ok = sv->done_cv.wait_for (
       lk, std::chrono::duration<double> (timeout_s), [&] { return r->status != 1; });
   if (!ok) return set_error (LGH_ERR_NOT_CONVERGED, "lgh_server_wait: timed out");
-  if (r->status < 0) return set_error (-r->status, "lgh_server_wait: %s", sv->errmsg.c_str ());
+  if (r->status < 0) {
+    const int code = -r->status;
+    sv->reqs.erase (it);
+    return set_error (code, "lgh_server_wait: request failed%s%s",
+                      sv->errmsg.empty () ? "" : ": ", sv->errmsg.c_str ());
+  }
   if (latency_s) *latency_s = r->t_done - r->t_submit;
   sv->reqs.erase (it);
   return 0;
@@ -694,6 +990,12 @@ lgh_server_get_stats (lgh_server_t *sv, lgh_server_stats_t *st)
   }
   const double el = (sv->t_last > sv->t0) ? sv->t_last - sv->t0 : 0.;
   st->columns_per_s = el > 0. ? sv->cols_done / el : 0.;
+  st->t_admit_s = sv->t_admit;
+  st->t_tick_s = sv->t_tick;
+  st->t_harvest_s = sv->t_harvest;
+  st->harvests = sv->harvests;
+  st->t_up_s = sv->t_up;
+  st->t_down_s = sv->t_down;
   return 0;
 }
 
@@ -702,12 +1004,14 @@ lgh_server_destroy (lgh_server_t *sv)
 {
   if (!sv) return;
   sv->stop.store (true);
-  sv->cv.notify_all ();
+  {
+    std::lock_guard<std::mutex> lk (sv->mu);
+    sv->cv.notify_all ();
+    sv->ccv.notify_all ();
+  }
   if (sv->worker.joinable ()) sv->worker.join ();
-  if (sv->s) cudaStreamDestroy (sv->s);
-  if (sv->fresh_pin) cudaFreeHost (sv->fresh_pin);
-  if (sv->act_pin) cudaFreeHost (sv->act_pin);
-  delete sv;
+  if (sv->copier.joinable ()) sv->copier.join ();
+  srv_release (sv);
 }
 
 } /* extern "C" */

@@ -313,7 +313,7 @@ k_pcg_upd (ZK z, const T *__restrict__ dinv, T *__restrict__ X,
 /* ---- Chebyshev: d_new = a d + b D^{-1} r (on the fly at neighbours),
  *      x += d_new, r_new = r - Z d_new (zsolve_impl.h:108-141) ----------- */
 template <typename T, int CH>
-__global__ void __launch_bounds__ (ZS_THREADS, (CH * (16 / sizeof (T)) <= 8 ? 3 : 2))
+__global__ void __launch_bounds__ (ZS_THREADS, (CH * (16 / sizeof (T)) <= 8 ? 4 : 2))
 k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ vdv,
         const T *__restrict__ dinv, T *__restrict__ X,
         const T *__restrict__ Rold, T *__restrict__ Rnew,
@@ -325,8 +325,9 @@ k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ vdv,
    * Software pipeline over the group's rows: the next row's bounds and
    * its first G (column, value, value/diagonal) triples are loaded while
    * the current row's neighbour rows are gathered, so the only latency on
-   * a row's critical path is the gathers' own; the row's x is loaded
-   * ahead of the gathers. */
+   * a row's critical path is the gathers' own; the row's x loads with its
+   * own r and d after them (the same round trip), which keeps the
+   * two-pack FP64 form within 64 registers: 4 CTAs of 8 warps per SM. */
   ZS_GROUP_SETUP ();
   const bool first = flags & CHEB_FIRST, zx = flags & CHEB_ZERO_X;
   const bool wd = flags & CHEB_STORE_D;
@@ -350,12 +351,6 @@ k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ vdv,
     if (inx < z.n) {
       k0n = z.rowptr[inx];
       k1n = z.rowptr[inx + 1];
-    }
-    Pack<T> xs[CH];
-#pragma unroll
-    for (int h = 0; h < CH; h++) {
-      const int vi = lane + h * G;
-      xs[h] = (zx || vi >= nvec) ? pzero<T> () : ldp (X + i * ld + vi * W);
     }
     T acc[CH][W];
 #pragma unroll
@@ -406,7 +401,7 @@ k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ vdv,
         const int64_t o = i * ld + vi * W;
         Pack<T> ri = ldp (Rold + o);
         Pack<T> di = first ? pzero<T> () : ldp (Dold + o);
-        Pack<T> dn, rn, x = xs[h];
+        Pack<T> dn, rn, x = zx ? pzero<T> () : ldp (X + o);
 #pragma unroll
         for (int e = 0; e < W; e++) {
           dn.v[e] = fma (bdi, ri.v[e], a * di.v[e]);
@@ -893,7 +888,7 @@ k_cvt_flat (int64_t count, const TI *__restrict__ X, TO *__restrict__ Y)
 }
 
 template <typename TI, typename TO>
-static int
+int
 cvt_flat (int64_t count, const TI *X, TO *Y, cudaStream_t s)
 {
   const int grid = (int) std::max<int64_t> (1, std::min<int64_t> (
@@ -902,6 +897,11 @@ cvt_flat (int64_t count, const TI *X, TO *Y, cudaStream_t s)
   LGH_LAUNCH_CHECK ();
   return 0;
 }
+
+template int cvt_flat<double, float> (int64_t, const double *, float *,
+                                      cudaStream_t);
+template int cvt_flat<float, double> (int64_t, const float *, double *,
+                                      cudaStream_t);
 
 template <typename T>
 int
@@ -1187,15 +1187,8 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
           tids.push_back (K_CHEB);
           tbytes.push_back (zbytes + 6. * (double) n * wt * sizeof (T));
         }
-        ZS_DISPATCH (ch, {
-          k_cheb<T, CH_><<<fit_grid (k_cheb<T, CH_>, grid, ZS_THREADS, 0),
-                                          ZS_THREADS, 0, s>>> (zk, vals, zvd<T> (Z), dinv, bX, Ro, Rn,
-                                                      Do, Dn, ldt, nvec, glog,
-                                                      (T) a, (T) b,
-                                                      (k == 1 ? CHEB_FIRST : 0)
-                                                      | CHEB_STORE_D);
-        });
-        LGH_LAUNCH_CHECK ();
+        LGH_TRY (launch_cheb_step<T> (Z, bX, Ro, Rn, Do, Dn, ldt, a, b,
+                                      (k == 1 ? CHEB_FIRST : 0) | CHEB_STORE_D, s));
         if (tk) {
           LGH_TRY (ring.record (s));
           tids.push_back (-1);
@@ -1308,7 +1301,8 @@ template int server_tick_dots<double> (const Csr &, const double *,
                                        const double *, int, int, const int *,
                                        double, ZWork &, cudaStream_t);
 
-/* one Chebyshev-Jacobi step on a CSR operator (the multigrid smoother) */
+/* one Chebyshev-Jacobi step on a CSR operator (the multigrid smoother and
+ * the fixed-count Chebyshev mode) */
 template <typename T>
 int
 launch_cheb_step (const Csr &A, T *X, const T *Ro, T *Rn, const T *Do, T *Dn,

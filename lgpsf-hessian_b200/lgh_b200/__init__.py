@@ -90,7 +90,10 @@ class ServerStats(ctypes.Structure):
     _fields_ = [("completed", ctypes.c_long), ("columns", ctypes.c_long),
                 ("ticks", ctypes.c_long), ("pending", ctypes.c_long),
                 ("p50_s", ctypes.c_double), ("p99_s", ctypes.c_double),
-                ("max_s", ctypes.c_double), ("columns_per_s", ctypes.c_double)]
+                ("max_s", ctypes.c_double), ("columns_per_s", ctypes.c_double),
+                ("t_admit_s", ctypes.c_double), ("t_tick_s", ctypes.c_double),
+                ("t_harvest_s", ctypes.c_double), ("harvests", ctypes.c_long),
+                ("t_up_s", ctypes.c_double), ("t_down_s", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -274,6 +277,9 @@ SIGNATURES = {
                                           ctypes.c_int, P]),
     "lgh_test_spmm": (ctypes.c_int, [P, ctypes.c_int, P, P, ctypes.c_int]),
     "lgh_test_zsolve": (ctypes.c_int, [P, ctypes.c_int, P, P, ctypes.c_int]),
+    "lgh_test_cheb_step": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_int,
+                                          ctypes.c_int, P, P, P, P, P]),
     "lgh_test_gram": (ctypes.c_int, [I64, ctypes.c_int, P, P]),
     "lgh_gram_noalloc": (ctypes.c_int, [I64, ctypes.c_int, P, I64, P, I64]),
     "lgh_test_gemm_nn": (ctypes.c_int, [I64, ctypes.c_int, ctypes.c_int, P,
@@ -808,7 +814,7 @@ class Server:
             self._bufs[rid.value] = (None, out)
             return rid.value
         Xin = np.asfortranarray(X, dtype=np.float64)
-        out = np.zeros_like(Xin, order="F")
+        out = np.empty_like(Xin, order="F")   # every entry is written
         _chk(L.lgh_server_submit(self.h, kind, c, Xin.shape[1],
                                  Xin.ctypes.data, self.n, out.ctypes.data,
                                  self.n, ctypes.byref(rid)),
@@ -817,12 +823,13 @@ class Server:
         return rid.value
 
     def wait(self, rid, timeout=600.0):
+        """(result, latency seconds): the (n, m) column-major block the
+        library wrote (no reordering copy), or the logdet value."""
         lat = ctypes.c_double()
         _chk(load().lgh_server_wait(self.h, rid, timeout, ctypes.byref(lat)),
              "lgh_server_wait")
         _, out = self._bufs.pop(rid)
-        return (out[0] if out.ndim == 1 else np.ascontiguousarray(out)), \
-            lat.value
+        return (out[0] if out.ndim == 1 else out), lat.value
 
     def stats(self):
         st = ServerStats()
@@ -871,6 +878,25 @@ def test_zsolve(prior, X, fp32=False):
                                 Y.ctypes.data, 1 if fp32 else 0),
          "lgh_test_zsolve")
     return Y
+
+
+CHEB_FIRST, CHEB_ZERO_X, CHEB_STORE_D = 1, 2, 4
+
+
+def test_cheb_step(A, X, R, D, a, b, flags, fp32=False):
+    """One Chebyshev-Jacobi smoothing step (lgh_test_cheb_step); returns
+    the new (X, R, D)."""
+    X = np.array(X, dtype=np.float64, order="C")
+    R = np.ascontiguousarray(R, dtype=np.float64)
+    D = np.ascontiguousarray(D, dtype=np.float64)
+    Rn = np.zeros_like(R)
+    Dn = np.zeros_like(R)
+    _chk(load().lgh_test_cheb_step(A.h, X.shape[1], a, b, flags,
+                                   1 if fp32 else 0, X.ctypes.data,
+                                   R.ctypes.data, D.ctypes.data,
+                                   Rn.ctypes.data, Dn.ctypes.data),
+         "lgh_test_cheb_step")
+    return X, Rn, Dn
 
 
 def test_gram(X):

@@ -1,0 +1,85 @@
+"""The multigrid smoother's kernel (k_cheb, one Chebyshev-Jacobi step of a
+CSR operator on a row-major block) against a numpy restatement of the step,
+for every flag combination the V-cycle uses, in FP64 and FP32, on the 2D
+5-point and 3D 7-point Z operators and on a matrix with rows of mixed
+lengths, empty rows and rows without a diagonal entry (Jacobi scale 0).
+
+One step: d_new = a d + b D^{-1} r (flags & 1: the a d term left out),
+x += d_new (flags & 2: x taken as zero), r_new = r - A d_new, and d_new
+stored (flags & 4)."""
+
+import numpy as np
+import pytest
+
+import lgh_b200 as L
+import lgh_b200.problems as P
+
+pytestmark = pytest.mark.gpu
+
+FLAGS = [L.CHEB_FIRST | L.CHEB_ZERO_X | L.CHEB_STORE_D,
+         L.CHEB_FIRST | L.CHEB_STORE_D, L.CHEB_STORE_D, 0, L.CHEB_FIRST]
+
+
+def _ragged(n=1500, seed=5):
+    """Rows with 0..40 off-diagonal entries (longer than one 32-lane row
+    group); every 7th row has no diagonal entry."""
+    rng = np.random.default_rng(seed)
+    rows, cols, vals = [], [], []
+    for i in range(n):
+        k = int(rng.integers(0, 41))
+        nb = rng.choice(np.delete(np.arange(n), i), size=k, replace=False)
+        rows += [i] * k
+        cols += list(nb)
+        vals += list(0.1 * rng.standard_normal(k))
+        if i % 7:
+            rows.append(i)
+            cols.append(i)
+            vals.append(2.0 + rng.random())
+    return P.coo_to_csr(n, np.array(rows), np.array(cols), np.array(vals))
+
+
+@pytest.fixture(scope="module")
+def ops(cuda_device):
+    d = {
+        "z2d": P.z_operator(48, 2, 25.0, P.lumped_mass(48, 2)),
+        "z3d": P.z_operator(14, 3, 16.0, P.lumped_mass(14, 3)),
+        "ragged": _ragged(),
+    }
+    return {k: (v, L.Mat(v)) for k, v in d.items()}
+
+
+def _numpy_step(A, X, R, D, a, b, flags):
+    Ad = P.csr_to_dense(A)
+    diag = np.diag(Ad)
+    dinv = np.where(diag != 0, 1.0 / np.where(diag != 0, diag, 1.0), 0.0)
+    dn = b * dinv[:, None] * R
+    if not flags & L.CHEB_FIRST:
+        dn = dn + a * D
+    x = dn if flags & L.CHEB_ZERO_X else X + dn
+    return x, R - Ad @ dn, dn
+
+
+@pytest.mark.parametrize("name", ["z2d", "z3d", "ragged"])
+@pytest.mark.parametrize("fp32", [False, True])
+def test_cheb_step_matches_numpy(ops, name, fp32):
+    A, M = ops[name]
+    n = A["n"]
+    rng = np.random.default_rng(17)
+    tol = 2e-5 if fp32 else 1e-12
+    for w in (1, 3, 16, 60, 220):
+        X = rng.standard_normal((n, w))
+        R = rng.standard_normal((n, w))
+        D = rng.standard_normal((n, w))
+        if fp32:
+            X, R, D = (v.astype(np.float32).astype(np.float64) for v in (X, R, D))
+        for fl in FLAGS:
+            a, b = 0.37, 0.81
+            x1, r1, d1 = L.test_cheb_step(M, X, R, D, a, b, fl, fp32)
+            xe, re, de = _numpy_step(A, X, R, D, a, b, fl)
+            assert np.abs(x1 - xe).max() <= tol * (1 + np.abs(xe).max()), (w, fl)
+            assert np.abs(r1 - re).max() <= tol * (1 + np.abs(re).max()), (w, fl)
+            if fl & L.CHEB_STORE_D:
+                assert np.abs(d1 - de).max() <= tol * (1 + np.abs(de).max())
+            # deterministic: the same call gives the same bits
+            x2, r2, _ = L.test_cheb_step(M, X, R, D, a, b, fl, fp32)
+            assert np.array_equal(x1, x2) and np.array_equal(r1, r2)

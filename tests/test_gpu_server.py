@@ -113,7 +113,7 @@ def test_server_argument_errors(c1):
     n = cfg["N"]
     sv = L.Server(g, slots=4)
     with pytest.raises(L.LghError) as e:
-        sv.submit(L.Server.SOLVE, 1.0, np.ones((n, 5)))   # m > slots
+        sv.submit(L.Server.SOLVE, 1.0, np.ones((n, 0)))   # m = 0
     assert e.value.code == 60
     with pytest.raises(L.LghError) as e:
         sv.submit(L.Server.SOLVE, -1.0, np.ones((n, 1)))  # c <= floor
@@ -121,4 +121,59 @@ def test_server_argument_errors(c1):
     with pytest.raises(L.LghError) as e:
         sv.submit(7, 1.0, np.ones((n, 1)))
     assert e.value.code == 63
+    sv.close()
+
+
+def test_server_request_wider_than_slots(c1):
+    """A request with more columns than the slot block runs in parts and
+    gives the same bits as its columns submitted one at a time."""
+    cfg, keep, g = c1
+    n = cfg["N"]
+    rng = np.random.default_rng(21)
+    X = rng.standard_normal((n, 11))
+    Xs = rng.standard_normal((n, 9))
+    sv = L.Server(g, slots=4)
+    wide = sv.wait(sv.submit(L.Server.SOLVE, 0.7, X))[0]
+    wide_s = sv.wait(sv.submit(L.Server.SAMPLE, 0.7, Xs))[0]
+    ref = g.solve_batch([0.7], X)[0]
+    ref_s = g.sample_batch([0.7], Xs)[0]
+    assert _rd(wide, ref) < 1e-8
+    assert _rd(wide_s, ref_s) < 1e-8
+    one = np.column_stack([sv.wait(sv.submit(L.Server.SOLVE, 0.7,
+                                             X[:, j:j + 1]))[0]
+                           for j in range(X.shape[1])])
+    assert np.array_equal(one, wide)
+    sv.close()
+
+
+@pytest.fixture(scope="module")
+def c1_mixed(cuda_device):
+    cfg = P.grid_problem("c1")
+    B, Z = L.Mat(cfg["B"]), L.Mat(cfg["Z"])
+    pr = L.Prior(Z=Z, mass=cfg["mass"], opts=L.prior_opts(ksp_rtol=1e-12))
+    g = L.Glr(B, pr, L.glr_opts(ell=40, seed=0, check=0),
+              exec=L.exec_opts(precision=L.PREC_MIXED))
+    return cfg, (B, Z, pr), g
+
+
+def test_server_mixed_object(c1_mixed):
+    """A mixed-precision object's loop runs FP32 V-cycles under FP64 CG:
+    its results agree with the object's own batched operations to the
+    Z-solve tolerance and stay independent of the batch."""
+    cfg, keep, g = c1_mixed
+    n = cfg["N"]
+    reqs = _reqs(n, 9)
+    sv = L.Server(g, slots=8)
+    ids = [sv.submit(k, c, X) for k, c, X in reqs]
+    outs = [sv.wait(i)[0] for i in ids]
+    for (k, c, X), y in zip(reqs, outs):
+        if k == L.Server.LOGDET:
+            assert abs(y - g.logdet(c)) == 0.0
+            continue
+        ref = (g.solve_batch if k == L.Server.SOLVE else g.sample_batch)(
+            [c], X)[0]
+        assert _rd(y, ref) < 1e-8, (k, c)
+    k, c, X = reqs[0]
+    alone = sv.wait(sv.submit(k, c, X))[0]
+    assert np.array_equal(alone, outs[0])
     sv.close()
