@@ -424,30 +424,33 @@ k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ vdv,
 /* ---- PCG with an explicit preconditioner z = V(r) (the AMG V-cycle):
  * p_new = z + beta p_old on the fly at neighbours, q = Z p_new, (p, q) ---- */
 template <typename T, int CH>
-__global__ void __launch_bounds__ (ZS_THREADS, (CH * (16 / sizeof (T)) <= 8 ? 3 : 2))
+__global__ void __launch_bounds__ (ZS_THREADS, (CH * (16 / sizeof (T)) <= 8 ? 4 : 2))
 k_pcgx_pq (ZK z, const T *__restrict__ vals, const T *__restrict__ Zb,
            const T *__restrict__ Pold, T *__restrict__ Pnew,
            T *__restrict__ Qv, int ld, int nvec, int glog, int first,
            double *partA, unsigned *counter, double *scal, int *ival, int cap)
 {
   /* the next row's bounds and first G (column, value) pairs are loaded
-   * while the current row's neighbours are gathered (software pipeline) */
+   * while the current row's neighbours are gathered (software pipeline).
+   * The per-column beta and each lane's running (p, q) sums live in
+   * shared memory (the sums in the lane's own slots of the reduction
+   * area, added to in the same row order as register sums would be), which
+   * keeps the two-pack FP64 form within 64 registers: 4 CTAs per SM. */
   extern __shared__ double red[];
   ZS_GROUP_SETUP ();
   const double *beta = scal + S_BETA * cap;
-  T bet[CH][W];
+  T *bsm = reinterpret_cast<T *> (red + (size_t) ngroups * ld);
+  for (int c = threadIdx.x; c < ld; c += blockDim.x)
+    bsm[c] = first ? T (0) : (T) beta[c];
+  double *apq = red + (size_t) group * ld;
 #pragma unroll
-  for (int h = 0; h < CH; h++)
+  for (int h = 0; h < CH; h++) {
+    const int vi = lane + h * G;
+    if (vi < nvec)
 #pragma unroll
-    for (int e = 0; e < W; e++) {
-      const int c = (lane + h * G) * W + e;
-      bet[h][e] = (!first && c < ld) ? (T) beta[c] : T (0);
-    }
-  double aPQ[CH][W];
-#pragma unroll
-  for (int h = 0; h < CH; h++)
-#pragma unroll
-    for (int e = 0; e < W; e++) aPQ[h][e] = 0.;
+      for (int e = 0; e < W; e++) apq[vi * W + e] = 0.;
+  }
+  __syncthreads ();
   const int64_t stride = (int64_t) gridDim.x * ngroups;
   int64_t i = (int64_t) blockIdx.x * ngroups + group;
   int64_t k0 = 0, k1 = 0;
@@ -492,9 +495,10 @@ k_pcgx_pq (ZK z, const T *__restrict__ vals, const T *__restrict__ Zb,
           if (vi < nvec) {
             Pack<T> zj = ldp (Zb + (int64_t) c * ld + vi * W);
             Pack<T> pj = first ? pzero<T> () : ldp (Pold + (int64_t) c * ld + vi * W);
+            const Pack<T> bt = *reinterpret_cast<const Pack<T> *> (bsm + vi * W);
 #pragma unroll
             for (int e = 0; e < W; e++)
-              acc[h][e] = fma (v, fma (bet[h][e], pj.v[e], zj.v[e]), acc[h][e]);
+              acc[h][e] = fma (v, fma (bt.v[e], pj.v[e], zj.v[e]), acc[h][e]);
           }
         }
       }
@@ -512,11 +516,12 @@ k_pcgx_pq (ZK z, const T *__restrict__ vals, const T *__restrict__ Zb,
         Pack<T> zi = ldp (Zb + i * ld + vi * W);
         Pack<T> pi = first ? pzero<T> () : ldp (Pold + i * ld + vi * W);
         Pack<T> pn, q;
+        const Pack<T> bt = *reinterpret_cast<const Pack<T> *> (bsm + vi * W);
 #pragma unroll
         for (int e = 0; e < W; e++) {
-          pn.v[e] = fma (bet[h][e], pi.v[e], zi.v[e]);
+          pn.v[e] = fma (bt.v[e], pi.v[e], zi.v[e]);
           q.v[e] = acc[h][e];
-          aPQ[h][e] += (double) pn.v[e] * (double) q.v[e];
+          apq[vi * W + e] += (double) pn.v[e] * (double) q.v[e];
         }
         stp (Pnew + i * ld + vi * W, pn);
         stp (Qv + i * ld + vi * W, q);
@@ -527,7 +532,12 @@ k_pcgx_pq (ZK z, const T *__restrict__ vals, const T *__restrict__ Zb,
     mc = mcn;
     mv = mvn;
   }
-  block_colsum_store<T, CH> (aPQ, lane, group, G, nvec, ld, red, partA);
+  __syncthreads ();
+  for (int c = threadIdx.x; c < ld; c += blockDim.x) {
+    double sum = 0.;
+    for (int g = 0; g < ngroups; g++) sum += red[g * ld + c];
+    partA[(size_t) c * gridDim.x + blockIdx.x] = sum;
+  }
   const double *rz = scal + S_RZ * cap;
   double *al = scal + S_ALPHA * cap;
   int *act = ival + I_ACTIVE * cap;
@@ -803,6 +813,13 @@ zs_smem_bytes (int glog, int ld)
   return (ZS_THREADS >> glog) * ld * (int) sizeof (double);
 }
 
+/* k_pcgx_pq: the reduction area plus the per-column beta */
+static int
+zs_pq_smem_bytes (int glog, int ld)
+{
+  return zs_smem_bytes (glog, ld) + ld * (int) sizeof (double);
+}
+
 int
 ZWork::alloc (int64_t n_, int cap_, int is32_)
 {
@@ -1004,8 +1021,9 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
         if (tr) LGH_TRY (tr->begin (K_PCGX_PQ, zbytes + (it == 0 ? 3. : 4.) * bw, s));
         ZS_DISPATCH (ch, {
           auto k1 = k_pcgx_pq<T, CH_>;
-          set_smem_attr (k1, smem);
-          k1<<<fit_grid (k1, grid, ZS_THREADS, smem), ZS_THREADS, smem, s>>> (zk, vals, bZ, Pold, Pnew, bQ, ldt,
+          const int psm = zs_pq_smem_bytes (glog, ldt);
+          set_smem_attr (k1, psm);
+          k1<<<fit_grid (k1, grid, ZS_THREADS, psm), ZS_THREADS, psm, s>>> (zk, vals, bZ, Pold, Pnew, bQ, ldt,
                                              nvec, glog, it == 0, ws.partA.p,
                                              ws.counters.p, ws.scal.p,
                                              ws.ival.p, cap);
@@ -1239,7 +1257,7 @@ server_tick_pq (const Csr &Z, const T *Zb, const T *Pold, T *Pnew, T *Q, int ld,
   int glog, ch;
   row_group_shape (nvec, glog, ch);
   const int grid = std::min (row_grid (Z.n, glog), ws.nblocks);
-  const int smem = zs_smem_bytes (glog, ld);
+  const int smem = zs_pq_smem_bytes (glog, ld);
   ZK zk{ Z.n, Z.rowptr, Z.colidx };
   ZS_DISPATCH (ch, {
     auto k1 = k_pcgx_pq<T, CH_>;
