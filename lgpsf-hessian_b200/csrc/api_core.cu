@@ -262,11 +262,18 @@ __global__ void
 k_check_csr (int64_t n, int64_t ncols, const int64_t *rowptr, const int32_t *col,
              int *bad)
 {
+  /* bad[0]: malformed row pointers (1) or a column out of range (2);
+   * bad[1]: the bandwidth max |j - i| (clamped to INT_MAX) */
   for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t) gridDim.x * blockDim.x) {
     if (rowptr[i + 1] < rowptr[i]) { atomicExch (bad, 1); continue; }
-    for (int64_t k = rowptr[i]; k < rowptr[i + 1]; k++)
+    int64_t bw = 0;
+    for (int64_t k = rowptr[i]; k < rowptr[i + 1]; k++) {
       if (col[k] < 0 || col[k] >= ncols) atomicExch (bad, 2);
+      const int64_t d = col[k] > i ? col[k] - i : i - col[k];
+      if (d > bw) bw = d;
+    }
+    if (bw > 0) atomicMax (bad + 1, (int) (bw < 0x7fffffff ? bw : 0x7fffffff));
   }
 }
 
@@ -288,6 +295,7 @@ csr_finish (Csr &A)
   LGH_CUDA (cudaMemcpyAsync (h, flags.p, 2 * sizeof (int), cudaMemcpyDeviceToHost, s));
   LGH_CUDA (cudaStreamSynchronize (s));
   LGH_CHECK (h[0] == 0, LGH_ERR_ARG_WRONG, "csr: malformed row pointers or column index out of range");
+  A.bandwidth = h[1];
   LGH_CUDA (cudaMemsetAsync (flags.p, 0, sizeof (int), s));
   k_csr_diag<<<grid, 256, 0, s>>> (A.n, A.rowptr, A.colidx, A.vals, A.dinv,
                                    A.dinv32, A.vals32, flags.p);

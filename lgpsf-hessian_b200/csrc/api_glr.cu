@@ -646,7 +646,10 @@ batch_op (lgh_glr_t *g, int kind, int nshift, const double *c, int m,
   std::vector<double> ch (nshift);
   LGH_CUDA (cudaMemcpy (ch.data (), c, nshift * sizeof (double), cudaMemcpyDefault));
   for (int i = 0; i < nshift; i++) LGH_TRY (check_shift (g, ch[i], "batch"));
-  LGH_TRY (ensure_wz (g));
+  /* one shift and no W yet: the per-call formula of glr_common_impl.h:
+   * 1007-1024 / 1084-1091 (the same Z-solves of width m, no W) */
+  const bool direct = nshift == 1 && !g->have_wz && g->kept > 0;
+  if (!direct) LGH_TRY (ensure_wz (g));
   const int ldm = round_ld (m), kept = g->kept;
   DBuf<double> R, Y0, Xs, Wc, Dc, work;
   LGH_TRY (R.alloc ((size_t) n * ldm));
@@ -666,6 +669,20 @@ batch_op (lgh_glr_t *g, int kind, int nshift, const double *c, int m,
   if (kept > 0)
     LGH_TRY (launch_gemm_tn<double> (n, kept, m, g->U.p, g->ldu, R.p, ldm, Wc.p,
                                      kept, 0, work.p, work.n, s));
+  if (direct) {
+    /* t = f(c) r2 + U diag(f(lam + c) - f(c)) U^T r2, x = Z^{-1} M^{1/2} t */
+    const double cs = ch[0];
+    const double fc = (kind == 0) ? 1. / cs : 1. / sqrt (cs);
+    k_shift_coef<<<sgrid ((int64_t) kept * m), 256, 0, s>>> (kept, m, g->lam_d.p, cs,
+                                                            kind, Wc.p, Dc.p);
+    LGH_LAUNCH_CHECK ();
+    LGH_TRY (launch_gemm_nn<double> (n, kept, m, 1.0, g->U.p, g->ldu, Dc.p, kept, fc,
+                                     R.p, ldm, Xs.p, ldm, s));
+    LGH_TRY (glr_zsolve (g, m, Xs.p, ldm, ms, Y0.p, ldm, nullptr));
+    LGH_TRY (launch_rowmajor_to_colmajor (n, m, Y0.p, ldm, x, ldx, nullptr, s));
+    LGH_CUDA (cudaStreamSynchronize (s));
+    return 0;
+  }
   LGH_TRY (glr_zsolve (g, m, R.p, ldm, ms, Y0.p, ldm, nullptr));
   for (int si = 0; si < nshift; si++) {
     const double cs = ch[si];

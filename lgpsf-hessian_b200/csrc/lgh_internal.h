@@ -142,6 +142,7 @@ struct Csr
                                dependent gather of the diagonal */
   float *vd32 = nullptr;
   int max_row_nnz = 0;
+  int64_t bandwidth = 0;    /* max |j - i| over the entries */
 };
 
 /* ---- kernel launchers (k_*.cu) ------------------------------------------ */

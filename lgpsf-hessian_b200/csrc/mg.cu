@@ -26,6 +26,9 @@
 
 #include <omp.h>
 
+#include <stdio.h>
+#include <stdlib.h>
+
 #include <algorithm>
 #include <type_traits>
 #include <vector>
@@ -423,10 +426,16 @@ mg_build (const Csr &Z, int tile, double smoother_top, int nu, Hierarchy **out)
 {
   (void) tile;
   const double t0 = wall ();
+  /* phase seconds: download, Lanczos, coarsen, Galerkin products, uploads,
+   * coarse inverse (printed to stderr when LGH_MG_VERBOSE is set) */
+  double tp[6] = { 0., 0., 0., 0., 0., 0. };
+  double tq = wall ();
+  auto lap = [&] (int k) { const double t = wall (); tp[k] += t - tq; tq = t; };
   Hierarchy *h = new Hierarchy ();
   HCsr A;
   int rc = csr_download (Z, A);
   if (rc) { delete h; return rc; }
+  lap (0);
   const int64_t coarse_max = 1500;
   const double theta = 0.0;
   for (int l = 0; l < 12; l++) {
@@ -439,6 +448,7 @@ mg_build (const Csr &Z, int tile, double smoother_top, int nu, Hierarchy **out)
     const double lmax_own = (l == 0) ? lv.smax : lanczos_lmax (A, 40, 20260813ULL);
     lv.slo = 0.1 * lv.smax;
     lv.shi = smoother_top * lv.smax;
+    lap (1);
     if (l == 0) {
       lv.A = Z;
       lv.own = 0;
@@ -446,6 +456,7 @@ mg_build (const Csr &Z, int tile, double smoother_top, int nu, Hierarchy **out)
       rc = csr_upload (A, lv.A);
       if (rc) { delete h; return rc; }
     }
+    lap (4);
     if (A.n <= coarse_max || l == 11) {
       /* coarsest: dense inverse on the device, A^{-1} = L^{-T} L^{-1} */
       const int n0 = (int) A.n;
@@ -481,11 +492,13 @@ mg_build (const Csr &Z, int tile, double smoother_top, int nu, Hierarchy **out)
       if (rc) { delete h; return rc; }
       h->lev.push_back (lv);
       lv.own = 0;  /* ownership moved into h->lev */
+      lap (5);
       break;
     }
     HCsr P;
     int64_t nc = 0;
     sa_coarsen (A, theta, lmax_own, P, nc);
+    lap (2);
     if (nc >= A.n) {
       /* no coarsening progress: stop here with a dense coarse level is
        * impossible at this size */
@@ -504,13 +517,20 @@ mg_build (const Csr &Z, int tile, double smoother_top, int nu, Hierarchy **out)
           Ac.v[k] = 0.5 * (Ac.v[k] + AcT.v[kt]);
     }
     Ac.m = Ac.n;
+    lap (3);
     rc = csr_upload (P, lv.P);
     if (!rc) rc = csr_upload (R, lv.R);
     if (rc) { delete h; return rc; }
     h->lev.push_back (lv);
     A = std::move (Ac);
+    lap (4);
   }
   h->setup_s = wall () - t0;
+  if (getenv ("LGH_MG_VERBOSE"))
+    fprintf (stderr, "mg setup %.4f s: download %.4f lanczos %.4f coarsen %.4f "
+             "galerkin %.4f upload %.4f coarse %.4f (levels %zu, coarse n %d)\n",
+             h->setup_s, tp[0], tp[1], tp[2], tp[3], tp[4], tp[5],
+             h->lev.size (), h->n0);
   *out = h;
   return 0;
 }

@@ -1319,6 +1319,18 @@ template int server_tick_dots<double> (const Csr &, const double *,
                                        const double *, int, int, const int *,
                                        double, ZWork &, cudaStream_t);
 
+/* L2 bytes the smoother's neighbour reuse may span: a row's r and d rows
+ * are gathered again by the rows up to the bandwidth away, so the band of
+ * 2 bandwidth rows of both blocks must stay in L2 (126 MB, shared with the
+ * streaming writes).  A wider band is swept in column slices.
+ * LGH_CHEB_L2MB overrides the budget (0: never slice). */
+static double
+cheb_l2_budget ()
+{
+  const char *e = getenv ("LGH_CHEB_L2MB");
+  return (e ? atof (e) : 40.0) * 1048576.0;
+}
+
 /* one Chebyshev-Jacobi step on a CSR operator (the multigrid smoother and
  * the fixed-count Chebyshev mode) */
 template <typename T>
@@ -1327,20 +1339,34 @@ launch_cheb_step (const Csr &A, T *X, const T *Ro, T *Rn, const T *Do, T *Dn,
                   int ld, double a, double b, int flags, cudaStream_t s)
 {
   constexpr int W = Pack<T>::W;
-  const int nvec = ld / W;
-  int glog, ch;
-  row_group_shape (nvec, glog, ch);
-  const int grid = std::min (row_grid (A.n, glog), num_sms () * 8);
+  const int nvec_all = ld / W;
   ZK zk{ A.n, A.rowptr, A.colidx };
   const T *vals = zvals<T> (A);
   const T *dinv = zdinv<T> (A);
-  ZS_DISPATCH (ch, {
-    k_cheb<T, CH_><<<fit_grid (k_cheb<T, CH_>, grid, ZS_THREADS, 0),
-                                          ZS_THREADS, 0, s>>> (zk, vals, zvd<T> (A), dinv, X, Ro, Rn, Do,
-                                                Dn, ld, nvec, glog, (T) a,
-                                                (T) b, flags);
-  });
-  LGH_LAUNCH_CHECK ();
+  /* column slices of whole packs so that each slice's reuse band fits */
+  const double band = 2. * 2. * (double) A.bandwidth * ld * sizeof (T);
+  const double budget = cheb_l2_budget ();
+  int slices = 1;
+  if (budget > 0. && band > budget)
+    slices = std::min (nvec_all, (int) std::ceil (band / budget));
+  for (int sl = 0; sl < slices; sl++) {
+    const int v0 = (int) ((int64_t) nvec_all * sl / slices);
+    const int v1 = (int) ((int64_t) nvec_all * (sl + 1) / slices);
+    const int nvec = v1 - v0;
+    if (nvec <= 0) continue;
+    const int c0 = v0 * W;
+    int glog, ch;
+    row_group_shape (nvec, glog, ch);
+    const int grid = std::min (row_grid (A.n, glog), num_sms () * 8);
+    ZS_DISPATCH (ch, {
+      k_cheb<T, CH_><<<fit_grid (k_cheb<T, CH_>, grid, ZS_THREADS, 0),
+                                            ZS_THREADS, 0, s>>> (zk, vals, zvd<T> (A), dinv, X + c0, Ro + c0,
+                                                  Rn + c0, Do ? Do + c0 : nullptr,
+                                                  Dn ? Dn + c0 : nullptr, ld, nvec, glog,
+                                                  (T) a, (T) b, flags);
+    });
+    LGH_LAUNCH_CHECK ();
+  }
   return 0;
 }
 

@@ -83,3 +83,20 @@ def test_cheb_step_matches_numpy(ops, name, fp32):
             # deterministic: the same call gives the same bits
             x2, r2, _ = L.test_cheb_step(M, X, R, D, a, b, fl, fp32)
             assert np.array_equal(x1, x2) and np.array_equal(r1, r2)
+
+
+def test_cheb_step_column_slices_same_bits(ops, monkeypatch):
+    """An operator whose neighbour band would not fit the L2 budget is swept
+    in column slices; the slices give the same bits as one sweep."""
+    A, M = ops["z3d"]
+    n = A["n"]
+    rng = np.random.default_rng(23)
+    X, R, D = (rng.standard_normal((n, 220)) for _ in range(3))
+    out = {}
+    for budget in ("0", "0.05"):     # never slice / slice into many
+        monkeypatch.setenv("LGH_CHEB_L2MB", budget)
+        out[budget] = [L.test_cheb_step(M, X, R, D, 0.37, 0.81, fl)
+                       for fl in FLAGS]
+    for a, b in zip(out["0"], out["0.05"]):
+        for u, v in zip(a, b):
+            assert np.array_equal(u, v)

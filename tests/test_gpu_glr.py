@@ -213,6 +213,31 @@ def test_batch_matches_single():
         assert abs(ld[si] - g.logdet(c)) <= 1e-14 * abs(ld[si])
 
 
+def test_single_shift_batch_before_and_after_w():
+    """One shift on an object without W = Z^{-1} M^{1/2} U takes the
+    per-call formula (no W); once W exists (a multi-shift call builds it)
+    the same call goes through W.  Both agree with the single-vector
+    operations."""
+    cfg, keep = _c1()
+    B, Z, pr = keep
+    g = L.Glr(B, pr, L.glr_opts(ell=40, seed=0, check=0))
+    rng = np.random.default_rng(4)
+    R = rng.standard_normal((cfg["N"], 5))
+    c = 0.3
+    x_direct = g.solve_batch([c], R)[0]
+    s_direct = g.sample_batch([c], R)[0]
+    g.solve_batch([c, 2 * c], R[:, :1])          # builds W
+    x_w = g.solve_batch([c], R)[0]
+    s_w = g.sample_batch([c], R)[0]
+    for j in range(R.shape[1]):
+        ref = g.solve(c, R[:, j])
+        refs = g.sample(c, R[:, j])
+        assert _rd(x_direct[:, j], ref) < 1e-8
+        assert _rd(x_w[:, j], ref) < 1e-8
+        assert _rd(s_direct[:, j], refs) < 1e-8
+        assert _rd(s_w[:, j], refs) < 1e-8
+
+
 def test_sample_covariance_is_inverse_model_hessian():
     """x = G^{-T} xi has covariance H~(c)^{-1} exactly: the linear map S of
     sample satisfies S S^T = H~(c)^{-1} with H~ = Z M^{-1/2}(U L U^T + cI)
