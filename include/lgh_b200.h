@@ -372,6 +372,12 @@ typedef struct lgh_server_stats
   long   harvests;
   /* the copier thread's seconds moving inputs up and results down        */
   double t_up_s, t_down_s;
+  /* mean fraction of the slots occupied per tick, and the mean seconds a
+   * completed solve / sample request spent in each stage: submit to input
+   * staged, staged to first column placed, first column placed to last
+   * column harvested, last harvest to result on the host                 */
+  double occupancy;
+  double wait_stage_s, wait_admit_s, run_s, copy_out_s;
 }
 lgh_server_stats_t;
 

@@ -183,6 +183,7 @@ struct SReq
   cudaEvent_t ev_out = nullptr;   /* recorded after the last scatter      */
   int status = 1;     /* 1 pending/active, 0 done, < 0 error              */
   double t_submit = 0., t_done = 0.;
+  double t_staged = 0., t_placed = 0., t_ran = 0.;   /* stage timestamps */
 };
 
 struct Slot
@@ -258,6 +259,9 @@ struct lgh_server
   long completed = 0;
   std::atomic<long> ticks{ 0 }, cols_done{ 0 }, harvests{ 0 };   /* loop-written */
   double t_admit = 0., t_tick = 0., t_harvest = 0., t_up = 0., t_down = 0.;
+  double occ_sum = 0.;                 /* occupied slots summed over ticks */
+  double st_stage = 0., st_admit = 0., st_run = 0., st_out = 0.;
+  long st_n = 0;                       /* solve / sample requests timed   */
   std::vector<double> lat;
   double t0 = 0., t_last = 0.;
 };
@@ -304,6 +308,13 @@ srv_finish (lgh_server_t *sv, SReq *r, int rc)
     sv->lat.push_back (r->t_done - r->t_submit);
     sv->completed++;
     sv->t_last = r->t_done;
+    if (r->kind != 2) {
+      sv->st_stage += r->t_staged - r->t_submit;
+      sv->st_admit += r->t_placed - r->t_staged;
+      sv->st_run += r->t_ran - r->t_placed;
+      sv->st_out += r->t_done - r->t_ran;
+      sv->st_n++;
+    }
   }
   sv->done_cv.notify_all ();
   sv->ccv.notify_all ();
@@ -455,6 +466,7 @@ srv_copier (lgh_server_t *sv)
       if (rc) { srv_fail (sv, rc); return; }
       std::lock_guard<std::mutex> lk (sv->mu);
       sv->t_up += wall () - w0;
+      up->t_staged = wall ();
       up->staged = 1;
       sv->staged_cols += up->m;
       sv->cv.notify_all ();
@@ -527,6 +539,7 @@ srv_start (lgh_server_t *sv, const Adm &a, double *Pold)
   double *X = (double *) sv->ws.X.p, *R = (double *) sv->ws.R.p;
   if (a.j0 == 0) {
     r->cols_left = r->m;
+    r->t_placed = wall ();
     if (r->kind == 1 && kept > 0) {
       for (int c0 = 0; c0 < r->m; c0 += sv->cap) {
         const int mc = std::min (sv->cap, r->m - c0);
@@ -636,7 +649,9 @@ srv_harvest (lgh_server_t *sv, const std::vector<int> &act, double *Pold)
     LGH_LAUNCH_CHECK ();
     sv->cols_done += kb;
   }
+  const double tr = wall ();
   for (SReq *r : fin) {
+    r->t_ran = tr;
     LGH_CUDA (cudaEventCreateWithFlags (&r->ev_out, cudaEventDisableTiming));
     LGH_CUDA (cudaEventRecord (r->ev_out, s));
   }
@@ -704,6 +719,7 @@ srv_loop (lgh_server_t *sv)
       if (ge) { cudaGraphExecDestroy (ge); ge = nullptr; }
   };
   double ta = 0., tt = 0., th = 0.;   /* phase seconds, published per tick */
+  double occ = 0.;                    /* occupied slots summed over ticks */
   while (!sv->stop.load () && !sv->failed.load ()) {
     /* 1. admission into free slots */
     double w0 = wall ();
@@ -775,14 +791,15 @@ srv_loop (lgh_server_t *sv)
     tt += wall () - w0;
     if (!rc) {
       memcpy (act.data (), sv->act_pin, sv->cap * sizeof (int));
-      int occ = 0, conv = 0;
+      int occ_n = 0, conv = 0;
       for (int sl = 0; sl < sv->cap; sl++)
         if (sv->slots[sl].req) {
-          occ++;
+          occ_n++;
           conv += act[sl] == 0;
         }
+      occ += occ_n;
       if (conv > 0) hold++;
-      if (conv > 0 && (conv >= batch || conv == occ || hold >= 3)) {
+      if (conv > 0 && (conv >= batch || conv == occ_n || hold >= 3)) {
         w0 = wall ();
         rc = srv_harvest (sv, act, Pold);
         th += wall () - w0;
@@ -794,6 +811,7 @@ srv_loop (lgh_server_t *sv)
       sv->t_admit = ta;
       sv->t_tick = tt;
       sv->t_harvest = th;
+      sv->occ_sum = occ;
     }
     if (rc) { release_graphs (); srv_fail (sv, rc); return; }
   }
@@ -996,6 +1014,13 @@ lgh_server_get_stats (lgh_server_t *sv, lgh_server_stats_t *st)
   st->harvests = sv->harvests;
   st->t_up_s = sv->t_up;
   st->t_down_s = sv->t_down;
+  st->occupancy = sv->ticks > 0 ? sv->occ_sum / ((double) sv->ticks * sv->cap) : 0.;
+  if (sv->st_n > 0) {
+    st->wait_stage_s = sv->st_stage / sv->st_n;
+    st->wait_admit_s = sv->st_admit / sv->st_n;
+    st->run_s = sv->st_run / sv->st_n;
+    st->copy_out_s = sv->st_out / sv->st_n;
+  }
   return 0;
 }
 

@@ -93,7 +93,11 @@ class ServerStats(ctypes.Structure):
                 ("max_s", ctypes.c_double), ("columns_per_s", ctypes.c_double),
                 ("t_admit_s", ctypes.c_double), ("t_tick_s", ctypes.c_double),
                 ("t_harvest_s", ctypes.c_double), ("harvests", ctypes.c_long),
-                ("t_up_s", ctypes.c_double), ("t_down_s", ctypes.c_double)]
+                ("t_up_s", ctypes.c_double), ("t_down_s", ctypes.c_double),
+                ("occupancy", ctypes.c_double),
+                ("wait_stage_s", ctypes.c_double),
+                ("wait_admit_s", ctypes.c_double), ("run_s", ctypes.c_double),
+                ("copy_out_s", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
