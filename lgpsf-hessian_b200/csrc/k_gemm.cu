@@ -11,9 +11,16 @@
  *            triangular update X L^{-T} of CholQR2 (:402), U = Q C_kept
  *            (:567), Y += U W (:876).  64 x 64 tiles, k in steps of 16.
  *
- * Each thread accumulates a 4 x 4 register tile; operands are staged in
- * shared memory with 16-byte vector loads.  These products are O(n ell^2)
- * and bounded by the FP64 (or, for float blocks, FP32) pipe.
+ *   dense_apply  Y = A^{-1} B on the multigrid's dense coarse level.
+ *
+ * All three run on the FP64 tensor cores: a CTA of 4 warps owns a 64 x 64
+ * output tile, each warp a 32 x 32 quarter of 4 x 4 mma.sync m8n8k4 f64
+ * tiles; operands are staged k-major in shared memory 16 k-values at a
+ * time (rows padded to 68 doubles so that a fragment load touches 16
+ * distinct bank pairs), and the next stage is read into registers while
+ * the current one is multiplied.  Float blocks (mixed path) are widened to
+ * FP64 as they are staged; every product accumulates in FP64.  These
+ * products are O(n ell^2) and bounded by the FP64 tensor pipe.
  */
 
 #include <algorithm>
@@ -25,58 +32,103 @@ namespace lgh
 {
 
 constexpr int GB = 64, GK = 16;
+constexpr int SLD = GB + 4;   /* shared row stride, doubles */
 
+/* one staged k block: As[k][i] (k-major), Bs[k][j]; warp (wm, wn) adds
+ * its 32 x 32 quarter.  m8n8k4 f64 fragments: A (8 x 4, row) holds
+ * A[lane / 4][lane % 4], B (4 x 8, col) holds B[lane % 4][lane / 4],
+ * C holds C[lane / 4][2 (lane % 4) + {0, 1}]. */
+__device__ __forceinline__ void
+dmma_block (const double (*As)[SLD], const double (*Bs)[SLD], int wm, int wn,
+            int lane, double (&acc)[4][4][2])
+{
+#pragma unroll
+  for (int kk = 0; kk < GK; kk += 4) {
+    double a[4], b[4];
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      a[t] = As[kk + (lane & 3)][wm * 32 + t * 8 + (lane >> 2)];
+      b[t] = Bs[kk + (lane & 3)][wn * 32 + t * 8 + (lane >> 2)];
+    }
+#pragma unroll
+    for (int ti = 0; ti < 4; ti++)
+#pragma unroll
+      for (int tj = 0; tj < 4; tj++)
+        asm volatile ("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 "
+                      "{%0, %1}, {%2}, {%3}, {%0, %1};"
+                      : "+d"(acc[ti][tj][0]), "+d"(acc[ti][tj][1])
+                      : "d"(a[ti]), "d"(b[tj]));
+  }
+}
+
+/* the C element of acc[ti][tj][c] inside the CTA tile */
+__device__ __forceinline__ int
+dmma_row (int wm, int ti, int lane)
+{
+  return wm * 32 + ti * 8 + (lane >> 2);
+}
+
+__device__ __forceinline__ int
+dmma_col (int wn, int tj, int c, int lane)
+{
+  return wn * 32 + tj * 8 + (lane & 3) * 2 + c;
+}
+
+/* partial C = A^T B over rows [kb0, kb1) of row-major A (n x m1), B
+ * (n x m2), into work[z] (column-major m1 x m2) */
 template <typename T>
-__global__ void __launch_bounds__ (256)
+__global__ void __launch_bounds__ (128)
 k_gemm_tn_part (int64_t n, int m1, int m2, const T *__restrict__ A, int lda,
                 const T *__restrict__ B, int ldb, double *__restrict__ work,
                 int64_t kchunk)
 {
-  __shared__ double As[GK][GB + 1], Bs[GK][GB + 1];
-  const int tid = threadIdx.x;
-  const int tx = tid & 15, ty = tid >> 4;
+  __shared__ double As[GK][SLD], Bs[GK][SLD];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
   const int i0 = blockIdx.x * GB, j0 = blockIdx.y * GB;
   const int64_t kb0 = (int64_t) blockIdx.z * kchunk;
   int64_t kb1 = kb0 + kchunk;
   if (kb1 > n) kb1 = n;
-  double acc[4][4];
+  double acc[4][4][2];
 #pragma unroll
   for (int a = 0; a < 4; a++)
 #pragma unroll
-    for (int b = 0; b < 4; b++) acc[a][b] = 0.;
-  const int lr = tid >> 4;        /* 0..15 : k row in tile   */
-  const int lc = (tid & 15) * 4;  /* 0..60 : 4 columns       */
-  for (int64_t k0 = kb0; k0 < kb1; k0 += GK) {
-    const int64_t kr = k0 + lr;
+    for (int b = 0; b < 4; b++) acc[a][b][0] = acc[a][b][1] = 0.;
+  /* staging: thread -> k row (tid / 8), 8 consecutive columns */
+  const int lk = tid >> 3, lc = (tid & 7) * 8;
+  double ra[8], rb[8];
+  auto fetch = [&] (int64_t k0) {
+    const int64_t kr = k0 + lk;
+    const bool rin = kr < kb1;
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
+    for (int e = 0; e < 8; e++) {
       const int ci = i0 + lc + e, cj = j0 + lc + e;
-      As[lr][lc + e] = (kr < kb1 && ci < m1) ? (double) A[kr * lda + ci] : 0.;
-      Bs[lr][lc + e] = (kr < kb1 && cj < m2) ? (double) B[kr * ldb + cj] : 0.;
+      ra[e] = (rin && ci < m1) ? (double) A[kr * lda + ci] : 0.;
+      rb[e] = (rin && cj < m2) ? (double) B[kr * ldb + cj] : 0.;
+    }
+  };
+  if (kb0 < kb1) fetch (kb0);
+  for (int64_t k0 = kb0; k0 < kb1; k0 += GK) {
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      As[lk][lc + e] = ra[e];
+      Bs[lk][lc + e] = rb[e];
     }
     __syncthreads ();
-#pragma unroll
-    for (int kk = 0; kk < GK; kk++) {
-      double av[4], bv[4];
-#pragma unroll
-      for (int a = 0; a < 4; a++) av[a] = As[kk][ty + 16 * a];
-#pragma unroll
-      for (int b = 0; b < 4; b++) bv[b] = Bs[kk][tx + 16 * b];
-#pragma unroll
-      for (int a = 0; a < 4; a++)
-#pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = fma (av[a], bv[b], acc[a][b]);
-    }
+    if (k0 + GK < kb1) fetch (k0 + GK);   /* next stage behind the mma */
+    dmma_block (As, Bs, wm, wn, lane, acc);
     __syncthreads ();
   }
   double *wz = work + (size_t) blockIdx.z * m1 * m2;
 #pragma unroll
-  for (int a = 0; a < 4; a++)
+  for (int ti = 0; ti < 4; ti++)
 #pragma unroll
-    for (int b = 0; b < 4; b++) {
-      const int i = i0 + ty + 16 * a, j = j0 + tx + 16 * b;
-      if (i < m1 && j < m2) wz[i + (size_t) j * m1] = acc[a][b];
-    }
+    for (int tj = 0; tj < 4; tj++)
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const int i = i0 + dmma_row (wm, ti, lane), j = j0 + dmma_col (wn, tj, c, lane);
+        if (i < m1 && j < m2) wz[i + (size_t) j * m1] = acc[ti][tj][c];
+      }
 }
 
 __global__ void
@@ -102,8 +154,9 @@ k_gemm_tn_reduce (int m1, int m2, int nsplit, const double *__restrict__ work,
 static int
 tn_splits (int64_t n, int m1, int m2)
 {
+  /* about 4 resident 4-warp CTAs per SM over all tiles and slices */
   const int tiles = ((m1 + GB - 1) / GB) * ((m2 + GB - 1) / GB);
-  int want = (2 * num_sms () + tiles - 1) / tiles;
+  int want = (4 * num_sms () + tiles - 1) / tiles;
   int64_t maxs = (n + 255) / 256;
   if (want > maxs) want = (int) maxs;
   if (want < 1) want = 1;
@@ -131,7 +184,7 @@ launch_gemm_tn (int64_t n, int m1, int m2, const T *A, int lda, const T *B,
   int64_t kchunk = (n + ns - 1) / ns;
   kchunk = (kchunk + GK - 1) / GK * GK;
   dim3 grid ((m1 + GB - 1) / GB, (m2 + GB - 1) / GB, ns);
-  k_gemm_tn_part<T><<<grid, 256, 0, s>>> (n, m1, m2, A, lda, B, ldb, work,
+  k_gemm_tn_part<T><<<grid, 128, 0, s>>> (n, m1, m2, A, lda, B, ldb, work,
                                           kchunk);
   LGH_LAUNCH_CHECK ();
   const int64_t total = (int64_t) m1 * m2;
@@ -153,7 +206,7 @@ launch_gemm_tn_fixed (int64_t n, int m1, int m2, const double *A, int lda,
   int64_t kchunk = (n + nsplit - 1) / nsplit;
   kchunk = (kchunk + GK - 1) / GK * GK;
   dim3 grid ((m1 + GB - 1) / GB, (m2 + GB - 1) / GB, nsplit);
-  k_gemm_tn_part<double><<<grid, 256, 0, s>>> (n, m1, m2, A, lda, B, ldb,
+  k_gemm_tn_part<double><<<grid, 128, 0, s>>> (n, m1, m2, A, lda, B, ldb,
                                                work, kchunk);
   LGH_LAUNCH_CHECK ();
   const int64_t total = (int64_t) m1 * m2;
@@ -176,61 +229,130 @@ template int launch_gemm_tn<float> (int64_t, int, int, const float *, int,
                                     const float *, int, double *, int, int,
                                     double *, size_t, cudaStream_t);
 
+/* Y = alpha X M + beta Y0: X row-major n x k, M column-major k x m2 */
 template <typename T>
-__global__ void __launch_bounds__ (256)
+__global__ void __launch_bounds__ (128)
 k_gemm_nn (int64_t n, int k, int m2, double alpha, const T *__restrict__ X,
            int ldx, const double *__restrict__ M, int ldm, double beta,
            const T *Y0, int ldy0, T *Y, int ldy)
 {
-  __shared__ double Xs[GB][GK + 1], Ms[GK][GB + 1];
-  const int tid = threadIdx.x;
-  const int tx = tid & 15, ty = tid >> 4;
+  __shared__ double As[GK][SLD], Bs[GK][SLD];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
   const int64_t i0 = (int64_t) blockIdx.x * GB;
   const int j0 = blockIdx.y * GB;
-  double acc[4][4];
+  double acc[4][4][2];
 #pragma unroll
   for (int a = 0; a < 4; a++)
 #pragma unroll
-    for (int b = 0; b < 4; b++) acc[a][b] = 0.;
-  const int xr = tid >> 2, xk = (tid & 3) * 4;  /* X tile: 64 rows x 16 k */
-  const int mj = tid >> 2, mk = (tid & 3) * 4;  /* M tile: 16 k x 64 cols */
-  for (int k0 = 0; k0 < k; k0 += GK) {
-    const int64_t gi = i0 + xr;
+    for (int b = 0; b < 4; b++) acc[a][b][0] = acc[a][b][1] = 0.;
+  /* staging: thread -> tile row / column (tid / 2), 8 consecutive k */
+  const int lr = tid >> 1, lk = (tid & 1) * 8;
+  double ra[8], rb[8];
+  auto fetch = [&] (int k0) {
+    const int64_t gi = i0 + lr;
+    const int gj = j0 + lr;
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
-      const int kk = k0 + xk + e;
-      Xs[xr][xk + e] = (gi < n && kk < k) ? (double) X[gi * ldx + kk] : 0.;
-      const int gj = j0 + mj, mkk = k0 + mk + e;
-      Ms[mk + e][mj] = (gj < m2 && mkk < k) ? M[mkk + (size_t) gj * ldm] : 0.;
+    for (int e = 0; e < 8; e++) {
+      const int kk = k0 + lk + e;
+      ra[e] = (gi < n && kk < k) ? (double) X[gi * ldx + kk] : 0.;
+      rb[e] = (gj < m2 && kk < k) ? M[kk + (size_t) gj * ldm] : 0.;
+    }
+  };
+  if (k > 0) fetch (0);
+  for (int k0 = 0; k0 < k; k0 += GK) {
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      As[lk + e][lr] = ra[e];
+      Bs[lk + e][lr] = rb[e];
     }
     __syncthreads ();
-#pragma unroll
-    for (int kk = 0; kk < GK; kk++) {
-      double xv[4], mv[4];
-#pragma unroll
-      for (int a = 0; a < 4; a++) xv[a] = Xs[ty + 16 * a][kk];
-#pragma unroll
-      for (int b = 0; b < 4; b++) mv[b] = Ms[kk][tx + 16 * b];
-#pragma unroll
-      for (int a = 0; a < 4; a++)
-#pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = fma (xv[a], mv[b], acc[a][b]);
-    }
+    if (k0 + GK < k) fetch (k0 + GK);
+    dmma_block (As, Bs, wm, wn, lane, acc);
     __syncthreads ();
   }
 #pragma unroll
+  for (int ti = 0; ti < 4; ti++)
+#pragma unroll
+    for (int tj = 0; tj < 4; tj++)
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const int64_t i = i0 + dmma_row (wm, ti, lane);
+        const int j = j0 + dmma_col (wn, tj, c, lane);
+        if (i < n && j < m2) {
+          double v = alpha * acc[ti][tj][c];
+          if (beta != 0.) v += beta * (double) Y0[i * ldy0 + j];
+          Y[i * ldy + j] = (T) v;
+        }
+      }
+}
+
+/* Y = A^{-1} B on the dense coarse level: A^{-1} n0 x n0 column-major,
+ * B and Y n0 x ld row-major; columns w .. ld - 1 of Y are set to zero */
+template <typename T>
+__global__ void __launch_bounds__ (128)
+k_dense_apply (int n0, const double *__restrict__ Ainv, const T *__restrict__ B,
+               T *__restrict__ Y, int w, int ld)
+{
+  __shared__ double As[GK][SLD], Bs[GK][SLD];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  const int i0 = blockIdx.x * GB, c0 = blockIdx.y * GB;
+  double acc[4][4][2];
+#pragma unroll
   for (int a = 0; a < 4; a++)
 #pragma unroll
-    for (int b = 0; b < 4; b++) {
-      const int64_t i = i0 + ty + 16 * a;
-      const int j = j0 + tx + 16 * b;
-      if (i < n && j < m2) {
-        double v = alpha * acc[a][b];
-        if (beta != 0.) v += beta * (double) Y0[i * ldy0 + j];
-        Y[i * ldy + j] = (T) v;
-      }
+    for (int b = 0; b < 4; b++) acc[a][b][0] = acc[a][b][1] = 0.;
+  /* staging: thread -> k row (tid / 8), 8 consecutive rows / columns */
+  const int lk = tid >> 3, lc = (tid & 7) * 8;
+  double ra[8], rb[8];
+  auto fetch = [&] (int k0) {
+    const int gk = k0 + lk;
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      const int gi = i0 + lc + e, gc = c0 + lc + e;
+      ra[e] = (gk < n0 && gi < n0) ? Ainv[gi + (size_t) gk * n0] : 0.;
+      rb[e] = (gk < n0 && gc < w) ? (double) B[(size_t) gk * ld + gc] : 0.;
     }
+  };
+  fetch (0);
+  for (int k0 = 0; k0 < n0; k0 += GK) {
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      As[lk][lc + e] = ra[e];
+      Bs[lk][lc + e] = rb[e];
+    }
+    __syncthreads ();
+    if (k0 + GK < n0) fetch (k0 + GK);
+    dmma_block (As, Bs, wm, wn, lane, acc);
+    __syncthreads ();
+  }
+#pragma unroll
+  for (int ti = 0; ti < 4; ti++)
+#pragma unroll
+    for (int tj = 0; tj < 4; tj++)
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const int gi = i0 + dmma_row (wm, ti, lane), gc = c0 + dmma_col (wn, tj, c, lane);
+        if (gi < n0 && gc < ld) Y[(size_t) gi * ld + gc] = (gc < w) ? (T) acc[ti][tj][c] : T (0);
+      }
 }
+
+template <typename T>
+int
+launch_dense_apply (int n0, const double *Ainv, const T *B, T *Y, int w, int ld,
+                    cudaStream_t s)
+{
+  dim3 grid ((unsigned) ((n0 + GB - 1) / GB), (unsigned) ((ld + GB - 1) / GB));
+  k_dense_apply<T><<<grid, 128, 0, s>>> (n0, Ainv, B, Y, w, ld);
+  LGH_LAUNCH_CHECK ();
+  return 0;
+}
+
+template int launch_dense_apply<double> (int, const double *, const double *,
+                                         double *, int, int, cudaStream_t);
+template int launch_dense_apply<float> (int, const double *, const float *,
+                                        float *, int, int, cudaStream_t);
 
 template <typename T>
 int
@@ -240,7 +362,7 @@ launch_gemm_nn (int64_t n, int k, int m2, double alpha, const T *X, int ldx,
 {
   if (n == 0 || m2 == 0) return 0;
   dim3 grid ((unsigned) ((n + GB - 1) / GB), (unsigned) ((m2 + GB - 1) / GB));
-  k_gemm_nn<T><<<grid, 256, 0, s>>> (n, k, m2, alpha, X, ldx, M, ldm, beta,
+  k_gemm_nn<T><<<grid, 128, 0, s>>> (n, k, m2, alpha, X, ldx, M, ldm, beta,
                                      Y0, ldy0, Y, ldy);
   LGH_LAUNCH_CHECK ();
   return 0;

@@ -228,6 +228,11 @@ int launch_gemm_nn (int64_t n, int k, int m2, double alpha, const T *X,
                     int ldx, const double *M, int ldm, double beta,
                     const T *Y0, int ldy0, T *Y, int ldy, cudaStream_t s);
 size_t gemm_tn_work_elems (int64_t n, int m1, int m2);
+/* Y = A^{-1} B for a dense n0 x n0 column-major A^{-1} and row-major B, Y
+ * (n0 x ld); columns w .. ld - 1 of Y are zeroed */
+template <typename T>
+int launch_dense_apply (int n0, const double *Ainv, const T *B, T *Y, int w,
+                        int ld, cudaStream_t s);
 
 /* small dense FP64 (k_small.cu), matrices column-major n x n, ld n */
 /* Cholesky (lower) with the reference's single jitter retry; info[0] = 0

@@ -323,47 +323,6 @@ sa_coarsen (const HCsr &A, double theta, double lmax, HCsr &P, int64_t &nc)
 
 /* ---- device kernels ------------------------------------------------------ */
 
-/* Y = A^{-1} B for the dense coarse level: A^{-1} n0 x n0 (symmetric),
- * B, Y n0 x w row-major (ld) */
-template <typename T>
-__global__ void __launch_bounds__ (256)
-k_dense_apply (int n0, const double *__restrict__ Ainv, const T *__restrict__ B,
-               T *__restrict__ Y, int w, int ld)
-{
-  __shared__ double As[32][33];
-  __shared__ double Bs[32][65];
-  const int i0 = blockIdx.x * 32, c0 = blockIdx.y * 64;
-  const int tx = threadIdx.x & 63, ty = threadIdx.x >> 6;  /* 64 x 4 */
-  double acc[8];
-#pragma unroll
-  for (int a = 0; a < 8; a++) acc[a] = 0.;
-  for (int k0 = 0; k0 < n0; k0 += 32) {
-    for (int e = threadIdx.x; e < 32 * 32; e += 256) {
-      const int r = e & 31, k = e >> 5;
-      const int gi = i0 + r, gk = k0 + k;
-      As[r][k] = (gi < n0 && gk < n0) ? Ainv[gi + (size_t) gk * n0] : 0.;
-    }
-    for (int e = threadIdx.x; e < 32 * 64; e += 256) {
-      const int k = e >> 6, c = e & 63;
-      const int gk = k0 + k, gc = c0 + c;
-      Bs[k][c] = (gk < n0 && gc < w) ? (double) B[(size_t) gk * ld + gc] : 0.;
-    }
-    __syncthreads ();
-#pragma unroll 4
-    for (int k = 0; k < 32; k++) {
-      const double b = Bs[k][tx];
-#pragma unroll
-      for (int a = 0; a < 8; a++) acc[a] = fma (As[ty + 4 * a][k], b, acc[a]);
-    }
-    __syncthreads ();
-  }
-#pragma unroll
-  for (int a = 0; a < 8; a++) {
-    const int gi = i0 + ty + 4 * a, gc = c0 + tx;
-    if (gi < n0 && gc < ld) Y[(size_t) gi * ld + gc] = (gc < w) ? (T) acc[a] : T (0);
-  }
-}
-
 /* ---- host <-> device ------------------------------------------------------ */
 
 /* upload a host CSR into a device Csr (float copy and 1/diag filled) */
@@ -627,11 +586,9 @@ vcycle_level (Hierarchy *h, MgWork *W, size_t l, const T *B, T *X, int ld,
   KTrace *tr = (l == 0) ? trace : nullptr;   /* the fine level only */
   const double blk = (double) n * ld * sizeof (T);
   if (l + 1 == h->lev.size ()) {
-    dim3 grid ((unsigned) ((h->n0 + 31) / 32), (unsigned) ((ld + 63) / 64));
     if (trace) LGH_TRY (trace->begin (K_MG_COARSE,
                                       (double) h->n0 * h->n0 * 8 + 2. * blk, s));
-    k_dense_apply<T><<<grid, 256, 0, s>>> (h->n0, h->Ainv.p, B, X, w, ld);
-    LGH_LAUNCH_CHECK ();
+    LGH_TRY (launch_dense_apply<T> (h->n0, h->Ainv.p, B, X, w, ld, s));
     if (trace) LGH_TRY (trace->end (s));
     return 0;
   }
