@@ -172,6 +172,9 @@ hcsr_gemm (const HCsr &A, const HCsr &B)
   return C;
 }
 
+static double lanczos_tail (const std::vector<double> &al,
+                            const std::vector<double> &be);
+
 /* lambda_max(D^{-1} A) from CG-Lanczos with Jacobi (its steps, fixed
  * hashed probe), the estimate of zsolve_impl.h:284-313; extremal
  * eigenvalue of the tridiagonal by Sturm bisection */
@@ -210,6 +213,14 @@ lanczos_lmax (const HCsr &A, int its, uint64_t seed)
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < n; i++) p[i] = z[i] + b * p[i];
   }
+  return lanczos_tail (al, be);
+}
+
+/* the largest eigenvalue of the Lanczos tridiagonal of a CG run with step
+ * lengths al (alpha) and be (beta): bisection on the Sturm count */
+static double
+lanczos_tail (const std::vector<double> &al, const std::vector<double> &be)
+{
   const int m = (int) al.size ();
   if (m == 0) return 2.0;
   std::vector<double> d (m), e (m, 0.);
@@ -323,6 +334,173 @@ sa_coarsen (const HCsr &A, double theta, double lmax, HCsr &P, int64_t &nc)
 
 /* ---- device kernels ------------------------------------------------------ */
 
+/* ---- lambda_max(D^{-1} A) on the device -----------------------------------
+ * The recurrence of lanczos_lmax on a level's device operator: the same
+ * hashed start vector, Jacobi-preconditioned CG steps whose lengths form
+ * the Lanczos tridiagonal.  Three launches per step; each reduction sums
+ * fixed per-block partials in block order in the last block to finish (the
+ * same bits on every run); the step lengths come back in one copy. */
+constexpr int LZ_MAX = 64;
+constexpr int LZ_BLOCK = 256;
+
+struct LzState
+{
+  double rz;
+  double alpha[LZ_MAX], beta[LZ_MAX];
+  int na, nb, stop, step_ok;
+  unsigned ticket;
+};
+
+/* this block's sum of v into part[blockIdx.x]; in the last block to
+ * finish, thread 0 gets the total over all blocks and returns true */
+__device__ bool
+lz_reduce (double v, double *part, unsigned *ticket, double *total)
+{
+  __shared__ double red[LZ_BLOCK / 32];
+  __shared__ bool last;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync (0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads ();
+  if (threadIdx.x == 0) {
+    double sum = 0.;
+    for (int w = 0; w < LZ_BLOCK / 32; w++) sum += red[w];
+    part[blockIdx.x] = sum;
+    __threadfence ();
+    last = atomicAdd (ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads ();
+  if (!last || threadIdx.x != 0) return false;
+  __threadfence ();
+  double sum = 0.;
+  for (unsigned b = 0; b < gridDim.x; b++) sum += ((volatile double *) part)[b];
+  *total = sum;
+  *ticket = 0u;
+  return true;
+}
+
+__global__ void __launch_bounds__ (LZ_BLOCK)
+k_lz_init (int64_t n, uint64_t seed, const double *dinv, double *r, double *z,
+           double *p, double *part, LzState *st)
+{
+  double acc = 0.;
+  for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t) gridDim.x * blockDim.x) {
+    const double ri = 0.5 - (double) ((rng_state_at (seed, i, 0) >> 11)
+                                      * (1.0 / 9007199254740992.0));
+    const double zi = dinv[i] * ri;
+    r[i] = ri;
+    z[i] = zi;
+    p[i] = zi;
+    acc += ri * zi;
+  }
+  double tot;
+  if (lz_reduce (acc, part, &st->ticket, &tot)) st->rz = tot;
+}
+
+/* q = A p, alpha = (r, z) / (p, q) */
+__global__ void __launch_bounds__ (LZ_BLOCK)
+k_lz_q (int64_t n, const int64_t *rp, const int32_t *ci, const double *v,
+        const double *p, double *q, double *part, LzState *st)
+{
+  if (st->stop) return;
+  double acc = 0.;
+  for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t) gridDim.x * blockDim.x) {
+    double sum = 0.;
+    for (int64_t k = rp[i]; k < rp[i + 1]; k++) sum += v[k] * p[ci[k]];
+    q[i] = sum;
+    acc += p[i] * sum;
+  }
+  double pq;
+  if (lz_reduce (acc, part, &st->ticket, &pq)) {
+    if (!(pq > 0.) || st->na >= LZ_MAX) {
+      st->stop = 1;
+      st->step_ok = 0;
+    } else {
+      st->alpha[st->na++] = st->rz / pq;
+      st->step_ok = 1;
+    }
+  }
+}
+
+/* r -= alpha q, z = D^{-1} r, beta = (r, z)_new / (r, z)_old */
+__global__ void __launch_bounds__ (LZ_BLOCK)
+k_lz_r (int64_t n, const double *dinv, double *r, double *z, const double *q,
+        double *part, LzState *st)
+{
+  if (!st->step_ok) return;
+  const double a = st->alpha[st->na - 1];
+  double acc = 0.;
+  for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t) gridDim.x * blockDim.x) {
+    const double ri = r[i] - a * q[i];
+    const double zi = dinv[i] * ri;
+    r[i] = ri;
+    z[i] = zi;
+    acc += ri * zi;
+  }
+  double rz;
+  if (lz_reduce (acc, part, &st->ticket, &rz)) {
+    const double rzold = st->rz;
+    st->rz = rz;
+    if (rz <= 1e-300) {
+      st->stop = 1;
+      st->step_ok = 0;
+    } else {
+      st->beta[st->nb++] = rz / rzold;
+    }
+  }
+}
+
+/* p = z + beta p */
+__global__ void __launch_bounds__ (LZ_BLOCK)
+k_lz_p (int64_t n, const double *z, double *p, const LzState *st)
+{
+  if (!st->step_ok) return;
+  const double b = st->beta[st->nb - 1];
+  for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t) gridDim.x * blockDim.x)
+    p[i] = z[i] + b * p[i];
+}
+
+static int
+lanczos_lmax_dev (const Csr &A, int its, uint64_t seed, double *lmax)
+{
+  const int64_t n = A.n;
+  cudaStream_t s = stream ();
+  const int grid = (int) std::max<int64_t> (1, std::min<int64_t> (
+      (int64_t) num_sms () * 4, (n + LZ_BLOCK - 1) / LZ_BLOCK));
+  its = std::min (its, LZ_MAX);
+  DBuf<double> r, z, p, q, part;
+  DBuf<char> stb;
+  LGH_TRY (r.alloc (n));
+  LGH_TRY (z.alloc (n));
+  LGH_TRY (p.alloc (n));
+  LGH_TRY (q.alloc (n));
+  LGH_TRY (part.alloc (grid));
+  LGH_TRY (stb.alloc (sizeof (LzState)));
+  LzState *st = (LzState *) stb.p;
+  LGH_CUDA (cudaMemsetAsync (st, 0, sizeof (LzState), s));
+  k_lz_init<<<grid, LZ_BLOCK, 0, s>>> (n, seed, A.dinv, r.p, z.p, p.p, part.p, st);
+  LGH_LAUNCH_CHECK ();
+  for (int k = 0; k < its; k++) {
+    k_lz_q<<<grid, LZ_BLOCK, 0, s>>> (n, A.rowptr, A.colidx, A.vals, p.p, q.p,
+                                      part.p, st);
+    k_lz_r<<<grid, LZ_BLOCK, 0, s>>> (n, A.dinv, r.p, z.p, q.p, part.p, st);
+    k_lz_p<<<grid, LZ_BLOCK, 0, s>>> (n, z.p, p.p, st);
+  }
+  LGH_LAUNCH_CHECK ();
+  LzState h;
+  LGH_CUDA (cudaMemcpyAsync (&h, st, sizeof (LzState), cudaMemcpyDeviceToHost, s));
+  LGH_CUDA (cudaStreamSynchronize (s));
+  std::vector<double> al (h.alpha, h.alpha + h.na), be (h.beta, h.beta + h.nb);
+  *lmax = lanczos_tail (al, be);
+  return 0;
+}
+
+/* levels of at least this many rows estimate on the device */
+constexpr int64_t LZ_DEVICE_MIN = 20000;
+
 /* ---- host <-> device ------------------------------------------------------ */
 
 /* upload a host CSR into a device Csr (float copy and 1/diag filled) */
@@ -401,13 +579,6 @@ mg_build (const Csr &Z, int tile, double smoother_top, int nu, Hierarchy **out)
     MgLevel lv;
     lv.n = A.n;
     lv.nu = nu > 0 ? nu : 2;
-    lv.smax = lanczos_lmax (A, 40, 20260813ULL + (uint64_t) l);
-    /* the prolongator damping used the seed of level 0 on every level;
-     * keep that estimate (identical on level 0, one Lanczos run fewer) */
-    const double lmax_own = (l == 0) ? lv.smax : lanczos_lmax (A, 40, 20260813ULL);
-    lv.slo = 0.1 * lv.smax;
-    lv.shi = smoother_top * lv.smax;
-    lap (1);
     if (l == 0) {
       lv.A = Z;
       lv.own = 0;
@@ -416,6 +587,21 @@ mg_build (const Csr &Z, int tile, double smoother_top, int nu, Hierarchy **out)
       if (rc) { delete h; return rc; }
     }
     lap (4);
+    /* the prolongator damping used the seed of level 0 on every level;
+     * keep that estimate (identical on level 0, one Lanczos run fewer) */
+    double lmax_own = 0.;
+    if (A.n >= LZ_DEVICE_MIN) {
+      rc = lanczos_lmax_dev (lv.A, 40, 20260813ULL + (uint64_t) l, &lv.smax);
+      if (!rc && l > 0) rc = lanczos_lmax_dev (lv.A, 40, 20260813ULL, &lmax_own);
+      if (rc) { delete h; return rc; }
+    } else {
+      lv.smax = lanczos_lmax (A, 40, 20260813ULL + (uint64_t) l);
+      if (l > 0) lmax_own = lanczos_lmax (A, 40, 20260813ULL);
+    }
+    if (l == 0) lmax_own = lv.smax;
+    lv.slo = 0.1 * lv.smax;
+    lv.shi = smoother_top * lv.smax;
+    lap (1);
     if (A.n <= coarse_max || l == 11) {
       /* coarsest: dense inverse on the device, A^{-1} = L^{-T} L^{-1} */
       const int n0 = (int) A.n;
