@@ -116,59 +116,88 @@ hcsr_transpose (const HCsr &A)
 
 /* C = A B (Gustavson, dense accumulator), columns sorted per row; row
  * chunks in parallel, each with its own accumulator, then concatenated */
+/* rows of a product assembled chunk by chunk: each chunk's rows go into
+ * vectors of its own (moved out once, so threads never write shared
+ * headers), then the chunks are concatenated in parallel at their
+ * offsets; the result does not depend on the thread count */
+struct HChunk
+{
+  std::vector<int32_t> ci;
+  std::vector<double> v;
+  std::vector<int64_t> cnt;
+};
+
+static void
+hcsr_concat (std::vector<HChunk> &ch, int64_t n, HCsr &C)
+{
+  const int nch = (int) ch.size ();
+  std::vector<int64_t> off (nch + 1, 0), roff (nch + 1, 0);
+  for (int c = 0; c < nch; c++) {
+    off[c + 1] = off[c] + (int64_t) ch[c].ci.size ();
+    roff[c + 1] = roff[c] + (int64_t) ch[c].cnt.size ();
+  }
+  C.rp.assign (n + 1, 0);
+  C.ci.resize (off[nch]);
+  C.v.resize (off[nch]);
+#pragma omp parallel for schedule(static)
+  for (int c = 0; c < nch; c++) {
+    if (!ch[c].ci.empty ()) {
+      memcpy (C.ci.data () + off[c], ch[c].ci.data (), ch[c].ci.size () * sizeof (int32_t));
+      memcpy (C.v.data () + off[c], ch[c].v.data (), ch[c].v.size () * sizeof (double));
+    }
+    int64_t pos = off[c];
+    for (size_t r = 0; r < ch[c].cnt.size (); r++) {
+      pos += ch[c].cnt[r];
+      C.rp[roff[c] + (int64_t) r + 1] = pos;
+    }
+  }
+}
+
 static HCsr
 hcsr_gemm (const HCsr &A, const HCsr &B)
 {
   HCsr C;
   C.n = A.n;
   C.m = B.m;
-  C.rp.assign (C.n + 1, 0);
   const int nt = std::max (1, std::min (omp_get_max_threads (), 64));
   const int nchunk = (int) std::min<int64_t> (std::max<int64_t> (A.n, 1), 4 * nt);
-  std::vector<std::vector<int32_t>> cci (nchunk);
-  std::vector<std::vector<double>> cv (nchunk);
-  std::vector<std::vector<int64_t>> crn (nchunk);
+  std::vector<HChunk> ch (nchunk);
 #pragma omp parallel num_threads(nt)
   {
     std::vector<double> acc (B.m, 0.);
     std::vector<int64_t> mark (B.m, -1);
     std::vector<int32_t> cols;
 #pragma omp for schedule(dynamic, 1)
-    for (int ch = 0; ch < nchunk; ch++) {
-      const int64_t r0 = A.n * ch / nchunk, r1 = A.n * (ch + 1) / nchunk;
+    for (int c = 0; c < nchunk; c++) {
+      const int64_t r0 = A.n * c / nchunk, r1 = A.n * (c + 1) / nchunk;
+      HChunk loc;
+      loc.cnt.reserve (r1 - r0);
       for (int64_t i = r0; i < r1; i++) {
         cols.clear ();
         for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++) {
           const int64_t j = A.ci[k];
           const double a = A.v[k];
           for (int64_t q = B.rp[j]; q < B.rp[j + 1]; q++) {
-            const int32_t c = B.ci[q];
-            if (mark[c] != i) {
-              mark[c] = i;
-              acc[c] = 0.;
-              cols.push_back (c);
+            const int32_t col = B.ci[q];
+            if (mark[col] != i) {
+              mark[col] = i;
+              acc[col] = 0.;
+              cols.push_back (col);
             }
-            acc[c] += a * B.v[q];
+            acc[col] += a * B.v[q];
           }
         }
         std::sort (cols.begin (), cols.end ());
-        for (int32_t c : cols) {
-          cci[ch].push_back (c);
-          cv[ch].push_back (acc[c]);
+        for (int32_t col : cols) {
+          loc.ci.push_back (col);
+          loc.v.push_back (acc[col]);
         }
-        crn[ch].push_back ((int64_t) cols.size ());
+        loc.cnt.push_back ((int64_t) cols.size ());
       }
+      ch[c] = std::move (loc);
     }
   }
-  int64_t i = 0;
-  for (int ch = 0; ch < nchunk; ch++) {
-    for (int64_t cnt : crn[ch]) {
-      C.rp[i + 1] = C.rp[i] + cnt;
-      i++;
-    }
-    C.ci.insert (C.ci.end (), cci[ch].begin (), cci[ch].end ());
-    C.v.insert (C.v.end (), cv[ch].begin (), cv[ch].end ());
-  }
+  hcsr_concat (ch, C.n, C);
   return C;
 }
 
@@ -255,6 +284,7 @@ sa_coarsen (const HCsr &A, double theta, double lmax, HCsr &P, int64_t &nc)
 {
   const int64_t n = A.n;
   std::vector<double> diag (n);
+#pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < n; i++) diag[i] = hcsr_diag (A, i);
   auto strong = [&] (int64_t i, int64_t k) {
     const int64_t j = A.ci[k];
@@ -276,6 +306,7 @@ sa_coarsen (const HCsr &A, double theta, double lmax, HCsr &P, int64_t &nc)
   }
   /* pass 2: attach to the strongest aggregated neighbour (pass-1 state) */
   std::vector<int64_t> agg1 = agg;
+#pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < n; i++) {
     if (agg1[i] >= 0) continue;
     double best = -1.;
@@ -295,40 +326,52 @@ sa_coarsen (const HCsr &A, double theta, double lmax, HCsr &P, int64_t &nc)
   for (int64_t i = 0; i < n; i++) p0[i] = 1. / sqrt (sz[agg[i]]);
   /* omega = 4/3 / lambda_max(D^{-1}A) (the level's own estimate) */
   const double omega = (4.0 / 3.0) / lmax;
-  /* P = (I - omega D^{-1} A) P0, row by row */
+  /* P = (I - omega D^{-1} A) P0, rows in parallel chunks */
   P.n = n;
   P.m = nc;
-  P.rp.assign (n + 1, 0);
-  P.ci.clear ();
-  P.v.clear ();
-  std::vector<double> acc;
-  std::vector<int64_t> cols;
-  for (int64_t i = 0; i < n; i++) {
-    cols.clear ();
-    acc.clear ();
-    auto add = [&] (int64_t c, double val) {
-      for (size_t t = 0; t < cols.size (); t++)
-        if (cols[t] == c) { acc[t] += val; return; }
-      cols.push_back (c);
-      acc.push_back (val);
-    };
-    add (agg[i], p0[i]);
-    const double sc = omega / diag[i];
-    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++) {
-      const int64_t j = A.ci[k];
-      add (agg[j], -sc * A.v[k] * p0[j]);
+  const int nt = std::max (1, std::min (omp_get_max_threads (), 64));
+  const int nchunk = (int) std::min<int64_t> (std::max<int64_t> (n, 1), 4 * nt);
+  std::vector<HChunk> ch (nchunk);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+  for (int c = 0; c < nchunk; c++) {
+    const int64_t r0 = n * c / nchunk, r1 = n * (c + 1) / nchunk;
+    HChunk loc;
+    loc.cnt.reserve (r1 - r0);
+    std::vector<int64_t> cols;
+    std::vector<double> acc;
+    for (int64_t i = r0; i < r1; i++) {
+      cols.clear ();
+      acc.clear ();
+      auto add = [&] (int64_t col, double val) {
+        for (size_t t = 0; t < cols.size (); t++)
+          if (cols[t] == col) { acc[t] += val; return; }
+        cols.push_back (col);
+        acc.push_back (val);
+      };
+      add (agg[i], p0[i]);
+      const double sc = omega / diag[i];
+      for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++) {
+        const int64_t j = A.ci[k];
+        add (agg[j], -sc * A.v[k] * p0[j]);
+      }
+      /* ascending columns (insertion sort: rows hold a few aggregates) */
+      for (size_t t = 1; t < cols.size (); t++)
+        for (size_t u = t; u > 0 && cols[u - 1] > cols[u]; u--) {
+          std::swap (cols[u - 1], cols[u]);
+          std::swap (acc[u - 1], acc[u]);
+        }
+      int64_t kept = 0;
+      for (size_t t = 0; t < cols.size (); t++) {
+        if (acc[t] == 0.) continue;
+        loc.ci.push_back ((int32_t) cols[t]);
+        loc.v.push_back (acc[t]);
+        kept++;
+      }
+      loc.cnt.push_back (kept);
     }
-    std::vector<size_t> ord (cols.size ());
-    for (size_t t = 0; t < ord.size (); t++) ord[t] = t;
-    std::sort (ord.begin (), ord.end (),
-               [&] (size_t a, size_t b) { return cols[a] < cols[b]; });
-    for (size_t t : ord) {
-      if (acc[t] == 0.) continue;
-      P.ci.push_back ((int32_t) cols[t]);
-      P.v.push_back (acc[t]);
-    }
-    P.rp[i + 1] = (int64_t) P.ci.size ();
+    ch[c] = std::move (loc);
   }
+  hcsr_concat (ch, n, P);
 }
 
 
