@@ -256,7 +256,9 @@ def run_ours(args):
     torch.cuda.set_device(local)
     if world > 1:
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=900))
+        # every rank runs the same replica work between collectives, so a
+        # rank that waits this long has lost its peers
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
     import lgh_b200 as L
     from lgh_b200 import problems as P
