@@ -178,7 +178,7 @@ struct Small
     LGH_TRY (C.alloc (nn));
     /* split-K workspace: enough for every (m1, m2) <= (maxw, maxw) shape */
     LGH_TRY (work.alloc (std::max (gemm_tn_work_elems (rows, maxw, maxw),
-                                   (size_t) (2 * num_sms () + 64) * 64 * 64)));
+                                   gemm_tn_work_max (maxw, maxw))));
     LGH_TRY (sel.alloc (8));
     LGH_TRY (lam.alloc (n));
     LGH_TRY (order.alloc (n));

@@ -154,7 +154,8 @@ k_gemm_tn_reduce (int m1, int m2, int nsplit, const double *__restrict__ work,
 static int
 tn_splits (int64_t n, int m1, int m2)
 {
-  /* about 4 resident 4-warp CTAs per SM over all tiles and slices */
+  /* about 4 resident 4-warp CTAs per SM over all tiles and slices (the
+   * bound of gemm_tn_work_max follows this rule) */
   const int tiles = ((m1 + GB - 1) / GB) * ((m2 + GB - 1) / GB);
   int want = (4 * num_sms () + tiles - 1) / tiles;
   int64_t maxs = (n + 255) / 256;
@@ -168,6 +169,16 @@ size_t
 gemm_tn_work_elems (int64_t n, int m1, int m2)
 {
   return (size_t) tn_splits (n, m1, m2) * m1 * m2;
+}
+
+/* a workspace bound for every shape m1 <= m1max, m2 <= m2max: with t tiles
+ * the split count is at most ceil(4 S / t), so splits x tiles <= 4 S + t,
+ * and each tile holds at most GB x GB partial sums */
+size_t
+gemm_tn_work_max (int m1max, int m2max)
+{
+  const size_t tmax = (size_t) ((m1max + GB - 1) / GB) * ((m2max + GB - 1) / GB);
+  return (4 * (size_t) num_sms () + tmax) * GB * GB;
 }
 
 template <typename T>

@@ -890,8 +890,9 @@ lgh_server_create (lgh_glr_t *glr, const lgh_server_opts_t *opts,
   if (!rc) rc = sv->fresh_d.alloc (sv->ld);
   if (!rc) rc = sv->H.alloc ((size_t) glr->n * sv->ld);
   if (!rc) rc = sv->coef.alloc ((size_t) kp * sv->cap);
+  /* the harvests' U^T products run at every width up to the slot count */
   if (!rc) rc = sv->gemmwork.alloc (std::max<size_t> (
-             gemm_tn_work_elems (glr->n, kp, sv->cap), 64));
+             gemm_tn_work_max (kp, sv->cap), 64));
   if (!rc) rc = sv->ldc.alloc (1);
   if (!rc) rc = sv->ldo.alloc (1);
   if (!rc) rc = sv->hv_d.alloc (sizeof (Harvest));

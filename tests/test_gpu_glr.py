@@ -124,6 +124,24 @@ def test_extend_equals_one_shot(spd, backend):
     assert np.max(np.abs(l1 - l2) / np.abs(l1)) < 1e-10
 
 
+def test_extend_to_400_on_40k_rows():
+    """Incremental extension 200 -> 400 on a 200^2 grid (40000 rows: enough
+    rows that the split-K products run at their full split count, so every
+    BCGS2 panel product needs its largest partial-sum workspace), against
+    the one-shot build at ell = 400."""
+    n, dim = 200, 2
+    mass = P.lumped_mass(n, dim)
+    Z = L.Mat(P.z_operator(n, dim, 25.0, mass))
+    B = L.Mat(P.b_operator(n, dim, 0.01, 0.03, mass,
+                           P.a_field(n, dim, "sincos")))
+    pr = L.Prior(Z=Z, mass=mass, opts=L.prior_opts(ksp_rtol=1e-12))
+    g1 = L.Glr(B, pr, L.glr_opts(ell=400, seed=0, trunc_rel=0.0, check=0))
+    g2 = L.Glr(B, pr, L.glr_opts(ell=200, seed=0, trunc_rel=0.0, check=0))
+    g2.extend(200)
+    l1, l2 = g1.eigs()[:100], g2.eigs()[:100]
+    assert np.max(np.abs(l1 - l2) / np.abs(l1)) < 1e-9
+
+
 @pytest.mark.parametrize("spd", [True, False])
 def test_parity_with_oracle_test_glr(spd):
     p, B, pr, keep = _setup(spd, "mat")
