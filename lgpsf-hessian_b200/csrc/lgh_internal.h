@@ -161,6 +161,11 @@ template <typename T>
 int launch_spmm (const Csr &A, const T *X, int ldx, T *Y, int ldy, int w,
                  cudaStream_t s);
 
+/* lanes per row (2^glog) and 16-byte packs per lane (ch) of the row-group
+ * kernels for a block of nvec packs; kmax > 0 (the operator's longest row)
+ * lets a narrow block use half the lanes with two packs each */
+void row_group_shape (int nvec, int &glog, int &ch, int kmax = 0);
+
 /* CTAs of kernel fn (threads per CTA, dynamic shared memory) that are
  * resident on the device at once (occupancy x SMs; cached per kernel).
  * Row-group kernels walk interleaved row tiles with a stride loop, so a

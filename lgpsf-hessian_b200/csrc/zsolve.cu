@@ -39,7 +39,6 @@
 namespace lgh
 {
 
-void row_group_shape (int nvec, int &glog, int &ch);
 int row_grid (int64_t n, int glog);
 
 constexpr int ZS_THREADS = 256;
@@ -960,7 +959,7 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
     const int ldt = round_ld (wt);
     const int nvec = ldt / W;
     int glog, ch;
-    row_group_shape (nvec, glog, ch);
+    row_group_shape (nvec, glog, ch, Z.max_row_nnz);
     const int grid = std::min (row_grid (n, glog), ws.nblocks);
     const int smem = zs_smem_bytes (glog, ldt);
     const int cap = ws.cap;
@@ -1255,7 +1254,7 @@ server_tick_pq (const Csr &Z, const T *Zb, const T *Pold, T *Pnew, T *Q, int ld,
   constexpr int W = Pack<T>::W;
   const int nvec = ld / W;
   int glog, ch;
-  row_group_shape (nvec, glog, ch);
+  row_group_shape (nvec, glog, ch, Z.max_row_nnz);
   const int grid = std::min (row_grid (Z.n, glog), ws.nblocks);
   const int smem = zs_pq_smem_bytes (glog, ld);
   ZK zk{ Z.n, Z.rowptr, Z.colidx };
@@ -1293,7 +1292,7 @@ server_tick_dots (const Csr &Z, const T *R, const T *Zb, int ld, int w,
   constexpr int W = Pack<T>::W;
   const int nvec = ld / W;
   int glog, ch;
-  row_group_shape (nvec, glog, ch);
+  row_group_shape (nvec, glog, ch, Z.max_row_nnz);
   const int grid = std::min (row_grid (Z.n, glog), ws.nblocks);
   const int smem = zs_smem_bytes (glog, ld);
   ZK zk{ Z.n, Z.rowptr, Z.colidx };
@@ -1356,7 +1355,7 @@ launch_cheb_step (const Csr &A, T *X, const T *Ro, T *Rn, const T *Do, T *Dn,
     if (nvec <= 0) continue;
     const int c0 = v0 * W;
     int glog, ch;
-    row_group_shape (nvec, glog, ch);
+    row_group_shape (nvec, glog, ch, A.max_row_nnz);
     const int grid = std::min (row_grid (A.n, glog), num_sms () * 8);
     ZS_DISPATCH (ch, {
       k_cheb<T, CH_><<<fit_grid (k_cheb<T, CH_>, grid, ZS_THREADS, 0),
@@ -1434,7 +1433,7 @@ zresid_launch (const Csr &Z, int64_t n, int w, const double *Bm, int ldb,
   const int ld = round_ld (w);
   const int nvec = ld / 2;
   int glog, ch;
-  row_group_shape (nvec, glog, ch);
+  row_group_shape (nvec, glog, ch, Z.max_row_nnz);
   const int grid = std::min (row_grid (n, glog), nblocks);
   const int smem = zs_smem_bytes (glog, ld);
   ZK zk{ Z.n, Z.rowptr, Z.colidx };
