@@ -19,11 +19,12 @@ same jobs end to end through the C ABI from pinned host buffers (e2e), the
 per-kernel roofline of the dominant kernel from the library's live event
 timing, per-RHS solve latency p50/p99, SM clocks sampled during the timed
 region, a Poisson request stream through the request loop (serving), and
-the CPU baseline (the oracle on the host cores, a bounded
-sample extrapolated to a job).
+the CPU baseline (one complete job of the oracle on all host cores).
 
 --impl reference: the reference's CPU path restated by the oracle
-(oracle/), all host threads, a bounded sample per step, same metric.
+(oracle/), all host threads, same workload and metric; the K timed steps
+together run complete jobs (each job cut into bounded pieces that are
+spread evenly over the steps), so the steps' measured time is whole jobs.
 """
 
 import argparse
@@ -57,8 +58,6 @@ def parse():
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-cols", type=int, default=0,
-                    help="sketch columns in the CPU sample (0 = host cores)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
@@ -69,6 +68,17 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--serve-rates", default="",
                     help="comma-separated request rates for --config c5")
+    ap.add_argument("--kernel-case", default="",
+                    choices=["", "zsolve", "spmm", "build"],
+                    help="run one device case and print the library's "
+                         "per-kernel event timing (for ncu captures of "
+                         "single kernels): zsolve = a blocked Z-solve of a "
+                         "seeded N x width block, spmm = B times it, build "
+                         "= one GLR build at ell = width")
+    ap.add_argument("--kc-config", default="c2")
+    ap.add_argument("--kc-width", type=int, default=220)
+    ap.add_argument("--kc-rtol", type=float, default=1e-10)
+    ap.add_argument("--kc-fp32", action="store_true")
     ap.add_argument("--config", default="c2", choices=["c2", "c3", "c4", "c5"],
                     help="c2: the headline job (default); c3 / c4: the "
                          "mixed-precision 3D extend and the batched-shift "
@@ -104,79 +114,133 @@ def workload(cfg):
 
 
 # --------------------------------------------------------------------------
-# CPU side: the oracle timed on the host cores (bounded sample)
+# CPU side: the oracle (the reference's replicated CPU path restated) on the
+# host cores
 
 
-def cpu_sample(cfg, cols=0):
-    """Time the oracle (the reference's replicated CPU path restated) on a
-    bounded sample of the job and extrapolate: one F-apply over `cols`
-    sketch columns (columns run in parallel over the host threads), the
-    dense part (two CholQR2 at the full N x ell, the ell x ell eigensolve)
-    and one single-RHS solve (2 Z-solves); job = F-applies over
-    (q+2)*ell + rank columns + 2 CholQR2 + 16 solves (over the threads)."""
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_job(cfg, oracle, nthreads, rhs):
+    """One complete C2 job on the oracle, as a sequence of bounded pieces
+    (a generator: each next() runs one piece).  The same job as the e2e
+    arm: the prior with its multigrid set-up, the build (ell 220, rank cap
+    200, q 1, check on; F-applies in waves of `nthreads` columns, one
+    column per thread), the 16-RHS solve at c = 1 (column-parallel), the
+    logdet.  Yields the logdet last."""
+    B, Z = cfg["_orc_B"], cfg["_orc_Z"]
+    pr = oracle.Prior(Z, cfg["mass"], ksp_rtol=ZRTOL, pc="amg")
+    yield None
+    o = oracle.opts_default(ell=ELL, q_power=QPOW, seed=SEED, trunc_rel=0.0,
+                            check=1)
+    b = oracle.Build(B, pr, o, cap=RANK, wave=nthreads)
+    while b.step():
+        yield None
+    yield None
+    g = b.finish()
+    g.solve_block(SHIFT, rhs)
+    yield g.logdet(SHIFT)
+
+
+def reference_pieces(nthreads):
+    """Pieces of one reference_job: prior, build, solve + logdet."""
+    import oracle
+    return 1 + oracle.build_pieces(ELL, QPOW, RANK, nthreads) + 1
+
+
+def oracle_setup(cfg):
     import oracle
     nthreads = os.cpu_count() or 1
     oracle.set_threads(nthreads)
-    cols = cols or nthreads
-    B = oracle.Csr(cfg["B"]["rowptr"], cfg["B"]["colidx"], cfg["B"]["vals"])
-    Z = oracle.Csr(cfg["Z"]["rowptr"], cfg["Z"]["colidx"], cfg["Z"]["vals"])
-    pr = oracle.Prior(Z, cfg["mass"], ksp_rtol=ZRTOL, pc="amg")
-    ctx = oracle.lib().orc_glr_context(B.h, pr.h)
-    N = cfg["N"]
-    X = oracle.sketch(SEED, N, 0, cols)
-    Xc = np.ascontiguousarray(X.T)
-    Yc = np.empty_like(Xc)
+    if "_orc_B" not in cfg:
+        cfg["_orc_B"] = oracle.Csr(cfg["B"]["rowptr"], cfg["B"]["colidx"],
+                                   cfg["B"]["vals"])
+        cfg["_orc_Z"] = oracle.Csr(cfg["Z"]["rowptr"], cfg["Z"]["colidx"],
+                                   cfg["Z"]["vals"])
+    rhs = np.asfortranarray(
+        np.random.default_rng(7).standard_normal((cfg["N"], NRHS)))
+    return oracle, nthreads, rhs
+
+
+def _sample_note(nthreads):
+    return ("oracle (the reference's replicated CPU path restated in C++, "
+            "OpenBLAS), %d threads on %s: complete C2 jobs, each the prior "
+            "with its smoothed-aggregation set-up, the build (F-applies of "
+            "one column per thread, per-column CG rtol %g with the V-cycle "
+            "PC in the role of the reference's CG + PCGAMG), the 16-RHS "
+            "solve and the logdet" % (nthreads, cpu_model(), ZRTOL))
+
+
+def cpu_baseline(cfg):
+    """One complete job on the oracle, timed end to end (no sample, no
+    extrapolation)."""
+    oracle, nthreads, rhs = oracle_setup(cfg)
     t0 = time.perf_counter()
-    oracle.lib().orc_glr_apply_F(ctx, cols, Xc.ctypes.data_as(oracle.c_dbl_p),
-                                 Yc.ctypes.data_as(oracle.c_dbl_p))
-    t_f = time.perf_counter() - t0
-    Q = np.asfortranarray(np.random.default_rng(0).standard_normal((N, ELL)))
-    t0 = time.perf_counter()
-    oracle.lib().orc_cholqr2(N, ELL, Q.ctypes.data_as(oracle.c_dbl_p))
-    t_orth = time.perf_counter() - t0
-    T = np.random.default_rng(1).standard_normal((ELL, ELL))
-    t0 = time.perf_counter()
-    oracle.dsyevd(T + T.T, vecs=True)
-    t_eig = time.perf_counter() - t0
-    oracle.lib().orc_glr_destroy(ctx)
-    # one solve = 2 single-column Z-solves ~ the F-apply's per-column
-    # Z-solve cost; columns of the F-apply ran in parallel
-    waves_f = ((QPOW + 2) * ELL + RANK + cols - 1) // cols
-    t_solve_col = t_f / 2.0             # one wave = 2 Z-solves + 1 SpMV
-    waves_s = (NRHS + nthreads - 1) // nthreads
-    job = waves_f * t_f + 2 * (QPOW + 1) * t_orth + t_eig \
-        + waves_s * 2 * t_solve_col
-    sample = ("oracle F-apply of %d sketch columns (%d threads, CG rtol "
-              "%g with a smoothed-aggregation V-cycle PC, the reference's "
-              "CG + PCGAMG: %.1f s), CholQR2 at %dx%d (%.2f s), dsyevd %d "
-              "(%.3f s); job extrapolated as %d F waves + %d CholQR2 + eig + "
-              "%d solve waves = %.1f s"
-              % (cols, nthreads, ZRTOL, t_f, N, ELL, t_orth, ELL, t_eig,
-                 waves_f, 2 * (QPOW + 1), waves_s, job))
+    for _ in reference_job(cfg, oracle, nthreads, rhs):
+        pass
+    job = time.perf_counter() - t0
     return dict(value=1.0 / job, unit=UNIT, cores=nthreads, kind="port",
-                sample=sample, job_s=job)
+                cpu_model=cpu_model(),
+                sample=_sample_note(nthreads) + "; one job, %.1f s" % job)
 
 
 def run_reference(args):
+    """The reference arm: the oracle on all host threads, on the same
+    workload.  The K timed steps run exactly J complete jobs, J = ceil(K /
+    P) with P the pieces of one job, the pieces split evenly over the
+    steps, so ms_per_step x K is the measured time of J whole jobs.  The
+    W warm-up steps run the same share of pieces of a separate job that is
+    then dropped."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     from lgh_b200 import problems as P
     cfg = P.grid_problem(CONFIG)
-    vals = []
-    info = None
-    for i in range(args.warmup + args.steps):
-        info = cpu_sample(cfg, args.cpu_cols)
-        if i >= args.warmup:
-            vals.append(info["value"])
-    v = statistics.mean(vals)
+    oracle, nthreads, rhs = oracle_setup(cfg)
+    npc = reference_pieces(nthreads)
+    K, W = args.steps, args.warmup
+    J = -(-K // npc)
+    bounds = [(k * J * npc) // K for k in range(K + 1)]
+
+    def run_steps(nsteps, njobs, times):
+        jobs = (reference_job(cfg, oracle, nthreads, rhs)
+                for _ in range(njobs))
+        it = (x for job in jobs for x in job)
+        for k in range(nsteps):
+            t0 = time.perf_counter()
+            for _ in range(bounds[k + 1] - bounds[k]):
+                next(it, None)
+            if k == nsteps - 1 and times is not None:
+                for _ in it:             # the last step drains what is left
+                    pass
+            if times is not None:
+                times.append(time.perf_counter() - t0)
+
+    run_steps(min(W, K), 1, None)        # warm-up share of a dropped job
+    times = []
+    run_steps(K, J, times)
+    total = sum(times)
+    v = J / total
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 / v, "higher_is_better": True,
+            "n_gpus": args.gpus, "steps": K, "warmup": W,
+            "ms_per_step": 1e3 * total / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (config formulas)", "config": workload(cfg),
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": info["cores"],
-                             "kind": "port", "sample": info["sample"]},
+            "jobs_timed": J, "pieces_per_job": npc,
+            "step_note": "the %d timed steps run %d complete job(s), %d "
+                         "pieces each, split evenly over the steps"
+                         % (K, J, npc),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads,
+                             "kind": "port", "cpu_model": cpu_model(),
+                             "sample": _sample_note(nthreads)},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -303,7 +367,6 @@ def run_ours(args):
     torch.cuda.synchronize()
     clocks = Clocks(local)
     clocks.start()
-    L.kernel_timing(True)
     launches0 = Lb.lgh_launch_count()
     rt0 = L.runtime_counters()
     t_start, t_end = torch.cuda.Event(enable_timing=True), \
@@ -318,8 +381,6 @@ def run_ours(args):
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
-    ktimes = L.kernel_timing_get()
-    L.kernel_timing(False)
     launches = Lb.lgh_launch_count() - launches0
     rt1 = L.runtime_counters()
     runtime = {k: (rt1[k] - rt0[k]) / args.steps
@@ -330,6 +391,17 @@ def run_ours(args):
     build_s = [ev[0].elapsed_time(ev[1]) / 1e3 for ev, _ in timers]
     solve_s = [ev[1].elapsed_time(ev[2]) / 1e3 for ev, _ in timers]
     g_last = timers[-1][1]
+    del timers[:-1]
+
+    # per-kernel roofline: a separate, untimed pass of the same job with
+    # the library's per-launch CUDA-event registry on (the registry adds an
+    # event pair around every hot launch, so it stays off in the timed loop)
+    L.kernel_timing(True)
+    for _ in range(min(2, args.steps)):
+        job()
+    torch.cuda.synchronize()
+    ktimes = L.kernel_timing_get()
+    L.kernel_timing(False)
     stats = g_last.stats()
     report = g_last.report
 
@@ -406,7 +478,8 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (config formulas)",
-            "config": dict(workload(cfg), parallelism="replicas%d" % world),
+            "config": workload(cfg),
+            "replicas": world,
             "build_s": statistics.mean(build_s),
             "solves_per_s": NRHS / statistics.mean(solve_s),
             "solve_p50_ms": lat[len(lat) // 2],
@@ -436,8 +509,7 @@ def run_ours(args):
     if not args.no_e2e:
         line["e2e"] = run_e2e(args, cfg, L, torch, world, dist)
     if rank == 0 and world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = {k: v for k, v in cpu_sample(
-            cfg, args.cpu_cols).items() if k != "job_s"}
+        line["cpu_baseline"] = cpu_baseline(cfg)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -835,8 +907,49 @@ def run_c5(args):
     return 0
 
 
+def run_kernel_case(args):
+    """One device case through the C ABI with the per-kernel event
+    registry on; prints the wall time and each kernel's launches, time and
+    achieved bandwidth (algorithmic bytes / event time)."""
+    import lgh_b200 as L
+    from lgh_b200 import problems as P
+    L.load()
+    cfg = P.grid_problem(args.kc_config)
+    N, w = cfg["N"], args.kc_width
+    L.kernel_timing(True)
+    t0 = time.time()
+    if args.kernel_case == "zsolve":
+        Z = L.Mat(cfg["Z"])
+        pr = L.Prior(Z=Z, mass=cfg["mass"],
+                     opts=L.prior_opts(ksp_rtol=args.kc_rtol))
+        X = np.random.default_rng(0).standard_normal((N, w))
+        L.test_zsolve(pr, X, fp32=args.kc_fp32)
+        info = pr.info()
+    elif args.kernel_case == "spmm":
+        B = L.Mat(cfg["B"])
+        X = np.random.default_rng(0).standard_normal((N, w))
+        L.test_spmm(B, X, fp32=args.kc_fp32)
+        info = {}
+    else:
+        B, Z = L.Mat(cfg["B"]), L.Mat(cfg["Z"])
+        pr = L.Prior(Z=Z, mass=cfg["mass"],
+                     opts=L.prior_opts(ksp_rtol=args.kc_rtol))
+        g = L.Glr(B, pr, L.glr_opts(ell=w, seed=0, trunc_rel=0.0))
+        info = g.stats()
+    dt = time.time() - t0
+    print("case %s %s w=%d: %.3f s  %s" % (args.kernel_case, args.kc_config,
+                                           w, dt, info))
+    for k, (ms, n, by) in L.kernel_timing_get().items():
+        if n:
+            print("  %-24s launches %7d  %9.3f ms  %8.3f ms/launch  %7.1f "
+                  "GB/s" % (k, n, ms, ms / n, by / n / (ms / n / 1e3) / 1e9))
+    return 0
+
+
 def main():
     args = parse()
+    if args.kernel_case:
+        return run_kernel_case(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -404,11 +404,12 @@ void lgh_server_destroy (lgh_server_t *server);
  * reference: for callers that fix the device memory budget up front and
  * forbid a library to allocate.  Its split-K partial sums live in one
  * fixed 8 MiB device array inside the library, so w <= 1024 (w * w <=
- * 2^20 doubles; larger w returns LGH_ERR_ARG_OUTOFRANGE).  Make the first
- * call on each device before any stream capture begins (it looks the
- * array's address up once per device).  Calls share that array: calls from
- * different host threads race on it and must be serialised.  The call
- * synchronises before returning.                                          */
+ * 2^20 doubles; larger w returns LGH_ERR_ARG_OUTOFRANGE).  Every call
+ * looks the array's device address up on the current device.  The call runs
+ * on the legacy default stream and synchronises it before returning, so it
+ * cannot run while any stream capture is active in the process.  Calls
+ * share the array: calls from different host threads race on it and must
+ * be serialised.                                                          */
 int lgh_gram_noalloc (int64_t n, int w, const double *X, int64_t ldx,
                       double *G, int64_t ldg);
 

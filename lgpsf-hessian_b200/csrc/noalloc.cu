@@ -13,17 +13,17 @@
  * library holds it until the process exits.  Widths with w * w above that
  * size (w > 1024) are rejected with LGH_ERR_ARG_OUTOFRANGE.
  *
- * Set-up: the first call on each device (with that device current) looks
- * the array's device address up with cudaGetSymbolAddress, which may load
- * the module; that first call should be made before any stream capture
- * begins.  The call synchronises its stream before returning.  Calls
+ * Set-up: every call looks the array's device address up with
+ * cudaGetSymbolAddress on the current device (the first lookup on a device
+ * may load the module), so the address stays right across a device reset
+ * or a recreated primary context.  The call runs on the library's stream
+ * (the legacy default stream) and synchronises it before returning, so it
+ * cannot run while any stream capture is active in the process.  Calls
  * share the one array: two calls whose work overlaps on the GPU (calls
  * from different host threads) race on it and must be serialised by the
  * caller.  Each call overwrites every partial it reads, so nothing has to
  * start at zero and the array keeps the last call's partials.
  */
-
-#include <mutex>
 
 #include "lgh_internal.h"
 
@@ -41,12 +41,6 @@ int gemm_tn_splits (int64_t n, int m1, int m2);
  * name as a pointer: it stands for the symbol, not a device address) */
 static __device__ __align__ (256) double g_gram_scratch[LGH_NOALLOC_SCRATCH_DOUBLES];
 
-namespace
-{
-std::mutex g_mu;
-double *g_addr[128];
-}
-
 extern "C" int
 lgh_gram_noalloc (int64_t n, int w, const double *X, int64_t ldx, double *G,
                   int64_t ldg)
@@ -61,22 +55,12 @@ lgh_gram_noalloc (int64_t n, int w, const double *X, int64_t ldx, double *G,
              "be <= %ld, i.e. w <= 1024)", w, (long) LGH_NOALLOC_SCRATCH_DOUBLES);
   LGH_CHECK (ldx <= INT32_MAX && ldg <= INT32_MAX, LGH_ERR_ARG_OUTOFRANGE,
              "lgh_gram_noalloc: leading dimension too large");
-  int dev = 0;
-  LGH_CUDA (cudaGetDevice (&dev));
-  LGH_CHECK (dev >= 0 && dev < 128, LGH_ERR_SUP, "lgh_gram_noalloc: device %d", dev);
-  double *scratch;
-  {
-    std::lock_guard<std::mutex> lk (g_mu);
-    if (g_addr[dev] == nullptr) {
-      void *p = nullptr;
-      cudaError_t e = cudaGetSymbolAddress (&p, g_gram_scratch);
-      if (e != cudaSuccess || p == nullptr)
-        return set_error (LGH_ERR_GPU, "lgh_gram_noalloc: cudaGetSymbolAddress: %s",
-                          cudaGetErrorString (e));
-      g_addr[dev] = (double *) p;
-    }
-    scratch = g_addr[dev];
-  }
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress (&p, g_gram_scratch);
+  if (e != cudaSuccess || p == nullptr)
+    return set_error (LGH_ERR_GPU, "lgh_gram_noalloc: cudaGetSymbolAddress: %s",
+                      cudaGetErrorString (e));
+  double *scratch = (double *) p;
   int nsplit = gemm_tn_splits (n, w, w);
   const long fit = LGH_NOALLOC_SCRATCH_DOUBLES / ((long) w * w);
   if (nsplit > fit) nsplit = (int) fit;

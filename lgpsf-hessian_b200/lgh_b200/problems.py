@@ -191,6 +191,11 @@ CONFIGS = {
                ell=200, ell_ext=400),
     "c5": dict(n=128, dim=3, shift=16.0, lb=0.01, rho=0.02, a="sin3",
                ell=520, rank=500),
+    # config 3's operator formulas on a 32^3 grid, with the B length and
+    # radius scaled by 96/32 so that the kernel spans the same number of
+    # grid points as at 96^3 (a parity case the oracle finishes in seconds)
+    "c3_32": dict(n=32, dim=3, shift=16.0, lb=0.036, rho=0.075, a="sin3",
+                  ell=40, ell_ext=80),
 }
 
 

@@ -140,6 +140,21 @@ def lib():
     L.orc_glr_context.argtypes = [P, P]
     L.orc_cholqr2.restype = ctypes.c_int
     L.orc_cholqr2.argtypes = [I64, ctypes.c_int, c_dbl_p]
+    L.orc_glr_compute_cap.restype = ctypes.c_int
+    L.orc_glr_compute_cap.argtypes = [P, P, ctypes.POINTER(GlrOpts),
+                                      ctypes.c_int, ctypes.c_int,
+                                      ctypes.POINTER(P),
+                                      ctypes.POINTER(GlrReport)]
+    L.orc_build_begin.restype = P
+    L.orc_build_begin.argtypes = [P, P, ctypes.POINTER(GlrOpts), ctypes.c_int,
+                                  ctypes.c_int, ctypes.c_int]
+    L.orc_build_step.restype = ctypes.c_int
+    L.orc_build_step.argtypes = [P]
+    L.orc_build_finish.restype = P
+    L.orc_build_finish.argtypes = [P, ctypes.POINTER(GlrReport)]
+    L.orc_glr_solve_block.restype = ctypes.c_int
+    L.orc_glr_solve_block.argtypes = [P, ctypes.c_double, ctypes.c_int,
+                                      c_dbl_p, c_dbl_p]
     _LIB = L
     return L
 
@@ -165,8 +180,9 @@ def ref_pure():
     return L
 
 
-def set_threads(n):
-    lib().orc_set_threads(int(n))
+def set_threads(n=0):
+    """OpenMP and OpenBLAS threads of the oracle (0: every host core)."""
+    lib().orc_set_threads(int(n) if n and n > 0 else (os.cpu_count() or 1))
 
 
 def randn_at(seed, i, j):
@@ -262,19 +278,25 @@ class Prior:
 class Glr:
     """Oracle GLR object (lgh_glr_compute and the downstream operations)."""
 
-    def __init__(self, B, prior, opts=None, incremental=True):
+    def __init__(self, B, prior, opts=None, incremental=True, cap=0,
+                 _handle=None, _report=None):
         self.B = B
         self.prior = prior
         self.opts = opts if opts is not None else opts_default()
+        self.n = B.n
+        if _handle is not None:          # handed over by Build.finish
+            self.h = _handle
+            self.report = _report
+            return
         self.h = ctypes.c_void_p()
         rep = GlrReport()
-        rc = lib().orc_glr_compute(B.h, prior.h, ctypes.byref(self.opts),
-                                   1 if incremental else 0,
-                                   ctypes.byref(self.h), ctypes.byref(rep))
+        rc = lib().orc_glr_compute_cap(B.h, prior.h, ctypes.byref(self.opts),
+                                       1 if incremental else 0, int(cap),
+                                       ctypes.byref(self.h),
+                                       ctypes.byref(rep))
         if rc != 0:
             raise RuntimeError("orc_glr_compute failed: %d" % rc)
         self.report = rep.as_dict()
-        self.n = B.n
 
     def extend(self, k):
         rep = GlrReport()
@@ -307,6 +329,16 @@ class Glr:
 
     def solve(self, c, rhs):
         return self._vv(lib().orc_glr_solve, c, rhs)
+
+    def solve_block(self, c, R):
+        """lgh_glr_solve on the columns of R (n x m), column-parallel."""
+        Rf = np.asfortranarray(R, dtype=np.float64)
+        X = np.empty_like(Rf)
+        rc = lib().orc_glr_solve_block(self.h, c, Rf.shape[1], _dp(Rf),
+                                       _dp(X))
+        if rc != 0:
+            raise RuntimeError("oracle solve_block failed: %d" % rc)
+        return X
 
     def sample(self, c, xi):
         return self._vv(lib().orc_glr_sample, c, xi)
@@ -344,6 +376,57 @@ class Glr:
         if getattr(self, "h", None) and _LIB is not None and self.h.value:
             _LIB.orc_glr_destroy(self.h)
             self.h = ctypes.c_void_p()
+
+
+class Build:
+    """The oracle's replicated build advanced one bounded piece at a time
+    (one sketch, one wave of `wave` F-apply columns, one CholQR2, the
+    Rayleigh-Ritz step, one wave of the residual check).  Stepping to the
+    end gives the same object, bit for bit, as Glr(...) on the same
+    arguments."""
+
+    def __init__(self, B, prior, opts, cap=0, wave=0, incremental=True):
+        self.B, self.prior, self.opts = B, prior, opts
+        self.h = lib().orc_build_begin(B.h, prior.h, ctypes.byref(opts),
+                                       1 if incremental else 0, int(cap),
+                                       int(wave))
+        if not self.h:
+            raise RuntimeError("orc_build_begin: bad ell")
+        self.done = False
+
+    def step(self):
+        """Run one piece; True while pieces remain."""
+        st = lib().orc_build_step(self.h)
+        if st < 0:
+            raise RuntimeError("oracle build step failed: %d" % -st)
+        self.done = st == 0
+        return not self.done
+
+    def finish(self):
+        rep = GlrReport()
+        h = lib().orc_build_finish(self.h, ctypes.byref(rep))
+        self.h = None
+        if not h:
+            raise RuntimeError("oracle build not finished")
+        return Glr(self.B, self.prior, self.opts, _handle=ctypes.c_void_p(h),
+                   _report=rep.as_dict())
+
+    def __del__(self):
+        # an unfinished build (abandoned part way) releases its object
+        if getattr(self, "h", None) and _LIB is not None:
+            _LIB.orc_build_finish(self.h, None)
+            self.h = None
+
+
+def build_pieces(ell, q_power, kept, wave, check=True):
+    """Number of Build.step() calls of a build whose kept count is `kept`
+    (sketch, (q_power + 2) F-applies in waves, q_power + 1 CholQR2, the
+    Rayleigh-Ritz step, the check's waves)."""
+    w = wave if wave > 0 else ell
+    n = 1 + (q_power + 2) * (-(-ell // w)) + (q_power + 1) + 1
+    if check and kept > 0:
+        n += -(-kept // w)
+    return n
 
 
 def dsyevd(A, vecs=False):

@@ -7,6 +7,10 @@
 # generated translation unit stays under _ref/ (git-ignored).  When the
 # reference tree is absent (the GPU host) nothing is built and the committed
 # golden fixtures made from this library are used instead.
+#
+# The reference tree is read from $LGH_REFERENCE_ROOT.  Unset, it defaults
+# to /root/reference, the read-only mount of the reference project in the
+# container where the fixtures were generated; set it to build elsewhere.
 set -e
 REF=${LGH_REFERENCE_ROOT:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)

@@ -756,6 +756,9 @@ struct orc_glr
   std::vector<double> U;   /* n x kept, column-major */
   std::vector<double> lam; /* treated, |lam|-descending */
   int kept;
+  int cap; /* keep at most cap modes (rank r + oversample p: ell = r + p,
+            * cap = r); 0 = no cap.  An extension of this build, not a
+            * reference option; the device library applies the same rule. */
   /* sketch state kept for the incremental extension: Q (n x ell) and the
    * raw projected A = Q^T F Q (ell x ell, column-major) */
   std::vector<double> Q, A;
@@ -904,6 +907,14 @@ rayleigh_ritz_select (orc_glr *g, int ell, const double *Q,
   rep->kept = kept;
   rep->lam_abs_max = absmax;
   rep->next_abs = (kept < ell) ? fabs (evals[order[kept]]) : 0.;
+  if (g->cap > 0 && kept > g->cap) {
+    /* rank cap: the cap largest |lambda|; the first mode it cuts, treated,
+     * becomes next_abs */
+    kept = g->cap;
+    rep->kept = kept;
+    const double l = evals[order[kept]];
+    rep->next_abs = fabs (g->opts.treat == 1 ? std::max (l, 0.) : l);
+  }
   rep->lam_raw_max = evals[ell - 1];
   rep->lam_raw_min = evals[0];
   rep->n_negative_raw = 0;
@@ -934,70 +945,134 @@ rayleigh_ritz_select (orc_glr *g, int ell, const double *Q,
   return 0;
 }
 
-/* residual check: max_j ||F u_j - lam_raw_j u_j|| (glr_common_impl.h:576-600) */
-static void
-residual_check (orc_glr *g, const std::vector<double> &evals,
-                const std::vector<int> &order, orc_glr_report_t *rep)
+/* replicated build (glr_common_impl.h:414-608) as a resumable sequence of
+ * pieces.  The reference's build is one call; it is restated here as a
+ * state machine so that a caller can advance it one bounded piece at a
+ * time (one sketch, one wave of F-apply columns, one CholQR2, the
+ * Rayleigh-Ritz step, one wave of the residual check).  Every Z-solve and
+ * B product is per column, so splitting an F-apply into column waves gives
+ * the same bits as the whole block; orc_glr_compute runs the same machine
+ * with one wave per F-apply. */
+enum { BLD_SKETCH, BLD_F, BLD_ORTH, BLD_RR, BLD_CHECK, BLD_DONE };
+
+struct orc_build
 {
+  orc_glr *g;
+  orc_glr_report_t rep;
+  int wave;  /* F-apply columns per piece */
+  int phase;
+  int fpass; /* which F-apply of the build: 0 .. q_power + 1 */
+  int col;   /* next column of the current F-apply */
+  int rc;
+  std::vector<double> Q, Y, FU, evals;
+  std::vector<int> order;
+};
+
+static void
+build_init (orc_build *b, orc_glr *g, int wave)
+{
+  b->g = g;
+  memset (&b->rep, 0, sizeof (b->rep));
+  b->wave = wave > 0 ? wave : g->opts.ell;
+  b->phase = BLD_SKETCH;
+  b->fpass = 0;
+  b->col = 0;
+  b->rc = 0;
+}
+
+/* one piece; returns 1 while pieces remain, 0 when done, or an error code
+ * (negated) */
+static int
+build_step (orc_build *b)
+{
+  orc_glr *g = b->g;
+  const int ell = g->opts.ell;
   const int64_t n = g->n;
-  const int kept = g->kept;
-  if (!g->opts.check || kept == 0) return;
-  std::vector<double> FU ((size_t) n * kept);
+  orc_glr_report_t *rep = &b->rep;
   double t0 = now_s ();
-  apply_F_block (g, kept, g->U.data (), FU.data ());
-  rep->t_operator += now_s () - t0;
-  for (int j = 0; j < kept; j++) {
-    double lraw = evals[order[j]], s = 0.;
-    for (int64_t i = 0; i < n; i++) {
-      double d = FU[i + (size_t) j * n] - lraw * g->U[i + (size_t) j * n];
-      s += d * d;
+  switch (b->phase) {
+  case BLD_SKETCH:
+    b->Q.assign ((size_t) n * ell, 0.);
+    b->Y.assign ((size_t) n * ell, 0.);
+    orc_sketch (g->opts.seed, n, 0, ell, b->Q.data ());
+    b->phase = BLD_F;
+    b->fpass = 0;
+    b->col = 0;
+    return 1;
+  case BLD_F: {
+    const int m = std::min (b->wave, ell - b->col);
+    apply_F_block (g, m, b->Q.data () + (size_t) b->col * n,
+                   b->Y.data () + (size_t) b->col * n);
+    rep->t_operator += now_s () - t0;
+    b->col += m;
+    if (b->col < ell) return 1;
+    b->col = 0;
+    /* F(Omega), then q_power power passes, then the projection pass */
+    b->phase = (b->fpass < g->opts.q_power + 1) ? BLD_ORTH : BLD_RR;
+    return 1;
+  }
+  case BLD_ORTH:
+    if (cholqr2 (n, ell, b->Y.data ())) { b->rc = 76; return -76; }
+    rep->t_dense += now_s () - t0;
+    b->Q.swap (b->Y); /* Q = Y; Y is rewritten whole by the next F-apply */
+    b->fpass++;
+    b->phase = BLD_F;
+    return 1;
+  case BLD_RR: {
+    std::vector<double> A ((size_t) ell * ell);
+    int bm = (int) n, bn = ell;
+    double one = 1.0, zero = 0.0;
+    scipy_dgemm_ ("T", "N", &bn, &bn, &bm, &one, b->Q.data (), &bm,
+                  b->Y.data (), &bm, &zero, A.data (), &bn);
+    int rc = rayleigh_ritz_select (g, ell, b->Q.data (), A.data (), rep,
+                                   &b->evals, &b->order);
+    if (rc) { b->rc = rc; return -rc; }
+    if (g->incremental) { g->Q.swap (b->Q); g->A.swap (A); }
+    std::vector<double> ().swap (b->Y);
+    if (g->opts.check && g->kept > 0) {
+      b->FU.assign ((size_t) n * g->kept, 0.);
+      b->col = 0;
+      b->phase = BLD_CHECK;
+      return 1;
     }
-    rep->resid_max = std::max (rep->resid_max, sqrt (s));
+    b->phase = BLD_DONE;
+    return 0;
+  }
+  case BLD_CHECK: {
+    const int kept = g->kept;
+    const int m = std::min (b->wave, kept - b->col);
+    apply_F_block (g, m, g->U.data () + (size_t) b->col * n,
+                   b->FU.data () + (size_t) b->col * n);
+    rep->t_operator += now_s () - t0;
+    b->col += m;
+    if (b->col < kept) return 1;
+    /* residual check: max_j ||F u_j - lam_raw_j u_j|| (:576-600) */
+    for (int j = 0; j < kept; j++) {
+      double lraw = b->evals[b->order[j]], s = 0.;
+      for (int64_t i = 0; i < n; i++) {
+        double d = b->FU[i + (size_t) j * n] - lraw * g->U[i + (size_t) j * n];
+        s += d * d;
+      }
+      rep->resid_max = std::max (rep->resid_max, sqrt (s));
+    }
+    std::vector<double> ().swap (b->FU);
+    b->phase = BLD_DONE;
+    return 0;
+  }
+  default:
+    return 0;
   }
 }
 
-/* replicated build (glr_common_impl.h:414-608) */
 static int
 build_replicated (orc_glr *g, orc_glr_report_t *rep)
 {
-  const int ell = g->opts.ell;
-  const int64_t n = g->n;
-  memset (rep, 0, sizeof (*rep));
-  std::vector<double> Y ((size_t) n * ell), Q ((size_t) n * ell);
-  orc_sketch (g->opts.seed, n, 0, ell, Q.data ());
-  double t0 = now_s ();
-  apply_F_block (g, ell, Q.data (), Y.data ());
-  rep->t_operator += now_s () - t0;
-  for (int p = 0; p < g->opts.q_power; p++) {
-    t0 = now_s ();
-    if (cholqr2 (n, ell, Y.data ())) return 76;
-    rep->t_dense += now_s () - t0;
-    Q = Y;
-    t0 = now_s ();
-    apply_F_block (g, ell, Q.data (), Y.data ());
-    rep->t_operator += now_s () - t0;
-  }
-  t0 = now_s ();
-  if (cholqr2 (n, ell, Y.data ())) return 76;
-  rep->t_dense += now_s () - t0;
-  Q = Y;
-  t0 = now_s ();
-  apply_F_block (g, ell, Q.data (), Y.data ());
-  rep->t_operator += now_s () - t0;
-  std::vector<double> A ((size_t) ell * ell);
-  {
-    int bm = (int) n, bn = ell;
-    double one = 1.0, zero = 0.0;
-    scipy_dgemm_ ("T", "N", &bn, &bn, &bm, &one, Q.data (), &bm, Y.data (),
-                  &bm, &zero, A.data (), &bn);
-  }
-  std::vector<double> evals;
-  std::vector<int> order;
-  int rc = rayleigh_ritz_select (g, ell, Q.data (), A.data (), rep, &evals,
-                                 &order);
-  if (rc) return rc;
-  residual_check (g, evals, order, rep);
-  if (g->incremental) { g->Q.swap (Q); g->A.swap (A); }
+  orc_build b;
+  build_init (&b, g, 0);
+  int st;
+  while ((st = build_step (&b)) == 1) {}
+  if (st < 0) return -st;
+  *rep = b.rep;
   return 0;
 }
 
@@ -1062,14 +1137,10 @@ extend_incremental (orc_glr *g, int k_new, orc_glr_report_t *rep)
   return 0;
 }
 
-extern "C" int
-orc_glr_compute (const orc_csr *B, orc_prior *prior,
-                 const orc_glr_opts_t *opts, int incremental, orc_glr **out,
-                 orc_glr_report_t *report)
+static orc_glr *
+glr_new (const orc_csr *B, orc_prior *prior, const orc_glr_opts_t *opts,
+         int incremental, int cap)
 {
-  orc_glr_report_t rep;
-  /* 0 < ell <= N (glr_common_impl.h:651-654) */
-  if (opts->ell <= 0 || opts->ell > B->n) return 63;
   orc_glr *g = new orc_glr;
   g->n = B->n;
   g->B = B;
@@ -1078,11 +1149,68 @@ orc_glr_compute (const orc_csr *B, orc_prior *prior,
   g->opts = *opts;
   g->incremental = incremental;
   g->kept = 0;
+  g->cap = cap > 0 ? cap : 0;
+  return g;
+}
+
+extern "C" int
+orc_glr_compute_cap (const orc_csr *B, orc_prior *prior,
+                     const orc_glr_opts_t *opts, int incremental, int cap,
+                     orc_glr **out, orc_glr_report_t *report)
+{
+  orc_glr_report_t rep;
+  /* 0 < ell <= N (glr_common_impl.h:651-654) */
+  if (opts->ell <= 0 || opts->ell > B->n) return 63;
+  orc_glr *g = glr_new (B, prior, opts, incremental, cap);
   int rc = build_replicated (g, &rep);
   if (rc) { orc_prior_destroy (prior); delete g; return rc; }
   if (report) *report = rep;
   *out = g;
   return 0;
+}
+
+extern "C" int
+orc_glr_compute (const orc_csr *B, orc_prior *prior,
+                 const orc_glr_opts_t *opts, int incremental, orc_glr **out,
+                 orc_glr_report_t *report)
+{
+  return orc_glr_compute_cap (B, prior, opts, incremental, 0, out, report);
+}
+
+/* The same build, advanced by the caller one piece at a time: begin, then
+ * step until it returns 0 (negative: the error code of the failed step,
+ * negated), then finish, which hands over the object and the report.
+ * `wave` = F-apply columns per piece (0: a whole F-apply per piece). */
+extern "C" orc_build *
+orc_build_begin (const orc_csr *B, orc_prior *prior,
+                 const orc_glr_opts_t *opts, int incremental, int cap,
+                 int wave)
+{
+  if (opts->ell <= 0 || opts->ell > B->n) return NULL;
+  orc_build *b = new orc_build;
+  build_init (b, glr_new (B, prior, opts, incremental, cap), wave);
+  return b;
+}
+
+extern "C" int
+orc_build_step (orc_build *b)
+{
+  return build_step (b);
+}
+
+extern "C" orc_glr *
+orc_build_finish (orc_build *b, orc_glr_report_t *report)
+{
+  orc_glr *g = b->g;
+  if (b->phase != BLD_DONE || b->rc) {
+    orc_prior_destroy (g->prior);
+    delete g;
+    g = NULL;
+  } else if (report) {
+    *report = b->rep;
+  }
+  delete b;
+  return g;
 }
 
 /* glr_common_impl.h:684-719 */
@@ -1208,6 +1336,30 @@ orc_glr_solve (orc_glr *g, double c, const double *rhs, double *x)
   filter_core (g, f.data (), 1. / c, w1.data (), w2.data ());
   for (int64_t i = 0; i < n; i++) w2[i] *= g->prior->msqrt[i];
   orc_prior_solveZ (g->prior, w2.data (), x);
+  return 0;
+}
+
+/* lgh_glr_solve (glr_common_impl.h:1007-1024) on m right-hand sides at
+ * one shift, column-major n x m: the two Z-solves run column-parallel
+ * (orc_prior_solve_block), the master formula as one block product
+ * (glr_common_impl.h:910-929).  Per column the same arithmetic as m calls
+ * of orc_glr_solve, with the BLAS-2 passes over U batched into BLAS-3. */
+extern "C" int
+orc_glr_solve_block (orc_glr *g, double c, int m, const double *rhs,
+                     double *x)
+{
+  const int64_t n = g->n;
+  if (!(c > 0.)) return 63;
+  std::vector<double> W1 ((size_t) n * m), W2 ((size_t) n * m),
+      f (std::max (g->kept, 1));
+  orc_prior_solve_block (g->prior, m, rhs, W1.data ());
+  for (int j = 0; j < m; j++)
+    for (int64_t i = 0; i < n; i++) W1[i + (size_t) j * n] *= g->prior->msqrt[i];
+  for (int i = 0; i < g->kept; i++) f[i] = 1. / (g->lam[i] + c);
+  orc_glr_filter_block (g, f.data (), 1. / c, m, W1.data (), W2.data ());
+  for (int j = 0; j < m; j++)
+    for (int64_t i = 0; i < n; i++) W2[i + (size_t) j * n] *= g->prior->msqrt[i];
+  orc_prior_solve_block (g->prior, m, W2.data (), x);
   return 0;
 }
 

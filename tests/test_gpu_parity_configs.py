@@ -1,0 +1,176 @@
+"""Device-vs-oracle parity at the benchmark's own configurations.
+
+* Config 2, the headline job's operator (512^2 grid, N = 262144, B with
+  ~183 nnz/row): ell = 220 (rank 200 + oversample 20, rank cap 200), q = 1,
+  seed 0, residual check on; the Z-solves of both sides at rtol 1e-12.
+  The same sketch enters both builds (the hashed generator of
+  glr_common_impl.h:35-73), so the kept spectra, the logdet and the
+  solve / sample outputs agree to Z-solve accuracy.
+* Config 3's operator formulas on a 32^3 grid (7-point Z = h L + 16 M),
+  lgh_glr_compute at ell = 40 then lgh_glr_extend by 40 (the incremental
+  extension of glr_scalapack_impl.h:689-915), in FP64 and in mixed
+  precision, against the oracle's compute + extend on the same inputs
+  (the extend gate of tests/test_glr.cpp:299-316 is the one-shot
+  equality; here the target is the oracle's own extended object).
+* Mixed precision, per eigenvalue.  In the mixed form B's values are FP32
+  (config 3 defines them so).  Rounding B to FP32 perturbs F by about
+  eps_32 ||F|| in norm, so against the FP64 B every eigenvalue moves by up
+  to a few eps_32 lambda_max, a bound relative to lambda_max and not to
+  lambda_i.  The mixed algorithm itself (FP32 blocks with FP64
+  accumulation, FP64 Rayleigh-Ritz) is gated per eigenvalue against an
+  FP64 build of the same FP32-rounded B: relative error <= 1e-5 on every
+  kept eigenvalue.
+"""
+
+import numpy as np
+import pytest
+
+import lgh_b200 as L
+import oracle
+from lgh_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+
+EPS32 = float(np.finfo(np.float32).eps)
+
+
+def _rd(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def _rounded32(csr):
+    out = dict(csr)
+    out["vals"] = np.asarray(csr["vals"]).astype(np.float32).astype(
+        np.float64)
+    return out
+
+
+def _oracle_objs(cfg, B=None, pc="amg", rtol=1e-12):
+    B = cfg["B"] if B is None else B
+    Bo = oracle.Csr(B["rowptr"], B["colidx"], B["vals"])
+    Zo = oracle.Csr(cfg["Z"]["rowptr"], cfg["Z"]["colidx"], cfg["Z"]["vals"])
+    po = oracle.Prior(Zo, cfg["mass"], ksp_rtol=rtol, pc=pc)
+    return Bo, Zo, po
+
+
+@pytest.fixture(scope="module")
+def c2(cuda_device):
+    L.load()
+    cfg = P.grid_problem("c2")
+    B, Z = L.Mat(cfg["B"]), L.Mat(cfg["Z"])
+    pr = L.Prior(Z=Z, mass=cfg["mass"], opts=L.prior_opts(ksp_rtol=1e-12))
+    return cfg, B, Z, pr
+
+
+def test_c2_headline_build_parity_with_oracle(c2):
+    """ell 220 / rank cap 200 at the headline operator, device vs oracle."""
+    cfg, B, Z, pr = c2
+    o = L.glr_opts(ell=220, q_power=1, seed=0, trunc_rel=0.0, check=1)
+    g = L.Glr(B, pr, o, exec=L.exec_opts(rank_cap=200))
+    oracle.set_threads(0)
+    Bo, Zo, po = _oracle_objs(cfg)
+    go = oracle.Glr(Bo, po, oracle.opts_default(ell=220, q_power=1, seed=0,
+                                                trunc_rel=0.0, check=1),
+                    cap=200)
+    assert g.report["kept"] == go.report["kept"] == 200
+    ld, lo = g.eigs(), go.eigs()
+    # every kept eigenvalue to 1e-8 relative (the C1 gate), and to 1e-11
+    # of lambda_max
+    assert np.max(np.abs(ld - lo) / lo) < 1e-8
+    assert np.max(np.abs(ld - lo)) < 1e-11 * lo[0]
+    for k in ("lam_abs_max", "next_abs"):
+        assert abs(g.report[k] - go.report[k]) < 1e-8 * abs(go.report[k])
+    assert abs(g.logdet(1.0) - go.logdet(1.0)) < 1e-9 * abs(go.logdet(1.0))
+    R = oracle.sketch(3, cfg["N"], 0, 2)
+    for j in range(2):
+        assert _rd(g.solve(1.0, R[:, j]), go.solve(1.0, R[:, j])) < 1e-7
+        assert _rd(g.sample(1.0, R[:, j]), go.sample(1.0, R[:, j])) < 1e-7
+    # the residual check of the capped build (the worst of the 200
+    # eigenpairs) reports the same figure on both sides
+    assert abs(g.report["resid_max"] - go.report["resid_max"]) \
+        < 1e-3 * go.report["resid_max"]
+
+
+def test_c2_mixed_per_eigenvalue(c2):
+    """Mixed build at the headline shape: per eigenvalue against the FP64
+    build of the same FP32-rounded B; against the FP64 B within a few
+    eps_32 lambda_max."""
+    cfg, B, Z, pr = c2
+    o = L.glr_opts(ell=220, q_power=1, seed=0, trunc_rel=0.0, check=0)
+    gm = L.Glr(B, pr, o, exec=L.exec_opts(rank_cap=200,
+                                          precision=L.PREC_MIXED))
+    B32 = L.Mat(_rounded32(cfg["B"]))
+    g32 = L.Glr(B32, pr, o, exec=L.exec_opts(rank_cap=200))
+    g64 = L.Glr(B, pr, o, exec=L.exec_opts(rank_cap=200))
+    lm, l32, l64 = gm.eigs(), g32.eigs(), g64.eigs()
+    assert len(lm) == len(l32) == len(l64) == 200
+    assert np.max(np.abs(lm - l32) / l32) < 1e-5
+    assert np.max(np.abs(lm - l64)) < 8 * EPS32 * l64[0]
+    assert np.max(np.abs(l32 - l64)) < 8 * EPS32 * l64[0]
+
+
+@pytest.fixture(scope="module")
+def c3s(cuda_device):
+    L.load()
+    cfg = P.grid_problem("c3_32")
+    B, Z = L.Mat(cfg["B"]), L.Mat(cfg["Z"])
+    pr = L.Prior(Z=Z, mass=cfg["mass"], opts=L.prior_opts(ksp_rtol=1e-12))
+    return cfg, B, Z, pr
+
+
+def _compute_extend_dev(B, pr, prec):
+    g = L.Glr(B, pr, L.glr_opts(ell=40, q_power=1, seed=0, trunc_rel=0.0,
+                                check=1),
+              exec=L.exec_opts(precision=prec))
+    rep0 = dict(g.report)
+    g.extend(40)
+    return g, rep0
+
+
+def _compute_extend_oracle(cfg, B=None):
+    Bo, Zo, po = _oracle_objs(cfg, B)
+    go = oracle.Glr(Bo, po, oracle.opts_default(ell=40, q_power=1, seed=0,
+                                                trunc_rel=0.0, check=1))
+    rep0 = dict(go.report)
+    go.extend(40)
+    return go, rep0, (Bo, Zo, po)
+
+
+def test_c3_formulas_3d_compute_extend_fp64_parity(c3s):
+    cfg, B, Z, pr = c3s
+    assert cfg["N"] == 32 ** 3 and cfg["nnz_Z"] < 7 * cfg["N"]
+    g, rep0 = _compute_extend_dev(B, pr, L.PREC_FP64)
+    oracle.set_threads(0)
+    go, repo0, keep = _compute_extend_oracle(cfg)
+    assert rep0["kept"] == repo0["kept"] == 40
+    assert abs(rep0["resid_max"] - repo0["resid_max"]) \
+        < 1e-3 * repo0["resid_max"]
+    ld, lo = g.eigs(), go.eigs()
+    assert len(ld) == len(lo) == 80
+    assert np.max(np.abs(ld - lo) / lo) < 1e-8
+    assert abs(g.logdet(1.0) - go.logdet(1.0)) < 1e-9 * abs(go.logdet(1.0))
+    rhs = oracle.sketch(5, cfg["N"], 0, 1)[:, 0]
+    assert _rd(g.solve(1.0, rhs), go.solve(1.0, rhs)) < 1e-7
+    assert _rd(g.sample(1.0, rhs), go.sample(1.0, rhs)) < 1e-7
+    # the extended basis spans the oracle's leading eigenvectors
+    U, Uo = g.U()[:, :20], go.U()[:, :20]
+    s = np.linalg.svd(Uo.T @ U, compute_uv=False)
+    assert np.sqrt(max(0.0, 1.0 - float(np.min(s)) ** 2)) < 1e-5
+
+
+def test_c3_formulas_3d_compute_extend_mixed(c3s):
+    cfg, B, Z, pr = c3s
+    gm, _ = _compute_extend_dev(B, pr, L.PREC_MIXED)
+    oracle.set_threads(0)
+    go32, _, keep32 = _compute_extend_oracle(cfg, _rounded32(cfg["B"]))
+    go64, _, keep64 = _compute_extend_oracle(cfg)
+    lm, l32, l64 = gm.eigs(), go32.eigs(), go64.eigs()
+    assert len(lm) == len(l32) == 80
+    # the mixed algorithm, per eigenvalue, against FP64 on the same
+    # (FP32-rounded) operator
+    assert np.max(np.abs(lm - l32) / l32) < 1e-5
+    # the rounding of B's values, against the FP64 operator
+    assert np.max(np.abs(lm - l64)) < 8 * EPS32 * l64[0]
+    rhs = oracle.sketch(6, cfg["N"], 0, 1)[:, 0]
+    # downstream operations run in FP64 on the mixed model
+    assert _rd(gm.solve(1.0, rhs), go32.solve(1.0, rhs)) < 1e-4

@@ -119,3 +119,33 @@ def test_oracle_c1_shape_runs():
                                               trunc_rel=1e-3))
     lam = g.eigs()
     assert len(lam) > 0 and np.all(np.diff(lam) <= 0)
+
+
+def test_build_in_pieces_equals_one_shot():
+    """The oracle's build advanced in bounded pieces (7-column F-apply
+    waves) is the same object, bit for bit, as the one-shot build; the
+    piece count matches the plan; the rank cap keeps the largest |lambda|
+    and reports the first cut mode as next_abs."""
+    p, (B, Z, pr), g = _build(True)
+    o = oracle.opts_default(ell=40, q_power=1, trunc_abs=0., trunc_rel=1e-8,
+                            nb=8, panel=16, check=1)
+    b = oracle.Build(B, pr, o, wave=7)
+    steps = 1
+    while b.step():
+        steps += 1
+    gp = b.finish()
+    assert steps == oracle.build_pieces(40, 1, gp.report["kept"], 7)
+    assert np.array_equal(gp.eigs(), g.eigs())
+    assert np.array_equal(gp.U(), g.U())
+    assert gp.report["resid_max"] == g.report["resid_max"]
+    v = p["probe"]
+    assert np.array_equal(gp.solve(C, v), g.solve(C, v))
+    X = np.stack([v, 2 * v + 1], axis=1)
+    Xs = gp.solve_block(C, X)
+    for j in range(2):
+        x1 = g.solve(C, X[:, j])
+        assert _rd(Xs[:, j], x1) < 1e-13
+    gc = oracle.Glr(B, pr, o, cap=6)
+    assert gc.report["kept"] == 6
+    assert np.array_equal(gc.eigs(), g.eigs()[:6])
+    assert gc.report["next_abs"] == g.eigs()[6]
