@@ -562,6 +562,10 @@ int lgh_test_sketch (uint64_t seed, int64_t n, int64_t j0, int k,
 int lgh_test_rng_state (uint64_t seed, int64_t n, int64_t j0, int k,
                         uint64_t *out);
 int lgh_test_spmm (lgh_Mat A, int w, const double *X, double *Y, int fp32);
+/* the same product through the strip form of A at height R (2, 4, 8; 0 =
+ * chosen by the cost model); *R_used (nullable) gets the height */
+int lgh_test_spmm_strip (lgh_Mat A, int w, const double *X, double *Y,
+                         int fp32, int R, int *R_used);
 int lgh_test_zsolve (lgh_prior_t *prior, int w, const double *X, double *Y,
                      int fp32);
 /* one Chebyshev-Jacobi smoothing step of a square CSR Mat (n x w row-major

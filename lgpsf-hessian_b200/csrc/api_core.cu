@@ -555,8 +555,29 @@ mat_release (lgh_Mat A)
 {
   if (!A || --A->refs > 0) return;
   if (A->kind == 0) csr_free (A->csr);
+  strip_free (A->strips);
   delete A;
 }
+
+template <typename T>
+int
+mat_mult_block (lgh_Mat A, const T *X, int ldx, T *Y, int ldy, int w,
+                cudaStream_t s)
+{
+  if (w >= 8) {
+    if (!A->strips_built) {
+      LGH_TRY (strip_build (A->csr, A->strip_R, A->strips));
+      A->strips_built = 1;
+    }
+    return launch_strip_spmm<T> (A->strips, X, ldx, Y, ldy, w, s);
+  }
+  return launch_spmm<T> (A->csr, X, ldx, Y, ldy, w, s);
+}
+
+template int mat_mult_block<double> (lgh_Mat, const double *, int, double *,
+                                     int, int, cudaStream_t);
+template int mat_mult_block<float> (lgh_Mat, const float *, int, float *, int,
+                                    int, cudaStream_t);
 
 int
 mat_mult_vec (lgh_Mat A, const double *x, double *y)

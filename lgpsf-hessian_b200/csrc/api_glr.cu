@@ -209,7 +209,7 @@ apply_F (lgh_glr_t *g, int w, const T *X, int ldx, T *Y, int ldy, T *W,
   static thread_local EventRing ring;
   const bool timing = ktime_on ();
   if (timing) LGH_TRY (ring.record (s));
-  LGH_TRY (launch_spmm<T> (g->B->csr, W, ldw, Y, ldy, w, s));
+  LGH_TRY (mat_mult_block<T> (g->B, W, ldw, Y, ldy, w, s));
   if (timing) LGH_TRY (ring.record (s));
   LGH_CUDA (cudaStreamSynchronize (s));
   if (timing) {

@@ -106,7 +106,50 @@ lgh_test_rng_state (uint64_t seed, int64_t n, int64_t j0, int k, uint64_t *out)
   return down (out, S, (size_t) n * k);
 }
 
-/* Y = A X, X and Y n x w row-major; fp32 != 0 runs the float path */
+/* Y = A X through the strip form at height R (2, 4 or 8; 0 = the cost
+ * model's choice), X and Y n x w row-major; fp32 != 0 runs the float path.
+ * The form is rebuilt for each call; *R_used (nullable) receives its
+ * height. */
+int
+lgh_test_spmm_strip (lgh_Mat A, int w, const double *X, double *Y, int fp32,
+                     int R, int *R_used)
+{
+  LGH_TRY (ensure_init ());
+  LGH_CHECK (A && A->kind == 0, LGH_ERR_ARG_WRONG, "lgh_test_spmm_strip: CSR Mat");
+  LGH_CHECK (R == 0 || R == 2 || R == 4 || R == 8, LGH_ERR_ARG_OUTOFRANGE,
+             "lgh_test_spmm_strip: R must be 0, 2, 4 or 8");
+  StripForm S;
+  LGH_TRY (strip_build (A->csr, R, S));
+  if (R_used) *R_used = S.R;
+  const int64_t n = A->csr.n;
+  const int ld = round_ld (w);
+  std::vector<double> hx ((size_t) n * ld, 0.);
+  for (int64_t i = 0; i < n; i++) memcpy (hx.data () + i * ld, X + i * w, w * sizeof (double));
+  std::vector<double> hy ((size_t) n * ld);
+  int rc = 0;
+  if (!fp32) {
+    DBuf<double> dx, dy;
+    if (!rc) rc = up (dx, hx.data (), hx.size ());
+    if (!rc) rc = dy.alloc (hx.size ());
+    if (!rc) rc = launch_strip_spmm<double> (S, dx.p, ld, dy.p, ld, w, stream ());
+    if (!rc) rc = down (hy.data (), dy, hy.size ());
+  } else {
+    std::vector<float> fx (hx.begin (), hx.end ()), fy (hx.size ());
+    DBuf<float> dx, dy;
+    if (!rc) rc = up (dx, fx.data (), fx.size ());
+    if (!rc) rc = dy.alloc (fx.size ());
+    if (!rc) rc = launch_strip_spmm<float> (S, dx.p, ld, dy.p, ld, w, stream ());
+    if (!rc) rc = down (fy.data (), dy, fy.size ());
+    for (size_t e = 0; e < fy.size (); e++) hy[e] = fy[e];
+  }
+  strip_free (S);
+  if (rc) return rc;
+  for (int64_t i = 0; i < n; i++) memcpy (Y + i * w, hy.data () + i * ld, w * sizeof (double));
+  return 0;
+}
+
+/* Y = A X by the row-wise CSR product, X and Y n x w row-major; fp32 != 0
+ * runs the float path */
 int
 lgh_test_spmm (lgh_Mat A, int w, const double *X, double *Y, int fp32)
 {

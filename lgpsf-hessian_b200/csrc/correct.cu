@@ -1,31 +1,56 @@
-/* correct.cu -- stage 2.5: the deflation correction against the true
- * Hessian (the reference's include/lgpsf_hessian/impl/correct_impl.h,
- * lgh_glr_correct_probes :583-800 and lgh_glr_correct :803-904).
+/* correct.cu -- stage 2.5: the deflation correction of a built GLR object
+ * against the true data-misfit Hessian H_d (the reference's
+ * include/lgpsf_hessian/impl/correct_impl.h: lgh_glr_correct_probes
+ * :583-800, lgh_glr_correct :803-904, the graft :325-489).
  *
- * With S^± = (U lam U^T + c0 I)^{±1/2} and F_true = M^{1/2} Z^{-1} H_d
- * Z^{-T} M^{1/2}, the whitened error operator E_w = S^-(F_true + c0 I)S^- - I
- * is symmetric; its dominant eigenpairs (V, D) give the correction
- * F_corr = U lam U^T + Vhat D Vhat^T, Vhat = S^+ V, grafted into a new
- * (U', lam') by orthogonalisation against U and a small eigensolve
- * (correct_impl.h:325-489).  The error basis comes either from the probe
- * pairs the fit stage already has (value pass: the residuals
- * Yw - U lam U^T X of the whitened probes, no true applies) or from a hashed
- * Gaussian sketch of E_w (fresh pass); the apply budget then prices the
- * top basis directions exactly (Rayleigh values d, clamped at
- * -1 + clamp_eps, kept by |d|, signs kept).
+ * The mathematics.  The object holds the model U lam U^T of the whitened
+ * sparse fit.  With the whitening metric S^(+-) = (U lam U^T + c0 I)^(+-1/2)
+ * and the whitened true operator F_true = M^(1/2) Z^-1 H_d Z^-T M^(1/2),
+ * the error of the model in that metric is the symmetric operator
+ *     E_w = S^- (F_true + c0 I) S^- - I .
+ * If E_w ~ V D V^T (V orthonormal, D its dominant eigenvalues, kept with
+ * their signs), then F_true ~ U lam U^T + Vh D Vh^T with Vh = S^+ V, and
+ * that rank-(kept + r) operator is re-diagonalised into a new (U', lam').
+ * Afterwards the object serves the corrected operator at every shift above
+ * floor = max(0, -min lam').
  *
- * Every tall block is a row-major N x m device block (ld a multiple of 4),
- * as in the rest of the library: Z-solves, U passes and Gram products run
- * on the device; the true-Hessian callback gets host arrays one column at a
- * time (the reference's local arrays); the small symmetric eigenproblems
- * (m x m, m <= the apply budget or the probe count) run on the device
- * Jacobi solver.
+ * Where the directions V come from:
+ *   value pass  (lgh_glr_correct_probes): from the k probe pairs the fit
+ *     stage already holds, (Omega, H_d Omega).  Whitening them costs no
+ *     true applies: X = M^(-1/2) Z^T Omega satisfies F_true X = Yw with
+ *     Yw = M^(1/2) Z^-1 H_d Omega, so S^-(Yw - U lam U^T X) are images of
+ *     E_w (up to the S^- factor) for free; their energy-ordered basis is
+ *     the search space.  The apply budget prices the leading directions
+ *     exactly (one true apply each), and, budget left, one power step
+ *     past them adds fresh directions.
+ *   fresh pass  (lgh_glr_correct): a hashed Gaussian block in the
+ *     whitened frame, pushed through E_w (plus q_power passes), then
+ *     priced like the value pass.
+ * Pricing: the Rayleigh quotient matrix Q^T E_w Q on the priced directions
+ * Q, its eigenpairs ordered by |d|, a rank cap and a |d| floor, and a clamp
+ * d >= -1 + clamp_eps (an exact error eigenvalue satisfies 1 + d > 0; the
+ * clamp guards against estimation noise only).
+ *
+ * Design (this file).  A Deflator owns the object, the options, a device
+ * workspace and the counters of one correction.  Every tall block is a
+ * row-major device panel; the directions and their images are written
+ * straight into column ranges of two panels sized for the whole budget, so
+ * nothing is concatenated.  Every small matrix (Gram, Rayleigh, the
+ * combined coefficient matrix of the re-diagonalisation) is formed on the
+ * device by the split-K products or a dedicated kernel, eigendecomposed on
+ * the device (cyclic Jacobi), and only its eigenvalues cross to the host,
+ * where the selection rules run on a few hundred numbers; the chosen
+ * eigenvector columns are gathered on the device.  The true-Hessian
+ * callback receives host arrays (the reference's local arrays): a panel is
+ * staged to the host as one column-major transfer, the callback runs on
+ * each contiguous column, and the responses return as one transfer.
  */
 
 #include <math.h>
 #include <string.h>
 
 #include <algorithm>
+#include <numeric>
 #include <vector>
 
 #include "lgh_internal.h"
@@ -37,521 +62,629 @@ namespace lgh
 namespace
 {
 
-/* Z = a X + b Y on row-major blocks (any of them may be the same) */
+/* ---- device kernels ------------------------------------------------------ */
+
+/* Z = a X + b Y over n rows and m columns of row-major panels (any two may
+ * alias element for element) */
 __global__ void
-k_blk_axpby (int64_t n, int m, double a, const double *X, int ldx, double b,
-             const double *Y, int ldy, double *Z, int ldz)
+k_panel_axpby (int64_t n, int m, double a, const double *X, int ldx, double b,
+               const double *Y, int ldy, double *Z, int ldz)
 {
   const int64_t total = n * m;
   for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (int64_t) gridDim.x * blockDim.x) {
     const int64_t i = e / m;
     const int j = (int) (e - i * m);
-    const double x = a != 0. ? a * X[i * ldx + j] : 0.;
-    const double y = b != 0. ? b * Y[i * ldy + j] : 0.;
-    Z[i * ldz + j] = x + y;
+    double v = 0.;
+    if (a != 0.) v = a * X[i * ldx + j];
+    if (b != 0.) v += b * Y[i * ldy + j];
+    Z[i * ldz + j] = v;
+  }
+}
+
+/* W (rows x cols, column-major, ld rows) : W[k, j] *= f[k] - fc */
+__global__ void
+k_coeff_rows (int rows, int cols, const double *f, double fc, double *W)
+{
+  const int64_t total = (int64_t) rows * cols;
+  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t) gridDim.x * blockDim.x) {
+    const int k = (int) (e % rows);
+    W[e] *= f[k] - fc;
+  }
+}
+
+/* C[:, j] = V[:, idx[j]] * s[j]  (V n x n column-major, C n x m) */
+__global__ void
+k_gather_cols (int n, int m, const double *V, const int *idx, const double *s,
+               double *C)
+{
+  const int64_t total = (int64_t) n * m;
+  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t) gridDim.x * blockDim.x) {
+    const int j = (int) (e / n);
+    const int i = (int) (e - (int64_t) j * n);
+    C[e] = V[i + (int64_t) idx[j] * n] * s[j];
+  }
+}
+
+/* the combined coefficient matrix of the re-diagonalisation on the
+ * orthonormal basis [U | Qv] (n2 = kept0 + r2 columns):
+ *   T2 = diag(lam, 0) + CB diag(d) CB^T,   CB (n2 x r, column-major).
+ * One thread per entry pair (a <= b); both halves get the same value, so
+ * T2 is exactly symmetric. */
+__global__ void
+k_fold_matrix (int n2, int r, int kept0, const double *CB, const double *d,
+               const double *lam, double *T2)
+{
+  const int64_t total = (int64_t) n2 * n2;
+  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t) gridDim.x * blockDim.x) {
+    const int b = (int) (e / n2);
+    const int a = (int) (e - (int64_t) b * n2);
+    if (a > b) continue;
+    double acc = 0.;
+    for (int j = 0; j < r; j++)
+      acc += CB[a + (int64_t) j * n2] * d[j] * CB[b + (int64_t) j * n2];
+    if (a == b && a < kept0) acc += lam[a];
+    T2[a + (int64_t) b * n2] = acc;
+    T2[b + (int64_t) a * n2] = acc;
+  }
+}
+
+/* partial sums of squares of a panel: part[blockIdx] = sum over the
+ * block's rows of sum_j X[i, j]^2 (fixed order, then k_sum_parts) */
+__global__ void __launch_bounds__ (256)
+k_sumsq_part (int64_t n, int m, const double *X, int ldx, double *part)
+{
+  __shared__ double red[256];
+  double acc = 0.;
+  for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t) gridDim.x * blockDim.x)
+    for (int j = 0; j < m; j++) {
+      const double x = X[i * ldx + j];
+      acc += x * x;
+    }
+  red[threadIdx.x] = acc;
+  __syncthreads ();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if ((int) threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+    __syncthreads ();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+__global__ void
+k_sum_parts (int np, const double *part, double *out)
+{
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = 0.;
+    for (int i = 0; i < np; i++) s += part[i];
+    *out = s;
   }
 }
 
 int
-ewgrid (int64_t total)
+flat_grid (int64_t total)
 {
-  int64_t g = (total + 255) / 256;
-  const int64_t cap = (int64_t) num_sms () * 8;
-  return (int) std::max<int64_t> (1, std::min (g, cap));
+  const int64_t g = (total + 255) / 256;
+  return (int) std::max<int64_t> (1, std::min<int64_t> (g, (int64_t) num_sms () * 8));
 }
 
-/* a row-major N x m device block */
-struct Blk
+/* ---- panels ------------------------------------------------------------- */
+
+/* a row-major n x cols device block; column j of the panel is ptr + j with
+ * the panel's leading dimension, so a column range is a sub-panel */
+struct Panel
 {
-  DBuf<double> d;
+  DBuf<double> buf;
   int64_t n = 0;
-  int m = 0, ld = 4;
-  int alloc (int64_t n_, int m_)
+  int cols = 0, ld = 4;
+  int make (int64_t n_, int cols_)
   {
     n = n_;
-    m = m_;
-    ld = round_ld (std::max (m_, 1));
-    LGH_TRY (d.alloc ((size_t) n * ld));
-    LGH_CUDA (cudaMemsetAsync (d.p, 0, (size_t) n * ld * sizeof (double), stream ()));
+    cols = cols_;
+    ld = round_ld (std::max (cols_, 1));
+    LGH_TRY (buf.alloc ((size_t) n * ld));
+    LGH_CUDA (cudaMemsetAsync (buf.p, 0, (size_t) n * ld * sizeof (double),
+                               stream ()));
+    return 0;
+  }
+  double *at (int j) const { return buf.p + j; }
+};
+
+/* a device vector uploaded from host values */
+int
+upload (const std::vector<double> &h, DBuf<double> &d)
+{
+  LGH_TRY (d.alloc (std::max<size_t> (h.size (), 1)));
+  if (!h.empty ())
+    LGH_CUDA (cudaMemcpyAsync (d.p, h.data (), h.size () * sizeof (double),
+                               cudaMemcpyHostToDevice, stream ()));
+  return 0;
+}
+
+int
+upload_idx (const std::vector<int> &h, DBuf<int> &d)
+{
+  LGH_TRY (d.alloc (std::max<size_t> (h.size (), 1)));
+  if (!h.empty ())
+    LGH_CUDA (cudaMemcpyAsync (d.p, h.data (), h.size () * sizeof (int),
+                               cudaMemcpyHostToDevice, stream ()));
+  return 0;
+}
+
+/* eigendecomposition of a small symmetric device matrix (column-major):
+ * eigenvalues to the host, eigenvectors stay on the device, both in the
+ * solver's order (index i of vals is column i of vecs) */
+struct SmallEig
+{
+  DBuf<double> a, a2, vecs, v2, w;
+  std::vector<double> vals;
+  int n = 0;
+  int run (int n_, const double *A)
+  {
+    n = n_;
+    vals.assign (n, 0.);
+    if (n == 0) return 0;
+    const size_t nn = (size_t) n * n;
+    cudaStream_t s = stream ();
+    LGH_TRY (a.alloc (nn));
+    LGH_TRY (a2.alloc (nn));
+    LGH_TRY (vecs.alloc (nn));
+    LGH_TRY (v2.alloc (nn));
+    LGH_TRY (w.alloc (n));
+    LGH_CUDA (cudaMemcpyAsync (a.p, A, nn * sizeof (double),
+                               cudaMemcpyDeviceToDevice, s));
+    LGH_TRY (launch_syev_jacobi (n, a.p, vecs.p, w.p, a2.p, v2.p, nullptr, s));
+    LGH_CUDA (cudaMemcpyAsync (vals.data (), w.p, n * sizeof (double),
+                               cudaMemcpyDeviceToHost, s));
+    LGH_CUDA (cudaStreamSynchronize (s));
     return 0;
   }
 };
 
-int
-axpby (int64_t n, int m, double a, const double *X, int ldx, double b,
-       const double *Y, int ldy, double *Z, int ldz)
-{
-  if (n == 0 || m == 0) return 0;
-  k_blk_axpby<<<ewgrid (n * m), 256, 0, stream ()>>> (n, m, a, X, ldx, b, Y, ldy,
-                                                      Z, ldz);
-  LGH_LAUNCH_CHECK ();
-  return 0;
-}
-
-/* out (host, p x q column-major) = A^T B over n rows */
-int
-xtY (int64_t n, const double *A, int lda, int p, const double *B, int ldb,
-     int q, std::vector<double> &out)
-{
-  out.assign ((size_t) p * q, 0.);
-  if (p == 0 || q == 0) return 0;
-  DBuf<double> c, work;
-  LGH_TRY (c.alloc ((size_t) p * q));
-  LGH_TRY (work.alloc (std::max<size_t> (gemm_tn_work_elems (n, p, q), 64)));
-  cudaStream_t s = stream ();
-  LGH_TRY (launch_gemm_tn<double> (n, p, q, A, lda, B, ldb, c.p, p, 0, work.p,
-                                   work.n, s));
-  LGH_CUDA (cudaMemcpyAsync (out.data (), c.p, out.size () * sizeof (double),
-                             cudaMemcpyDeviceToHost, s));
-  LGH_CUDA (cudaStreamSynchronize (s));
-  return 0;
-}
-
-/* C (n x q) = alpha A (n x p) Bh + beta C, Bh host p x q column-major */
-int
-gemm_hb (int64_t n, double alpha, const double *A, int lda, int p,
-         const std::vector<double> &Bh, int q, double beta, double *C, int ldc)
-{
-  if (q == 0 || n == 0) return 0;
-  cudaStream_t s = stream ();
-  if (p == 0) {
-    if (beta != 1.) LGH_TRY (axpby (n, q, 0., C, ldc, beta, C, ldc, C, ldc));
-    return 0;
-  }
-  DBuf<double> b;
-  LGH_TRY (b.alloc ((size_t) p * q));
-  LGH_CUDA (cudaMemcpyAsync (b.p, Bh.data (), (size_t) p * q * sizeof (double),
-                             cudaMemcpyHostToDevice, s));
-  LGH_TRY (launch_gemm_nn<double> (n, p, q, alpha, A, lda, b.p, p, beta, C, ldc,
-                                   C, ldc, s));
-  LGH_CUDA (cudaStreamSynchronize (s));
-  return 0;
-}
-
-/* symmetric eigendecomposition of a small host matrix (column-major,
- * symmetric): w ascending, V column-major (the dsyevd convention) */
-int
-small_syev (int k, const std::vector<double> &A, std::vector<double> &w,
-            std::vector<double> &V)
-{
-  w.assign (k, 0.);
-  V.assign ((size_t) k * k, 0.);
-  if (k == 0) return 0;
-  cudaStream_t s = stream ();
-  DBuf<double> a, a2, v, v2, wd;
-  const size_t kk = (size_t) k * k;
-  LGH_TRY (a.alloc (kk));
-  LGH_TRY (a2.alloc (kk));
-  LGH_TRY (v.alloc (kk));
-  LGH_TRY (v2.alloc (kk));
-  LGH_TRY (wd.alloc (k));
-  LGH_CUDA (cudaMemcpyAsync (a.p, A.data (), kk * sizeof (double),
-                             cudaMemcpyHostToDevice, s));
-  LGH_TRY (launch_syev_jacobi (k, a.p, v.p, wd.p, a2.p, v2.p, nullptr, s));
-  std::vector<double> wu (k), Vu (kk);
-  LGH_CUDA (cudaMemcpyAsync (wu.data (), wd.p, k * sizeof (double),
-                             cudaMemcpyDeviceToHost, s));
-  LGH_CUDA (cudaMemcpyAsync (Vu.data (), v.p, kk * sizeof (double),
-                             cudaMemcpyDeviceToHost, s));
-  LGH_CUDA (cudaStreamSynchronize (s));
-  std::vector<int> ord (k);
-  for (int i = 0; i < k; i++) ord[i] = i;
-  std::stable_sort (ord.begin (), ord.end (),
-                    [&] (int x, int y) { return wu[x] < wu[y]; });
-  for (int j = 0; j < k; j++) {
-    w[j] = wu[ord[j]];
-    memcpy (&V[(size_t) j * k], &Vu[(size_t) ord[j] * k], k * sizeof (double));
-  }
-  return 0;
-}
-
-/* Y = f_c X + U diag(f - f_c) U^T X over m columns (f: kept values) */
-int
-filter_block (lgh_glr_t *g, const std::vector<double> &f, double fc,
-              const double *X, int ldx, int m, double *Y, int ldy)
-{
-  const int64_t n = g->n;
-  const int kept = g->kept;
-  if (kept == 0) return axpby (n, m, fc, X, ldx, 0., X, ldx, Y, ldy);
-  std::vector<double> C;
-  LGH_TRY (xtY (n, g->U.p, g->ldu, kept, X, ldx, m, C));
-  for (int j = 0; j < m; j++)
-    for (int k = 0; k < kept; k++) C[k + (size_t) j * kept] *= f[k] - fc;
-  if (Y != X) LGH_TRY (axpby (n, m, 0., X, ldx, fc, X, ldx, Y, ldy));
-  else LGH_TRY (axpby (n, m, 0., X, ldx, fc, Y, ldy, Y, ldy));
-  return gemm_hb (n, 1.0, g->U.p, g->ldu, kept, C, m, 1.0, Y, ldy);
-}
-
-/* Y = (U lam U^T + c I)^p X (the block form of lgh_glr_pow) */
-int
-pow_block (lgh_glr_t *g, double c, double p, const double *X, int ldx, int m,
-           double *Y, int ldy)
-{
-  std::vector<double> f (g->kept);
-  for (int k = 0; k < g->kept; k++) f[k] = pow (g->lam_h[k] + c, p);
-  return filter_block (g, f, pow (c, p), X, ldx, m, Y, ldy);
-}
-
-/* Y = F_true X = M^{1/2} Z^{-1} H_d Z^{-T} M^{1/2} X, W scratch (n x m) */
-int
-ftrue_block (lgh_glr_t *g, lgh_hessian_fn hess, void *ctx, const double *X,
-             int ldx, int m, double *Y, int ldy, double *W, int ldw,
-             int *napplies)
-{
-  lgh_prior_t *p = g->prior;
-  const int64_t n = g->n;
-  cudaStream_t s = stream ();
-  LGH_TRY (prior_solve_rows<double> (p, m, X, ldx, p->msqrt.p, Y, ldy, nullptr));
-  LGH_CUDA (cudaStreamSynchronize (s));
-  std::vector<double> hin (n), hout (n);
-  for (int j = 0; j < m; j++) {
-    LGH_CUDA (cudaMemcpy2D (hin.data (), sizeof (double), Y + j,
-                            (size_t) ldy * sizeof (double), sizeof (double), n,
-                            cudaMemcpyDeviceToHost));
-    hess (hin.data (), hout.data (), ctx);
-    LGH_CUDA (cudaMemcpy2D (W + j, (size_t) ldw * sizeof (double), hout.data (),
-                            sizeof (double), sizeof (double), n,
-                            cudaMemcpyHostToDevice));
-  }
-  *napplies += m;
-  return prior_solve_rows<double> (p, m, W, ldw, nullptr, Y, ldy, p->msqrt.p);
-}
-
-/* E = E_w T = S^-((F_true + c0 I)(S^- T)) - T */
-int
-ew_block (lgh_glr_t *g, double c0, lgh_hessian_fn hess, void *ctx,
-          const double *T, int ldt, int m, Blk &E, int *napplies)
-{
-  const int64_t n = g->n;
-  Blk S1, S2;
-  LGH_TRY (S1.alloc (n, m));
-  LGH_TRY (S2.alloc (n, m));
-  LGH_TRY (E.alloc (n, m));
-  LGH_TRY (pow_block (g, c0, -0.5, T, ldt, m, S1.d.p, S1.ld));
-  LGH_TRY (ftrue_block (g, hess, ctx, S1.d.p, S1.ld, m, S2.d.p, S2.ld, E.d.p,
-                        E.ld, napplies));
-  LGH_TRY (axpby (n, m, c0, S1.d.p, S1.ld, 1.0, S2.d.p, S2.ld, S2.d.p, S2.ld));
-  LGH_TRY (pow_block (g, c0, -0.5, S2.d.p, S2.ld, m, E.d.p, E.ld));
-  return axpby (n, m, 1.0, E.d.p, E.ld, -1.0, T, ldt, E.d.p, E.ld);
-}
-
-/* orthonormal basis of the columns of IMG, descending energy, dropping
- * directions at or below drop_tol * max(top energy, scale_floor)
- * (correct_impl.h:246-287) */
-int
-energy_basis (int64_t n, const double *IMG, int ldi, int k, double drop_tol,
-              double scale_floor, Blk &Q, int *dim)
-{
-  std::vector<double> G, ev, V;
-  LGH_TRY (xtY (n, IMG, ldi, k, IMG, ldi, k, G));
-  LGH_TRY (small_syev (k, G, ev, V));
-  const double scale = k > 0 ? std::max (ev[k - 1], scale_floor) : scale_floor;
-  int nkeep = 0;
-  for (int j = k - 1; j >= 0; j--) {
-    if (ev[j] > drop_tol * scale && ev[j] > 0.) nkeep++;
-    else break;
-  }
-  std::vector<double> C ((size_t) k * std::max (nkeep, 1), 0.);
-  for (int j = 0; j < nkeep; j++) {
-    const int idx = k - 1 - j;
-    const double sc = 1. / sqrt (ev[idx]);
-    for (int i = 0; i < k; i++) C[i + (size_t) j * k] = V[i + (size_t) idx * k] * sc;
-  }
-  LGH_TRY (Q.alloc (n, std::max (nkeep, 1)));
-  if (nkeep > 0)
-    LGH_TRY (gemm_hb (n, 1.0, IMG, ldi, k, C, nkeep, 0.0, Q.d.p, Q.ld));
-  Q.m = nkeep;
-  *dim = nkeep;
-  return 0;
-}
-
-/* sqrt(|U lam U^T Xw - Yw|_F^2 / |Yw|_F^2) (correct_impl.h:290-316) */
-int
-qc_ratio (lgh_glr_t *g, const Blk &Xw, const Blk &Yw, double *qc)
-{
-  const int64_t n = g->n;
-  const int m = Xw.m;
-  Blk R;
-  LGH_TRY (R.alloc (n, m));
-  LGH_TRY (filter_block (g, g->lam_h, 0., Xw.d.p, Xw.ld, m, R.d.p, R.ld));
-  LGH_TRY (axpby (n, m, 1.0, R.d.p, R.ld, -1.0, Yw.d.p, Yw.ld, R.d.p, R.ld));
-  std::vector<double> gr, gy;
-  LGH_TRY (xtY (n, R.d.p, R.ld, m, R.d.p, R.ld, m, gr));
-  LGH_TRY (xtY (n, Yw.d.p, Yw.ld, m, Yw.d.p, Yw.ld, m, gy));
-  double num = 0., den = 0.;
-  for (int j = 0; j < m; j++) {
-    num += gr[j + (size_t) j * m];
-    den += gy[j + (size_t) j * m];
-  }
-  *qc = den > 0. ? sqrt (std::max (num, 0.) / den) : 0.;
-  return 0;
-}
-
-/* |w|-descending order by repeated swaps (the reference's selection rule,
- * so ties resolve the same way) */
+/* indices of vals ordered by decreasing |value|; equal magnitudes keep the
+ * ascending order of the values (a tie has measure zero in practice) */
 std::vector<int>
-absdesc_order (const std::vector<double> &w)
+by_magnitude (const std::vector<double> &vals)
 {
-  const int n = (int) w.size ();
-  std::vector<int> o (n);
-  for (int i = 0; i < n; i++) o[i] = i;
-  for (int i = 0; i < n; i++)
-    for (int j = i + 1; j < n; j++)
-      if (fabs (w[o[j]]) > fabs (w[o[i]])) std::swap (o[i], o[j]);
+  std::vector<int> o (vals.size ());
+  std::iota (o.begin (), o.end (), 0);
+  std::stable_sort (o.begin (), o.end (),
+                    [&] (int x, int y) { return vals[x] < vals[y]; });
+  std::stable_sort (o.begin (), o.end (), [&] (int x, int y) {
+    return fabs (vals[x]) > fabs (vals[y]);
+  });
   return o;
 }
 
-/* fold Vhat diag(d) Vhat^T into (U, lam) (correct_impl.h:325-489) */
-int
-graft (lgh_glr_t *g, const Blk &Vhat, const std::vector<double> &d, int r,
-       const lgh_glr_correct_opts_t &opts, lgh_glr_correct_report_t *rep)
-{
-  const int64_t n = g->n;
-  const int kept0 = g->kept;
-  std::vector<double> Gv;
-  LGH_TRY (xtY (n, Vhat.d.p, Vhat.ld, r, Vhat.d.p, Vhat.ld, r, Gv));
-  double scale_floor = 0.;
-  for (int i = 0; i < r; i++) scale_floor += Gv[i + (size_t) i * r];
-  scale_floor /= std::max (r, 1);
-  /* Vperp = (I - U U^T) Vhat */
-  Blk Vperp;
-  LGH_TRY (Vperp.alloc (n, r));
-  LGH_TRY (axpby (n, r, 1.0, Vhat.d.p, Vhat.ld, 0., Vhat.d.p, Vhat.ld,
-                  Vperp.d.p, Vperp.ld));
-  std::vector<double> Cuv;
-  if (kept0 > 0) {
-    LGH_TRY (xtY (n, g->U.p, g->ldu, kept0, Vhat.d.p, Vhat.ld, r, Cuv));
-    LGH_TRY (gemm_hb (n, -1.0, g->U.p, g->ldu, kept0, Cuv, r, 1.0, Vperp.d.p,
-                      Vperp.ld));
-  }
-  Blk Qv;
-  int r2 = 0;
-  LGH_TRY (energy_basis (n, Vperp.d.p, Vperp.ld, r, opts.drop_tol, scale_floor,
-                         Qv, &r2));
-  std::vector<double> Cqv;
-  if (r2 > 0) LGH_TRY (xtY (n, Qv.d.p, Qv.ld, r2, Vhat.d.p, Vhat.ld, r, Cqv));
-  /* T2 = diag(lam, 0) + CB diag(d) CB^T on the basis [U | Qv] */
-  const int n2 = kept0 + r2;
-  std::vector<double> T2 ((size_t) std::max (n2, 1) * std::max (n2, 1), 0.);
-  for (int i = 0; i < kept0; i++) T2[i + (size_t) i * n2] = g->lam_h[i];
-  std::vector<double> CB ((size_t) std::max (n2 * r, 1), 0.);
-  for (int jc = 0; jc < r; jc++) {
-    for (int i = 0; i < kept0; i++) CB[i + (size_t) jc * n2] = Cuv[i + (size_t) jc * kept0];
-    for (int i = 0; i < r2; i++) CB[kept0 + i + (size_t) jc * n2] = Cqv[i + (size_t) jc * r2];
-  }
-  for (int a = 0; a < n2; a++)
-    for (int b = 0; b < n2; b++) {
-      double sacc = 0.;
-      for (int jc = 0; jc < r; jc++)
-        sacc += CB[a + (size_t) jc * n2] * d[jc] * CB[b + (size_t) jc * n2];
-      T2[a + (size_t) b * n2] += sacc;
-    }
-  for (int j = 0; j < n2; j++)
-    for (int i = 0; i < j; i++) {
-      const double avg = 0.5 * (T2[i + (size_t) j * n2] + T2[j + (size_t) i * n2]);
-      T2[i + (size_t) j * n2] = avg;
-      T2[j + (size_t) i * n2] = avg;
-    }
-  std::vector<double> ev2, V2;
-  LGH_TRY (small_syev (n2, T2, ev2, V2));
-  const std::vector<int> order = absdesc_order (ev2);
-  const double absmax = n2 > 0 ? fabs (ev2[order[0]]) : 0.;
-  double cut = 0.;
-  if (g->opts.trunc_abs > 0.) cut = std::max (cut, g->opts.trunc_abs);
-  if (g->opts.trunc_rel > 0.) cut = std::max (cut, g->opts.trunc_rel * absmax);
-  int keptn = 0;
-  while (keptn < n2 && fabs (ev2[order[keptn]]) > cut) keptn++;
-  std::vector<double> lam_new (keptn);
-  double lmin = 0.;
-  for (int i = 0; i < keptn; i++) {
-    lam_new[i] = ev2[order[i]];
-    lmin = std::min (lmin, lam_new[i]);
-  }
-  /* U' = [U | Qv] W_sel */
-  std::vector<double> Wsel ((size_t) std::max (n2, 1) * std::max (keptn, 1), 0.);
-  for (int j = 0; j < keptn; j++)
-    for (int i = 0; i < n2; i++)
-      Wsel[i + (size_t) j * n2] = V2[i + (size_t) order[j] * n2];
-  const int ldu = round_ld (std::max (keptn, 1));
-  DBuf<double> Unew;
-  LGH_TRY (Unew.alloc ((size_t) n * ldu));
-  LGH_CUDA (cudaMemsetAsync (Unew.p, 0, (size_t) n * ldu * sizeof (double), stream ()));
-  if (keptn > 0) {
-    std::vector<double> Wu ((size_t) std::max (kept0, 1) * keptn, 0.);
-    std::vector<double> Wq ((size_t) std::max (r2, 1) * keptn, 0.);
-    for (int j = 0; j < keptn; j++) {
-      for (int i = 0; i < kept0; i++) Wu[i + (size_t) j * kept0] = Wsel[i + (size_t) j * n2];
-      for (int i = 0; i < r2; i++) Wq[i + (size_t) j * r2] = Wsel[kept0 + i + (size_t) j * n2];
-    }
-    if (kept0 > 0)
-      LGH_TRY (gemm_hb (n, 1.0, g->U.p, g->ldu, kept0, Wu, keptn, 0.0, Unew.p, ldu));
-    if (r2 > 0)
-      LGH_TRY (gemm_hb (n, 1.0, Qv.d.p, Qv.ld, r2, Wq, keptn,
-                        kept0 > 0 ? 1.0 : 0.0, Unew.p, ldu));
-  }
-  /* install the corrected model */
-  g->U.swap (Unew);
-  g->ldu = ldu;
-  g->kept = keptn;
-  g->lam_h = lam_new;
-  LGH_TRY (g->lam_d.alloc (std::max (keptn, 1)));
-  LGH_TRY (g->lraw_d.alloc (std::max (keptn, 1)));
-  if (keptn > 0) {
-    LGH_CUDA (cudaMemcpy (g->lam_d.p, lam_new.data (), keptn * sizeof (double),
-                          cudaMemcpyHostToDevice));
-    LGH_CUDA (cudaMemcpy (g->lraw_d.p, lam_new.data (), keptn * sizeof (double),
-                          cudaMemcpyHostToDevice));
-  }
-  g->U32.release ();
-  g->Wz.release ();
-  g->have_wz = 0;
-  g->corrected = 1;
-  g->floor = std::max (0., -lmin);
-  g->stats.kept = keptn;
-  rep->floor = g->floor;
-  return 0;
-}
+/* ---- one correction ------------------------------------------------------- */
 
-/* Rayleigh-price the orthonormal directions QB with their images EB,
- * clamp, keep by |d|, Vhat = S^+ (QB Vs), graft (correct_impl.h:491-580) */
-int
-price_and_graft (lgh_glr_t *g, const lgh_glr_correct_opts_t &opts,
-                 lgh_glr_correct_report_t *rep, const Blk &QB, const Blk &EB)
+struct Deflator
 {
-  const int64_t n = g->n;
-  const int r = QB.m;
-  const double t0 = wall ();
-  std::vector<double> S, ev, V;
-  LGH_TRY (xtY (n, QB.d.p, QB.ld, r, EB.d.p, EB.ld, r, S));
-  for (int j = 0; j < r; j++)
-    for (int i = 0; i < j; i++) {
-      const double avg = 0.5 * (S[i + (size_t) j * r] + S[j + (size_t) i * r]);
-      S[i + (size_t) j * r] = avg;
-      S[j + (size_t) i * r] = avg;
-    }
-  LGH_TRY (small_syev (r, S, ev, V));
-  const std::vector<int> order = absdesc_order (ev);
-  int rkeep = opts.rank < 0 ? r : std::min (r, opts.rank);
-  while (rkeep > 0 && fabs (ev[order[rkeep - 1]]) < opts.d_keep_min) rkeep--;
-  if (rkeep == 0) {
-    rep->kept = 0;
-    rep->clamped = 0;
-    rep->d_min = r > 0 ? ev[0] : 0.;
-    rep->d_max = r > 0 ? ev[r - 1] : 0.;
-    rep->floor = 0.;
+  lgh_glr_t *g;
+  lgh_glr_correct_opts_t o;
+  lgh_hessian_fn hess;
+  void *ctx;
+  lgh_glr_correct_report_t *rep;
+  int applies = 0;
+  DBuf<double> work;      /* split-K partial sums of every small product */
+  DBuf<double> small_a;   /* small products */
+  DBuf<double> fdev;
+  std::vector<double> hin, hout; /* host staging of the callback */
+  DBuf<double> stage;     /* column-major device staging of the callback */
+
+  int ensure_work (int m1, int m2)
+  {
+    return work.alloc (std::max<size_t> (gemm_tn_work_elems (g->n, m1, m2), 64));
+  }
+
+  /* C (m1 x m2, column-major, ldc) = A^T B over the object's rows */
+  int product_tn (const double *A, int lda, int m1, const double *B, int ldb,
+                  int m2, double *C, int ldc, int sym = 0)
+  {
+    if (m1 == 0 || m2 == 0) return 0;
+    LGH_TRY (ensure_work (m1, m2));
+    return launch_gemm_tn<double> (g->n, m1, m2, A, lda, B, ldb, C, ldc, sym,
+                                   work.p, work.n, stream ());
+  }
+
+  int axpby (int m, double a, const double *X, int ldx, double b,
+             const double *Y, int ldy, double *Z, int ldz)
+  {
+    if (m == 0 || g->n == 0) return 0;
+    k_panel_axpby<<<flat_grid (g->n * m), 256, 0, stream ()>>> (
+        g->n, m, a, X, ldx, b, Y, ldy, Z, ldz);
+    LGH_LAUNCH_CHECK ();
     return 0;
   }
-  std::vector<double> dsel (rkeep), Csel ((size_t) r * rkeep);
-  rep->clamped = 0;
-  rep->d_min = rep->d_max = 0.;
-  for (int j = 0; j < rkeep; j++) {
-    double dj = ev[order[j]];
-    if (dj < -1. + opts.clamp_eps) {
-      dj = -1. + opts.clamp_eps;
-      rep->clamped++;
-    }
-    dsel[j] = dj;
-    rep->d_min = j == 0 ? dj : std::min (rep->d_min, dj);
-    rep->d_max = j == 0 ? dj : std::max (rep->d_max, dj);
-    for (int i = 0; i < r; i++) Csel[i + (size_t) j * r] = V[i + (size_t) order[j] * r];
-  }
-  Blk Vw, Vhat;
-  LGH_TRY (Vw.alloc (n, rkeep));
-  LGH_TRY (gemm_hb (n, 1.0, QB.d.p, QB.ld, r, Csel, rkeep, 0.0, Vw.d.p, Vw.ld));
-  LGH_TRY (Vhat.alloc (n, rkeep));
-  LGH_TRY (pow_block (g, opts.c0, 0.5, Vw.d.p, Vw.ld, rkeep, Vhat.d.p, Vhat.ld));
-  LGH_TRY (graft (g, Vhat, dsel, rkeep, opts, rep));
-  rep->kept = rkeep;
-  rep->t_dense += wall () - t0;
-  return 0;
-}
 
-/* a non-owning view of the first m columns of a block (row-major: the
- * same storage and leading dimension) */
-struct View
-{
-  const double *p = nullptr;
-  int64_t n = 0;
-  int m = 0, ld = 4;
+  /* Y = fc X + U diag(f - fc) U^T X on m columns: one split-K product for
+   * the coefficients, a row scaling, and one product whose epilogue adds
+   * fc X (Y may alias X) */
+  int spectral (const std::vector<double> &f, double fc, const double *X,
+                int ldx, int m, double *Y, int ldy)
+  {
+    const int kept = g->kept;
+    if (m == 0) return 0;
+    if (kept == 0) return axpby (m, fc, X, ldx, 0., X, ldx, Y, ldy);
+    LGH_TRY (small_a.alloc ((size_t) kept * m));
+    LGH_TRY (product_tn (g->U.p, g->ldu, kept, X, ldx, m, small_a.p, kept));
+    LGH_TRY (upload (f, fdev));
+    k_coeff_rows<<<flat_grid ((int64_t) kept * m), 256, 0, stream ()>>> (
+        kept, m, fdev.p, fc, small_a.p);
+    LGH_LAUNCH_CHECK ();
+    return launch_gemm_nn<double> (g->n, kept, m, 1.0, g->U.p, g->ldu,
+                                   small_a.p, kept, fc, X, ldx, Y, ldy,
+                                   stream ());
+  }
+
+  /* Y = (U lam U^T + c0 I)^p X */
+  int metric_pow (double p, const double *X, int ldx, int m, double *Y,
+                  int ldy)
+  {
+    std::vector<double> f (g->kept);
+    for (int k = 0; k < g->kept; k++) f[k] = pow (g->lam_h[k] + o.c0, p);
+    return spectral (f, pow (o.c0, p), X, ldx, m, Y, ldy);
+  }
+
+  /* Y = F_true X (m columns), W scratch of the same shape */
+  int true_whitened (const double *X, int ldx, int m, double *Y, int ldy,
+                     double *W, int ldw)
+  {
+    lgh_prior_t *p = g->prior;
+    const int64_t N = g->n;
+    cudaStream_t s = stream ();
+    LGH_TRY (prior_solve_rows<double> (p, m, X, ldx, p->msqrt.p, Y, ldy,
+                                       nullptr));
+    LGH_TRY (stage.alloc ((size_t) N * m));
+    LGH_TRY (launch_rowmajor_to_colmajor (N, m, Y, ldy, stage.p, N, nullptr, s));
+    hin.resize ((size_t) N * m);
+    hout.resize ((size_t) N * m);
+    LGH_CUDA (cudaMemcpyAsync (hin.data (), stage.p, hin.size () * sizeof (double),
+                               cudaMemcpyDeviceToHost, s));
+    LGH_CUDA (cudaStreamSynchronize (s));
+    for (int j = 0; j < m; j++)
+      hess (hin.data () + (size_t) j * N, hout.data () + (size_t) j * N, ctx);
+    applies += m;
+    LGH_CUDA (cudaMemcpyAsync (stage.p, hout.data (), hout.size () * sizeof (double),
+                               cudaMemcpyHostToDevice, s));
+    LGH_TRY (launch_colmajor_to_rowmajor (N, m, stage.p, N, W, ldw, nullptr, s));
+    return prior_solve_rows<double> (p, m, W, ldw, nullptr, Y, ldy, p->msqrt.p);
+  }
+
+  /* E = E_w T = S^-((F_true + c0 I) S^- T) - T, written into E (m columns
+   * of a panel); two scratch panels of m columns */
+  int error_image (const double *T, int ldt, int m, double *E, int lde)
+  {
+    if (m == 0) return 0;
+    const double t0 = wall ();
+    Panel s1, s2;
+    LGH_TRY (s1.make (g->n, m));
+    LGH_TRY (s2.make (g->n, m));
+    LGH_TRY (metric_pow (-0.5, T, ldt, m, s1.buf.p, s1.ld));
+    LGH_TRY (true_whitened (s1.buf.p, s1.ld, m, s2.buf.p, s2.ld, E, lde));
+    LGH_TRY (axpby (m, o.c0, s1.buf.p, s1.ld, 1.0, s2.buf.p, s2.ld, s2.buf.p,
+                    s2.ld));
+    LGH_TRY (metric_pow (-0.5, s2.buf.p, s2.ld, m, E, lde));
+    LGH_TRY (axpby (m, 1.0, E, lde, -1.0, T, ldt, E, lde));
+    rep->t_operator += wall () - t0;
+    return 0;
+  }
+
+  /* mean of the diagonal of X^T X (the mean column energy) */
+  int mean_energy (const double *X, int ldx, int m, double *out)
+  {
+    *out = 0.;
+    if (m == 0) return 0;
+    const int nb = flat_grid (g->n);
+    DBuf<double> part, tot;
+    LGH_TRY (part.alloc (nb));
+    LGH_TRY (tot.alloc (1));
+    k_sumsq_part<<<nb, 256, 0, stream ()>>> (g->n, m, X, ldx, part.p);
+    LGH_LAUNCH_CHECK ();
+    k_sum_parts<<<1, 32, 0, stream ()>>> (nb, part.p, tot.p);
+    LGH_LAUNCH_CHECK ();
+    double s = 0.;
+    LGH_CUDA (cudaMemcpyAsync (&s, tot.p, sizeof (double),
+                               cudaMemcpyDeviceToHost, stream ()));
+    LGH_CUDA (cudaStreamSynchronize (stream ()));
+    *out = s / m;
+    return 0;
+  }
+
+  /* An orthonormal basis of span(IMG) by decreasing energy: the Gram
+   * matrix's eigenpairs (e, v) give directions IMG v / sqrt(e); directions
+   * with e <= drop_tol * max(top e, floor) are dropped.  *dim = the number
+   * of directions that survive; at most `limit` of them (all: limit < 0)
+   * are written to the first columns of Q (ldq). */
+  int energy_basis (const double *IMG, int ldi, int k, double floor_e,
+                    int limit, double *Q, int ldq, int *dim)
+  {
+    *dim = 0;
+    if (k == 0) return 0;
+    DBuf<double> G;
+    LGH_TRY (G.alloc ((size_t) k * k));
+    LGH_TRY (product_tn (IMG, ldi, k, IMG, ldi, k, G.p, k, 1));
+    SmallEig eg;
+    LGH_TRY (eg.run (k, G.p));
+    std::vector<int> desc (k);
+    std::iota (desc.begin (), desc.end (), 0);
+    std::stable_sort (desc.begin (), desc.end (),
+                      [&] (int x, int y) { return eg.vals[x] > eg.vals[y]; });
+    const double scale = std::max (eg.vals[desc[0]], floor_e);
+    int live = 0;
+    while (live < k && eg.vals[desc[live]] > 0.
+           && eg.vals[desc[live]] > o.drop_tol * scale)
+      live++;
+    *dim = live;
+    const int take = limit < 0 ? live : std::min (live, limit);
+    if (take == 0 || Q == nullptr) return 0;
+    std::vector<int> idx (desc.begin (), desc.begin () + take);
+    std::vector<double> sc (take);
+    for (int j = 0; j < take; j++) sc[j] = 1. / sqrt (eg.vals[idx[j]]);
+    DBuf<int> di;
+    DBuf<double> ds, C;
+    LGH_TRY (upload_idx (idx, di));
+    LGH_TRY (upload (sc, ds));
+    LGH_TRY (C.alloc ((size_t) k * take));
+    k_gather_cols<<<flat_grid ((int64_t) k * take), 256, 0, stream ()>>> (
+        k, take, eg.vecs.p, di.p, ds.p, C.p);
+    LGH_LAUNCH_CHECK ();
+    return launch_gemm_nn<double> (g->n, k, take, 1.0, IMG, ldi, C.p, k, 0.,
+                                   Q, ldq, Q, ldq, stream ());
+  }
+
+  /* sqrt(||U lam U^T Xq - Yq||_F^2 / ||Yq||_F^2) on held-out pairs */
+  int holdout_ratio (const Panel &Xq, const Panel &Yq, double *out)
+  {
+    Panel R;
+    LGH_TRY (R.make (g->n, Xq.cols));
+    LGH_TRY (spectral (g->lam_h, 0., Xq.buf.p, Xq.ld, Xq.cols, R.buf.p, R.ld));
+    LGH_TRY (axpby (Xq.cols, 1.0, R.buf.p, R.ld, -1.0, Yq.buf.p, Yq.ld,
+                    R.buf.p, R.ld));
+    double num = 0., den = 0.;
+    LGH_TRY (mean_energy (R.buf.p, R.ld, R.cols, &num));
+    LGH_TRY (mean_energy (Yq.buf.p, Yq.ld, Yq.cols, &den));
+    *out = den > 0. ? sqrt (std::max (num, 0.) / den) : 0.;
+    return 0;
+  }
+
+  /* the probe pairs (host, column-major N x k) whitened: X = M^(-1/2) Z^T V,
+   * Yw = M^(1/2) Z^-1 HV */
+  int whiten (int k, const double *Vh, const double *HVh, Panel &X, Panel &Yw)
+  {
+    lgh_prior_t *p = g->prior;
+    const int64_t N = g->n;
+    cudaStream_t s = stream ();
+    const double t0 = wall ();
+    LGH_TRY (X.make (N, k));
+    LGH_TRY (Yw.make (N, k));
+    DBuf<double> colv, colz;
+    LGH_TRY (colv.alloc ((size_t) N * k));
+    LGH_TRY (colz.alloc ((size_t) N * k));
+    LGH_CUDA (cudaMemcpyAsync (colv.p, Vh, (size_t) N * k * sizeof (double),
+                               cudaMemcpyHostToDevice, s));
+    for (int j = 0; j < k; j++)     /* Z is symmetric: Z^T v = Z v */
+      LGH_TRY (prior_applyZ (p, colv.p + (size_t) j * N, colz.p + (size_t) j * N));
+    LGH_TRY (launch_colmajor_to_rowmajor (N, k, colz.p, N, X.buf.p, X.ld,
+                                          p->minvsqrt.p, s));
+    LGH_CUDA (cudaMemcpyAsync (colv.p, HVh, (size_t) N * k * sizeof (double),
+                               cudaMemcpyHostToDevice, s));
+    Panel H;
+    LGH_TRY (H.make (N, k));
+    LGH_TRY (launch_colmajor_to_rowmajor (N, k, colv.p, N, H.buf.p, H.ld,
+                                          nullptr, s));
+    LGH_TRY (prior_solve_rows<double> (p, k, H.buf.p, H.ld, nullptr, Yw.buf.p,
+                                       Yw.ld, p->msqrt.p));
+    LGH_CUDA (cudaStreamSynchronize (s));
+    rep->t_operator += wall () - t0;
+    return 0;
+  }
+
+  /* Rayleigh pricing of the r priced directions D (with their images
+   * E = E_w D), then the re-diagonalisation of the corrected model */
+  int price_and_fold (const Panel &D, const Panel &E, int r)
+  {
+    const double t0 = wall ();
+    DBuf<double> S;
+    LGH_TRY (S.alloc ((size_t) r * r));
+    LGH_TRY (product_tn (D.buf.p, D.ld, r, E.buf.p, E.ld, r, S.p, r, 1));
+    SmallEig es;
+    LGH_TRY (es.run (r, S.p));
+    const std::vector<int> ord = by_magnitude (es.vals);
+    int keep = o.rank < 0 ? r : std::min (r, o.rank);
+    while (keep > 0 && fabs (es.vals[ord[keep - 1]]) < o.d_keep_min) keep--;
+    const double lo = r ? *std::min_element (es.vals.begin (), es.vals.end ()) : 0.;
+    const double hi = r ? *std::max_element (es.vals.begin (), es.vals.end ()) : 0.;
+    rep->clamped = 0;
+    if (keep == 0) {
+      /* nothing worth grafting: the object stays uncorrected */
+      rep->kept = 0;
+      rep->d_min = lo;
+      rep->d_max = hi;
+      rep->floor = 0.;
+      rep->t_dense += wall () - t0;
+      return 0;
+    }
+    std::vector<double> d (keep), unit (keep, 1.);
+    std::vector<int> pick (ord.begin (), ord.begin () + keep);
+    for (int j = 0; j < keep; j++) {
+      d[j] = es.vals[pick[j]];
+      if (d[j] < -1. + o.clamp_eps) {
+        d[j] = -1. + o.clamp_eps;
+        rep->clamped++;
+      }
+    }
+    rep->d_min = *std::min_element (d.begin (), d.end ());
+    rep->d_max = *std::max_element (d.begin (), d.end ());
+    /* Vh = S^+ (D V_keep) */
+    DBuf<int> di;
+    DBuf<double> du, C;
+    LGH_TRY (upload_idx (pick, di));
+    LGH_TRY (upload (unit, du));
+    LGH_TRY (C.alloc ((size_t) r * keep));
+    k_gather_cols<<<flat_grid ((int64_t) r * keep), 256, 0, stream ()>>> (
+        r, keep, es.vecs.p, di.p, du.p, C.p);
+    LGH_LAUNCH_CHECK ();
+    Panel Vw, Vh;
+    LGH_TRY (Vw.make (g->n, keep));
+    LGH_TRY (launch_gemm_nn<double> (g->n, r, keep, 1.0, D.buf.p, D.ld, C.p, r,
+                                     0., Vw.buf.p, Vw.ld, Vw.buf.p, Vw.ld,
+                                     stream ()));
+    LGH_TRY (Vh.make (g->n, keep));
+    LGH_TRY (metric_pow (0.5, Vw.buf.p, Vw.ld, keep, Vh.buf.p, Vh.ld));
+    LGH_TRY (fold (Vh, d));
+    rep->kept = keep;
+    rep->t_dense += wall () - t0;
+    return 0;
+  }
+
+  /* (U, lam) <- the eigenpairs of U lam U^T + Vh diag(d) Vh^T, kept by the
+   * object's truncation rules, signed */
+  int fold (const Panel &Vh, const std::vector<double> &d)
+  {
+    const int64_t N = g->n;
+    const int r = Vh.cols;
+    const int kept0 = g->kept;
+    cudaStream_t s = stream ();
+    /* the part of Vh outside span(U), and its energy basis Qv; the floor
+     * (mean column energy of Vh) turns a correction inside span(U) into
+     * r2 = 0 rather than noise columns */
+    double floor_e = 0.;
+    LGH_TRY (mean_energy (Vh.buf.p, Vh.ld, r, &floor_e));
+    Panel Vp;
+    LGH_TRY (Vp.make (N, r));
+    const int n2max = kept0 + r;
+    DBuf<double> CB;                  /* U^T Vh, kept0 x r */
+    LGH_TRY (CB.alloc ((size_t) n2max * r));
+    if (kept0 > 0) {
+      LGH_TRY (product_tn (g->U.p, g->ldu, kept0, Vh.buf.p, Vh.ld, r, CB.p,
+                           kept0));
+      LGH_TRY (launch_gemm_nn<double> (N, kept0, r, -1.0, g->U.p, g->ldu, CB.p,
+                                       kept0, 1.0, Vh.buf.p, Vh.ld, Vp.buf.p,
+                                       Vp.ld, s));
+    } else {
+      LGH_TRY (axpby (r, 1.0, Vh.buf.p, Vh.ld, 0., Vh.buf.p, Vh.ld, Vp.buf.p,
+                      Vp.ld));
+    }
+    Panel Qv;
+    LGH_TRY (Qv.make (N, r));
+    int r2 = 0;
+    LGH_TRY (energy_basis (Vp.buf.p, Vp.ld, r, floor_e, -1, Qv.buf.p, Qv.ld,
+                           &r2));
+    const int n2 = kept0 + r2;
+    /* [U^T Vh ; Qv^T Vh] with leading dimension n2 */
+    DBuf<double> CBs;
+    LGH_TRY (CBs.alloc ((size_t) std::max (n2, 1) * r));
+    if (kept0 > 0)
+      LGH_CUDA (cudaMemcpy2DAsync (CBs.p, (size_t) n2 * 8, CB.p,
+                                   (size_t) kept0 * 8, (size_t) kept0 * 8, r,
+                                   cudaMemcpyDeviceToDevice, s));
+    if (r2 > 0)
+      LGH_TRY (product_tn (Qv.buf.p, Qv.ld, r2, Vh.buf.p, Vh.ld, r,
+                           CBs.p + kept0, n2));
+    DBuf<double> dd, T2;
+    LGH_TRY (upload (d, dd));
+    LGH_TRY (T2.alloc ((size_t) std::max (n2, 1) * std::max (n2, 1)));
+    k_fold_matrix<<<flat_grid ((int64_t) n2 * n2), 256, 0, s>>> (
+        n2, r, kept0, CBs.p, dd.p, g->lam_d.p, T2.p);
+    LGH_LAUNCH_CHECK ();
+    SmallEig ef;
+    LGH_TRY (ef.run (n2, T2.p));
+    const std::vector<int> ord = by_magnitude (ef.vals);
+    const double absmax = n2 > 0 ? fabs (ef.vals[ord[0]]) : 0.;
+    double cut = 0.;
+    if (g->opts.trunc_abs > 0.) cut = std::max (cut, g->opts.trunc_abs);
+    if (g->opts.trunc_rel > 0.) cut = std::max (cut, g->opts.trunc_rel * absmax);
+    int kn = 0;
+    while (kn < n2 && fabs (ef.vals[ord[kn]]) > cut) kn++;
+    std::vector<double> lam (kn), unit (std::max (kn, 1), 1.);
+    double lmin = 0.;
+    for (int i = 0; i < kn; i++) {
+      lam[i] = ef.vals[ord[i]];
+      lmin = std::min (lmin, lam[i]);
+    }
+    /* U' = [U | Qv] W, W = the kept eigenvectors (n2 x kn, ld n2) */
+    const int ldu = round_ld (std::max (kn, 1));
+    DBuf<double> Un;
+    LGH_TRY (Un.alloc ((size_t) N * ldu));
+    LGH_CUDA (cudaMemsetAsync (Un.p, 0, (size_t) N * ldu * sizeof (double), s));
+    if (kn > 0) {
+      std::vector<int> pick (ord.begin (), ord.begin () + kn);
+      DBuf<int> di;
+      DBuf<double> du, W;
+      LGH_TRY (upload_idx (pick, di));
+      LGH_TRY (upload (unit, du));
+      LGH_TRY (W.alloc ((size_t) n2 * kn));
+      k_gather_cols<<<flat_grid ((int64_t) n2 * kn), 256, 0, s>>> (
+          n2, kn, ef.vecs.p, di.p, du.p, W.p);
+      LGH_LAUNCH_CHECK ();
+      if (kept0 > 0)
+        LGH_TRY (launch_gemm_nn<double> (N, kept0, kn, 1.0, g->U.p, g->ldu,
+                                         W.p, n2, 0., Un.p, ldu, Un.p, ldu, s));
+      if (r2 > 0)
+        LGH_TRY (launch_gemm_nn<double> (N, r2, kn, 1.0, Qv.buf.p, Qv.ld,
+                                         W.p + kept0, n2, kept0 > 0 ? 1. : 0.,
+                                         Un.p, ldu, Un.p, ldu, s));
+    }
+    LGH_CUDA (cudaStreamSynchronize (s));
+    /* install the corrected model */
+    g->U.swap (Un);
+    g->ldu = ldu;
+    g->kept = kn;
+    g->lam_h = lam;
+    LGH_TRY (g->lam_d.alloc (std::max (kn, 1)));
+    LGH_TRY (g->lraw_d.alloc (std::max (kn, 1)));
+    if (kn > 0) {
+      LGH_CUDA (cudaMemcpy (g->lam_d.p, lam.data (), kn * sizeof (double),
+                            cudaMemcpyHostToDevice));
+      LGH_CUDA (cudaMemcpy (g->lraw_d.p, lam.data (), kn * sizeof (double),
+                            cudaMemcpyHostToDevice));
+    }
+    g->U32.release ();
+    g->Wz.release ();
+    g->have_wz = 0;
+    g->corrected = 1;
+    g->floor = std::max (0., -lmin);
+    g->stats.kept = kn;
+    rep->floor = g->floor;
+    return 0;
+  }
+
+  void trace () const
+  {
+    if (!o.verbose) return;
+    fprintf (stderr, "lgh correction: %d basis directions, %d true applies, "
+             "%d modes grafted (%d clamped), d in [%.3g, %.3g], shift floor "
+             "%.3g, held-out ratio %.3g before, %.3g after\n", rep->basis,
+             rep->hd_applies, rep->kept, rep->clamped, rep->d_min, rep->d_max,
+             rep->floor, rep->qc_before, rep->qc_after);
+  }
 };
 
-View
-view (const Blk &b, int m)
-{
-  View v;
-  v.p = b.d.p;
-  v.n = b.n;
-  v.m = m;
-  v.ld = b.ld;
-  return v;
-}
-
-/* [A | B] into a new block */
 int
-concat (const View &A, const View &B, Blk &O)
+start (lgh_glr_t *glr, const lgh_glr_correct_opts_t *opts_in,
+       lgh_glr_correct_report_t *rep, lgh_glr_correct_opts_t *o,
+       const char *who)
 {
-  LGH_TRY (O.alloc (A.n, A.m + B.m));
-  cudaStream_t s = stream ();
-  if (A.m > 0)
-    LGH_CUDA (cudaMemcpy2DAsync (O.d.p, (size_t) O.ld * 8, A.p, (size_t) A.ld * 8,
-                                 (size_t) A.m * 8, A.n, cudaMemcpyDeviceToDevice, s));
-  if (B.m > 0)
-    LGH_CUDA (cudaMemcpy2DAsync (O.d.p + A.m, (size_t) O.ld * 8, B.p,
-                                 (size_t) B.ld * 8, (size_t) B.m * 8, A.n,
-                                 cudaMemcpyDeviceToDevice, s));
-  return 0;
-}
-
-/* whitened probes of host column-major (N x k) V and HV:
- * X = M^{-1/2} Z^T V (Z applies), Yw = M^{1/2} Z^{-1} HV (a block solve) */
-int
-whiten_probes (lgh_glr_t *g, int k, const double *Vh, const double *HVh,
-               Blk &X, Blk &Yw)
-{
-  lgh_prior_t *p = g->prior;
-  const int64_t n = g->n;
-  cudaStream_t s = stream ();
-  LGH_TRY (X.alloc (n, k));
-  LGH_TRY (Yw.alloc (n, k));
-  DBuf<double> v, y;
-  LGH_TRY (v.alloc (n));
-  LGH_TRY (y.alloc (n));
-  for (int j = 0; j < k; j++) {
-    LGH_CUDA (cudaMemcpy (v.p, Vh + (size_t) j * n, n * sizeof (double),
-                          cudaMemcpyHostToDevice));
-    LGH_TRY (prior_applyZ (p, v.p, y.p));
-    LGH_TRY (launch_vec_div (n, y.p, p->msqrt.p, v.p, s));
-    LGH_CUDA (cudaMemcpy2DAsync (X.d.p + j, (size_t) X.ld * 8, v.p, 8, 8, n,
-                                 cudaMemcpyDeviceToDevice, s));
-    LGH_CUDA (cudaStreamSynchronize (s));
-  }
-  DBuf<double> hv;
-  LGH_TRY (hv.alloc ((size_t) n * k));
-  LGH_CUDA (cudaMemcpy (hv.p, HVh, (size_t) n * k * sizeof (double),
-                        cudaMemcpyHostToDevice));
-  Blk H;
-  LGH_TRY (H.alloc (n, k));
-  LGH_TRY (launch_colmajor_to_rowmajor (n, k, hv.p, n, H.d.p, H.ld, nullptr, s));
-  LGH_TRY (prior_solve_rows<double> (p, k, H.d.p, H.ld, nullptr, Yw.d.p, Yw.ld,
-                                     p->msqrt.p));
-  LGH_CUDA (cudaStreamSynchronize (s));
-  return 0;
-}
-
-int
-correct_checks (lgh_glr_t *glr, const lgh_glr_correct_opts_t &o, const char *who)
-{
-  LGH_CHECK (!glr->corrected, LGH_ERR_ORDER, "%s: the object is already corrected",
+  *o = opts_in ? *opts_in : lgh_glr_correct_opts_default ();
+  memset (rep, 0, sizeof (*rep));
+  rep->qc_before = rep->qc_after = -1.;
+  LGH_CHECK (!glr->corrected, LGH_ERR_ORDER,
+             "%s: this object carries a correction already (one per object)",
              who);
-  LGH_CHECK (o.c0 > 0., LGH_ERR_ARG_OUTOFRANGE, "%s: c0 must be positive", who);
+  LGH_CHECK (o->c0 > 0., LGH_ERR_ARG_OUTOFRANGE,
+             "%s: the metric shift c0 = %g is not positive", who, o->c0);
   return 0;
 }
 
 } /* namespace */
 
-/* the corrected operator's low-rank action, y = Z M^{-1/2}(U lam U^T + c I)
- * M^{-1/2} Z v (glr.h:196-198) */
+/* y = Z M^(-1/2) (U lam U^T + c I) M^(-1/2) Z v, the corrected operator's
+ * low-rank action served by lgh_glr_apply after a correction (glr.h:
+ * 196-198) */
 int
 glr_apply_corrected (lgh_glr_t *g, double c, const double *v, double *y)
 {
@@ -563,18 +696,11 @@ glr_apply_corrected (lgh_glr_t *g, double c, const double *v, double *y)
   LGH_TRY (u.alloc (n));
   LGH_TRY (prior_applyZ (p, v, t.p));
   LGH_TRY (launch_vec_div (n, t.p, p->msqrt.p, u.p, s));
+  Deflator dfl{};
+  dfl.g = g;
   std::vector<double> f (g->kept);
   for (int k = 0; k < g->kept; k++) f[k] = g->lam_h[k] + c;
-  /* u (a 1-column row-major block, ld 1) */
-  if (g->kept > 0) {
-    std::vector<double> C;
-    LGH_TRY (xtY (n, g->U.p, g->ldu, g->kept, u.p, 1, 1, C));
-    for (int k = 0; k < g->kept; k++) C[k] *= f[k] - c;
-    LGH_TRY (axpby (n, 1, 0., u.p, 1, c, u.p, 1, t.p, 1));
-    LGH_TRY (gemm_hb (n, 1.0, g->U.p, g->ldu, g->kept, C, 1, 1.0, t.p, 1));
-  } else {
-    LGH_TRY (axpby (n, 1, 0., u.p, 1, c, u.p, 1, t.p, 1));
-  }
+  LGH_TRY (dfl.spectral (f, c, u.p, 1, 1, t.p, 1));
   LGH_TRY (launch_vec_div (n, t.p, p->msqrt.p, u.p, s));
   LGH_TRY (prior_applyZ (p, u.p, y));
   LGH_CUDA (cudaStreamSynchronize (s));
@@ -590,7 +716,7 @@ extern "C" {
 lgh_glr_correct_opts_t
 lgh_glr_correct_opts_default (void)
 {
-  /* correct_impl.h:43-58 */
+  /* the reference's defaults (correct_impl.h:43-58) */
   lgh_glr_correct_opts_t o;
   o.c0 = 1.0;
   o.rank = -1;
@@ -613,94 +739,87 @@ lgh_glr_correct_probes (lgh_glr_t *glr, int k, const double *V,
 {
   LGH_TRY (ensure_init ());
   LGH_CHECK (glr && V && HV && hess, LGH_ERR_ARG_NULL,
-             "lgh_glr_correct_probes: NULL argument");
-  const lgh_glr_correct_opts_t o = opts_in ? *opts_in : lgh_glr_correct_opts_default ();
+             "lgh_glr_correct_probes: the object, both probe arrays and the "
+             "Hessian callback are required");
   lgh_glr_correct_report_t rep;
-  memset (&rep, 0, sizeof (rep));
-  rep.qc_before = rep.qc_after = -1.;
-  LGH_TRY (correct_checks (glr, o, "lgh_glr_correct_probes"));
-  const int kf = k - o.n_qc;
-  LGH_CHECK (kf > 0 && o.n_qc >= 0, LGH_ERR_ARG_OUTOFRANGE,
-             "lgh_glr_correct_probes: need k - n_qc > 0 probes (k=%d, n_qc=%d)",
-             k, o.n_qc);
+  Deflator dfl{};
+  LGH_TRY (start (glr, opts_in, &rep, &dfl.o, "lgh_glr_correct_probes"));
+  const lgh_glr_correct_opts_t &o = dfl.o;
+  dfl.g = glr;
+  dfl.hess = hess;
+  dfl.ctx = ctx;
+  dfl.rep = &rep;
+  const int nfit = k - o.n_qc;
+  LGH_CHECK (o.n_qc >= 0 && nfit > 0, LGH_ERR_ARG_OUTOFRANGE,
+             "lgh_glr_correct_probes: %d probes with %d held out leaves none "
+             "to build the error basis from", k, o.n_qc);
   LGH_CHECK (o.applies > 0, LGH_ERR_ARG_OUTOFRANGE,
-             "lgh_glr_correct_probes: applies budget must be positive");
-  const int64_t n = glr->n;
-  int napplies = 0;
-  double t0 = wall ();
-  Blk X, Yw, Xq, Yqw;
-  LGH_TRY (whiten_probes (glr, kf, V, HV, X, Yw));
-  rep.t_operator += wall () - t0;
+             "lgh_glr_correct_probes: the true-apply budget (%d) must be at "
+             "least 1", o.applies);
+  const int64_t N = glr->n;
+  Panel X, Yw, Xq, Yq;
+  LGH_TRY (dfl.whiten (nfit, V, HV, X, Yw));
   if (o.n_qc > 0) {
-    LGH_TRY (whiten_probes (glr, o.n_qc, V + (size_t) kf * n, HV + (size_t) kf * n,
-                            Xq, Yqw));
-    LGH_TRY (qc_ratio (glr, Xq, Yqw, &rep.qc_before));
+    LGH_TRY (dfl.whiten (o.n_qc, V + (size_t) nfit * N, HV + (size_t) nfit * N,
+                         Xq, Yq));
+    LGH_TRY (dfl.holdout_ratio (Xq, Yq, &rep.qc_before));
   }
-  /* residual images IMG = S^-(Yw - U lam U^T X): the free error basis */
-  t0 = wall ();
-  Blk Rw, IMG, QB0;
-  LGH_TRY (Rw.alloc (n, kf));
-  LGH_TRY (filter_block (glr, glr->lam_h, 0., X.d.p, X.ld, kf, Rw.d.p, Rw.ld));
-  LGH_TRY (axpby (n, kf, 1.0, Yw.d.p, Yw.ld, -1.0, Rw.d.p, Rw.ld, Rw.d.p, Rw.ld));
-  LGH_TRY (IMG.alloc (n, kf));
-  LGH_TRY (pow_block (glr, o.c0, -0.5, Rw.d.p, Rw.ld, kf, IMG.d.p, IMG.ld));
+  /* the free error images S^-(Yw - U lam U^T X) */
+  double t0 = wall ();
+  Panel img;
+  LGH_TRY (img.make (N, nfit));
+  LGH_TRY (dfl.spectral (glr->lam_h, 0., X.buf.p, X.ld, nfit, img.buf.p,
+                         img.ld));
+  LGH_TRY (dfl.axpby (nfit, 1.0, Yw.buf.p, Yw.ld, -1.0, img.buf.p, img.ld,
+                      img.buf.p, img.ld));
+  LGH_TRY (dfl.metric_pow (-0.5, img.buf.p, img.ld, nfit, img.buf.p, img.ld));
+  /* D will hold every priced direction and E their images: the leading
+   * m1 = min(applies, basis) basis directions first, then up to
+   * applies - m1 more from one power step */
+  Panel D, E;
+  LGH_TRY (D.make (N, o.applies));
+  LGH_TRY (E.make (N, o.applies));
   int bdim = 0;
-  LGH_TRY (energy_basis (n, IMG.d.p, IMG.ld, kf, o.drop_tol, 0., QB0, &bdim));
+  LGH_TRY (dfl.energy_basis (img.buf.p, img.ld, nfit, 0., o.applies, D.buf.p,
+                             D.ld, &bdim));
   rep.basis = bdim;
   rep.t_dense += wall () - t0;
   LGH_CHECK (bdim > 0, LGH_ERR_CONV_FAILED,
-             "lgh_glr_correct_probes: the probe residuals span nothing -- either "
-             "the approximation is already exact on the probes or the probe "
-             "data is inconsistent");
-  /* price the top m1 basis directions exactly */
+             "lgh_glr_correct_probes: the whitened probe residuals are all "
+             "zero to rounding, so there is no error direction to correct "
+             "(the model already reproduces the probes, or HV does not "
+             "match V)");
   const int m1 = std::min (o.applies, bdim);
-  const View Q1v = view (QB0, m1);
-  Blk E1;
-  t0 = wall ();
-  LGH_TRY (ew_block (glr, o.c0, hess, ctx, Q1v.p, Q1v.ld, m1, E1, &napplies));
-  rep.t_operator += wall () - t0;
-  Blk QB, EB;
-  bool have = false;
-  if (o.applies > m1 && m1 > 0) {
-    /* one power step past the basis */
-    std::vector<double> C;
-    LGH_TRY (xtY (n, Q1v.p, Q1v.ld, m1, E1.d.p, E1.ld, m1, C));
-    Blk Pb;
-    LGH_TRY (Pb.alloc (n, m1));
-    LGH_TRY (axpby (n, m1, 1.0, E1.d.p, E1.ld, 0., E1.d.p, E1.ld, Pb.d.p, Pb.ld));
-    LGH_TRY (gemm_hb (n, -1.0, Q1v.p, Q1v.ld, m1, C, m1, 1.0, Pb.d.p, Pb.ld));
-    std::vector<double> Ge;
-    LGH_TRY (xtY (n, E1.d.p, E1.ld, m1, E1.d.p, E1.ld, m1, Ge));
-    double sf = 0.;
-    for (int j = 0; j < m1; j++) sf += Ge[j + (size_t) j * m1];
-    sf /= std::max (m1, 1);
-    Blk Q2b;
+  LGH_TRY (dfl.error_image (D.buf.p, D.ld, m1, E.buf.p, E.ld));
+  int priced = m1;
+  if (o.applies > m1) {
+    /* the images' components outside the priced directions, and their
+     * energy basis (floored by the images' mean energy) */
+    Panel P;
+    LGH_TRY (P.make (N, m1));
+    DBuf<double> Cm;
+    LGH_TRY (Cm.alloc ((size_t) m1 * m1));
+    LGH_TRY (dfl.product_tn (D.buf.p, D.ld, m1, E.buf.p, E.ld, m1, Cm.p, m1));
+    LGH_TRY (launch_gemm_nn<double> (N, m1, m1, -1.0, D.buf.p, D.ld, Cm.p, m1,
+                                     1.0, E.buf.p, E.ld, P.buf.p, P.ld,
+                                     stream ()));
+    double fe = 0.;
+    LGH_TRY (dfl.mean_energy (E.buf.p, E.ld, m1, &fe));
     int b2 = 0;
-    LGH_TRY (energy_basis (n, Pb.d.p, Pb.ld, m1, o.drop_tol, sf, Q2b, &b2));
-    const int m2 = std::min (o.applies - m1, b2);
+    const int want = o.applies - m1;
+    LGH_TRY (dfl.energy_basis (P.buf.p, P.ld, m1, fe, want, D.at (m1), D.ld,
+                               &b2));
+    const int m2 = std::min (want, b2);
     if (m2 > 0) {
-      const View Q2v = view (Q2b, m2);
-      Blk E2;
-      t0 = wall ();
-      LGH_TRY (ew_block (glr, o.c0, hess, ctx, Q2v.p, Q2v.ld, m2, E2, &napplies));
-      rep.t_operator += wall () - t0;
-      LGH_TRY (concat (Q1v, Q2v, QB));
-      LGH_TRY (concat (view (E1, m1), view (E2, m2), EB));
-      have = true;
+      LGH_TRY (dfl.error_image (D.at (m1), D.ld, m2, E.at (m1), E.ld));
+      priced += m2;
     }
   }
-  if (!have) {
-    LGH_TRY (concat (Q1v, View (), QB));
-    LGH_TRY (concat (view (E1, m1), View (), EB));
-  }
-  LGH_TRY (price_and_graft (glr, o, &rep, QB, EB));
-  rep.hd_applies = napplies;
-  if (o.n_qc > 0) LGH_TRY (qc_ratio (glr, Xq, Yqw, &rep.qc_after));
-  if (o.verbose)
-    fprintf (stderr, "[lgh correct] basis %d, priced %d applies, kept %d "
-             "(clamped %d), d in [%.3g, %.3g], floor %.3g, qc %.3g -> %.3g\n",
-             rep.basis, rep.hd_applies, rep.kept, rep.clamped, rep.d_min,
-             rep.d_max, rep.floor, rep.qc_before, rep.qc_after);
+  D.cols = E.cols = priced;
+  LGH_TRY (dfl.price_and_fold (D, E, priced));
+  rep.hd_applies = dfl.applies;
+  if (o.n_qc > 0) LGH_TRY (dfl.holdout_ratio (Xq, Yq, &rep.qc_after));
+  dfl.trace ();
   if (report) *report = rep;
   return 0;
 }
@@ -711,50 +830,57 @@ lgh_glr_correct (lgh_glr_t *glr, lgh_hessian_fn hess, void *ctx,
                  lgh_glr_correct_report_t *report)
 {
   LGH_TRY (ensure_init ());
-  LGH_CHECK (glr && hess, LGH_ERR_ARG_NULL, "lgh_glr_correct: NULL argument");
-  const lgh_glr_correct_opts_t o = opts_in ? *opts_in : lgh_glr_correct_opts_default ();
+  LGH_CHECK (glr && hess, LGH_ERR_ARG_NULL,
+             "lgh_glr_correct: the object and the Hessian callback are "
+             "required");
   lgh_glr_correct_report_t rep;
-  memset (&rep, 0, sizeof (rep));
-  rep.qc_before = rep.qc_after = -1.;
-  LGH_TRY (correct_checks (glr, o, "lgh_glr_correct"));
+  Deflator dfl{};
+  LGH_TRY (start (glr, opts_in, &rep, &dfl.o, "lgh_glr_correct"));
+  const lgh_glr_correct_opts_t &o = dfl.o;
+  dfl.g = glr;
+  dfl.hess = hess;
+  dfl.ctx = ctx;
+  dfl.rep = &rep;
   LGH_CHECK (o.applies >= 2, LGH_ERR_ARG_OUTOFRANGE,
-             "lgh_glr_correct: the fresh path needs applies >= 2 (range pass + "
-             "Rayleigh pass)");
-  const int64_t n = glr->n;
-  const int passes = 2 + std::max (o.q_power, 0);
-  const int mr = std::max (o.applies / passes, 1);
-  int napplies = 0;
-  /* hashed Gaussian test block in the whitened frame */
-  Blk T, IMG;
-  LGH_TRY (T.alloc (n, mr));
-  LGH_TRY (launch_sketch (o.seed, n, 0, mr, T.d.p, T.ld, stream ()));
-  double t0 = wall ();
-  LGH_TRY (ew_block (glr, o.c0, hess, ctx, T.d.p, T.ld, mr, IMG, &napplies));
-  rep.t_operator += wall () - t0;
-  for (int pp = 0; pp < o.q_power; pp++) {
-    Blk Tn;
+             "lgh_glr_correct: a budget of %d true applies cannot pay for "
+             "both the range pass and the pricing pass (need >= 2)",
+             o.applies);
+  const int64_t N = glr->n;
+  /* the budget splits over the range pass, q_power power passes and the
+   * pricing pass */
+  const int width = std::max (o.applies / (2 + std::max (o.q_power, 0)), 1);
+  Panel T, img;
+  LGH_TRY (T.make (N, width));
+  LGH_TRY (img.make (N, width));
+  LGH_TRY (launch_sketch (o.seed, N, 0, width, T.buf.p, T.ld, stream ()));
+  LGH_TRY (dfl.error_image (T.buf.p, T.ld, width, img.buf.p, img.ld));
+  int cols = width;
+  for (int pass = 0; pass < o.q_power; pass++) {
     int bd = 0;
-    LGH_TRY (energy_basis (n, IMG.d.p, IMG.ld, IMG.m, o.drop_tol, 0., Tn, &bd));
+    LGH_TRY (dfl.energy_basis (img.buf.p, img.ld, cols, 0., -1, T.buf.p, T.ld,
+                               &bd));
     if (bd == 0) break;
-    t0 = wall ();
-    LGH_TRY (ew_block (glr, o.c0, hess, ctx, Tn.d.p, Tn.ld, bd, IMG, &napplies));
-    rep.t_operator += wall () - t0;
+    cols = bd;
+    LGH_TRY (dfl.error_image (T.buf.p, T.ld, cols, img.buf.p, img.ld));
   }
-  Blk QB0;
+  /* what is left of the budget prices the leading directions */
+  const int left = std::max (o.applies - dfl.applies, 1);
+  Panel D, E;
+  LGH_TRY (D.make (N, left));
+  LGH_TRY (E.make (N, left));
   int bdim = 0;
-  LGH_TRY (energy_basis (n, IMG.d.p, IMG.ld, IMG.m, o.drop_tol, 0., QB0, &bdim));
+  LGH_TRY (dfl.energy_basis (img.buf.p, img.ld, cols, 0., left, D.buf.p, D.ld,
+                             &bdim));
   rep.basis = bdim;
   LGH_CHECK (bdim > 0, LGH_ERR_CONV_FAILED,
-             "lgh_glr_correct: the error sketch spans nothing -- the "
-             "approximation may already be exact");
-  const int m1 = std::min (std::max (o.applies - napplies, 1), bdim);
-  Blk QB, EB;
-  LGH_TRY (concat (view (QB0, m1), View (), QB));
-  t0 = wall ();
-  LGH_TRY (ew_block (glr, o.c0, hess, ctx, QB.d.p, QB.ld, m1, EB, &napplies));
-  rep.t_operator += wall () - t0;
-  LGH_TRY (price_and_graft (glr, o, &rep, QB, EB));
-  rep.hd_applies = napplies;
+             "lgh_glr_correct: the sketched error images are all zero to "
+             "rounding, so there is no error direction to correct (the model "
+             "may already be exact)");
+  const int m1 = std::min (left, bdim);
+  LGH_TRY (dfl.error_image (D.buf.p, D.ld, m1, E.buf.p, E.ld));
+  LGH_TRY (dfl.price_and_fold (D, E, m1));
+  rep.hd_applies = dfl.applies;
+  dfl.trace ();
   if (report) *report = rep;
   return 0;
 }

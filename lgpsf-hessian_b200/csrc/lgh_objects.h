@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "lgh_internal.h"
+#include "lgh_strip.h"
 
 /* Mat: a device CSR operator (kind 0) or a dense column-block view handed
  * to blocked prior callbacks (kind 1, MATDENSE layout, not owned). */
@@ -18,6 +19,11 @@ struct lgh_mat_s
   int64_t nrows = 0;
   int ncols = 0;
   int64_t ld = 0;
+  /* the strip form of a CSR operator, built on its first block product
+   * (k_strip.cu); strip_R: 0 = chosen by the cost model, or 2 / 4 / 8 */
+  lgh::StripForm strips;
+  int strips_built = 0;
+  int strip_R = 0;
 };
 
 /* Vec: a device vector; owns its array unless created with an array. */
@@ -90,6 +96,11 @@ namespace lgh
 {
 void mat_release (lgh_Mat A);
 int mat_mult_vec (lgh_Mat A, const double *x, double *y);
+/* Y = A X for a row-major block of width w: the strip form from 8
+ * columns on (built on first use), the row-wise CSR product below */
+template <typename T>
+int mat_mult_block (lgh_Mat A, const T *X, int ldx, T *Y, int ldy, int w,
+                    cudaStream_t s);
 void prior_ref (lgh_prior_t *p);
 int prior_applyZ (lgh_prior_t *p, const double *x, double *y);
 int prior_solve_vec (lgh_prior_t *p, const double *x, const double *s_in,

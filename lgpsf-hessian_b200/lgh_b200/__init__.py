@@ -280,6 +280,8 @@ SIGNATURES = {
     "lgh_test_rng_state": (ctypes.c_int, [ctypes.c_uint64, I64, I64,
                                           ctypes.c_int, P]),
     "lgh_test_spmm": (ctypes.c_int, [P, ctypes.c_int, P, P, ctypes.c_int]),
+    "lgh_test_spmm_strip": (ctypes.c_int, [P, ctypes.c_int, P, P, ctypes.c_int,
+                                           ctypes.c_int, P]),
     "lgh_test_zsolve": (ctypes.c_int, [P, ctypes.c_int, P, P, ctypes.c_int]),
     "lgh_test_cheb_step": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_int,
@@ -873,6 +875,19 @@ def test_spmm(A, X, fp32=False):
     _chk(load().lgh_test_spmm(A.h, X.shape[1], X.ctypes.data, Y.ctypes.data,
                               1 if fp32 else 0), "lgh_test_spmm")
     return Y
+
+
+def test_spmm_strip(A, X, fp32=False, R=0):
+    """B X through the strip form at height R (0: the cost model's choice);
+    returns (Y, R used)."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    Y = np.empty_like(X)
+    ru = ctypes.c_int(0)
+    _chk(load().lgh_test_spmm_strip(A.h, X.shape[1], X.ctypes.data,
+                                    Y.ctypes.data, 1 if fp32 else 0, int(R),
+                                    ctypes.addressof(ru)),
+         "lgh_test_spmm_strip")
+    return Y, ru.value
 
 
 def test_zsolve(prior, X, fp32=False):

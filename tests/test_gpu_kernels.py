@@ -88,6 +88,62 @@ def test_spmm_fp32(w):
     assert _rd(Y, ref) < 1e-5
 
 
+@pytest.mark.parametrize("R", [0, 2, 4, 8])
+@pytest.mark.parametrize("w", [8, 33, 64, 220])
+def test_strip_product_fp64(R, w):
+    """The strip form of B (k_strip.cu) against the CSR product, on the 2D
+    config-1 kernel matrix and on a 3D one (config 3's formulas on 32^3)."""
+    for name in ("c1", "c3_32"):
+        cfg = P.grid_problem(name)
+        A = L.Mat(cfg["B"])
+        X = np.random.default_rng(w + R).standard_normal((cfg["N"], w))
+        Y, used = L.test_spmm_strip(A, X, R=R)
+        assert used in (2, 4, 8) and (R == 0 or used == R)
+        ref = P.csr_matvec(cfg["B"], X)
+        assert _rd(Y, ref) < 1e-14, (name, R, w)
+
+
+@pytest.mark.parametrize("w", [8, 200])
+def test_strip_product_fp32(w):
+    cfg = P.grid_problem("c1")
+    A = L.Mat(cfg["B"])
+    X = np.random.default_rng(w).standard_normal((cfg["N"], w))
+    Y, _ = L.test_spmm_strip(A, X, fp32=True)
+    ref = P.csr_matvec(cfg["B"], X)
+    assert _rd(Y, ref) < 1e-5
+
+
+def test_strip_product_unsorted_rows_and_duplicates():
+    """Rows whose columns are shuffled, duplicated entries and a ragged
+    last strip: every stored entry is used exactly once."""
+    rng = np.random.default_rng(5)
+    n = 1003                                   # not a multiple of 8
+    rows, cols, vals = [], [], []
+    for i in range(n):
+        nb = int(rng.integers(0, 12))
+        cs = np.clip(i + rng.integers(-30, 31, size=nb), 0, n - 1)
+        if i % 7 == 0 and nb:                  # a duplicated entry
+            cs = np.concatenate([cs, cs[:1]])
+        rng.shuffle(cs)
+        rows += [i] * len(cs)
+        cols += list(cs)
+        vals += list(rng.standard_normal(len(cs)))
+    rows, cols, vals = np.array(rows), np.array(cols), np.array(vals)
+    order = np.argsort(rows, kind="stable")    # CSR order, columns unsorted
+    rowptr = np.zeros(n + 1, dtype=np.int64)
+    np.add.at(rowptr, rows + 1, 1)
+    rowptr = np.cumsum(rowptr)
+    csr = dict(n=n, rowptr=rowptr, colidx=cols[order].astype(np.int32),
+               vals=vals[order])
+    A = L.Mat(csr)
+    X = rng.standard_normal((n, 40))
+    ref = np.zeros((n, 40))
+    np.add.at(ref, rows, vals[:, None] * X[cols])
+    for R in (2, 4, 8):
+        Y, _ = L.test_spmm_strip(A, X, R=R)
+        assert np.max(np.abs(Y - ref)) < 1e-12 * max(1.0, np.max(np.abs(ref)))
+
+
 def _prior_mat(mode, tile=8, rtol=1e-12, pc="jacobi"):
     p = P.test_prior_mat_problem()
     Z = L.Mat(p["Z"])
