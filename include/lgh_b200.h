@@ -321,7 +321,13 @@ int lgh_glr_get_U (const lgh_glr_t *glr, double *U_dev, int64_t ld);
 /* Batched downstream operations on device column blocks (column-major,
  * leading dims ldr/ldx), m right-hand sides, nshift shifts c[0..nshift):
  * output block s (columns s*m .. s*m+m-1 of x) holds the result at c[s].
- * The Z-solves, which do not depend on c, run once per right-hand side.   */
+ * The Z-solves, which do not depend on c, run once per right-hand side;
+ * with more than one shift, every shift's Woodbury combination then runs
+ * in one fused tensor-core launch that writes x directly.  That tail is
+ * captured as a CUDA graph on the first call of a (kind, nshift, m) shape
+ * and replayed afterwards; its tile shape is picked by the library's
+ * autotuner on the first call of a shape (that call times each variant
+ * once; LGH_TUNE_CACHE = a file path keeps the choices across runs).    */
 int lgh_glr_solve_batch (lgh_glr_t *glr, int nshift, const double *c,
                          int m, const double *rhs, int64_t ldr, double *x,
                          int64_t ldx);
@@ -330,6 +336,12 @@ int lgh_glr_sample_batch (lgh_glr_t *glr, int nshift, const double *c,
                           int64_t ldx);
 int lgh_glr_logdet_batch (lgh_glr_t *glr, int nshift, const double *c,
                           double *out);
+/* The batched operations' graph and tuning state (all nullable): graph
+ * captures and replays of this object, the tile variant of its last
+ * combination, and the shapes the autotuner has measured in the process. */
+int lgh_glr_batch_info (const lgh_glr_t *glr, long *graph_captures,
+                        long *graph_replays, int *tile_variant,
+                        int *tuned_shapes);
 
 /* ---- the request loop ---------------------------------------------------
  * Continuous batching of solve / sample / logdet requests on a resident GLR

@@ -651,25 +651,23 @@ batch_op (lgh_glr_t *g, int kind, int nshift, const double *c, int m,
   const bool direct = nshift == 1 && !g->have_wz && g->kept > 0;
   if (!direct) LGH_TRY (ensure_wz (g));
   const int ldm = round_ld (m), kept = g->kept;
-  DBuf<double> R, Y0, Xs, Wc, Dc, work;
-  LGH_TRY (R.alloc ((size_t) n * ldm));
-  LGH_TRY (Y0.alloc ((size_t) n * ldm));
-  LGH_TRY (Xs.alloc ((size_t) n * ldm));
-  LGH_TRY (Wc.alloc ((size_t) std::max (kept, 1) * m));
-  LGH_TRY (Dc.alloc ((size_t) std::max (kept, 1) * m));
-  LGH_TRY (work.alloc (std::max<size_t> (gemm_tn_work_elems (n, std::max (kept, 1), m), 64)));
-  LGH_TRY (launch_colmajor_to_rowmajor (n, m, rhs, ldr, R.p, ldm, nullptr, s));
   const double *ms = g->prior->msqrt.p;
-  if (kind == 0) {
-    /* r2 = M^{1/2} Z^{-1} r (into R), y0 = Z^{-1} M^{1/2} r2 */
-    LGH_TRY (glr_zsolve (g, m, R.p, ldm, nullptr, Xs.p, ldm, ms));
-    R.swap (Xs);
-  }
-  /* sample: r2 = xi */
-  if (kept > 0)
+  if (direct) {
+    DBuf<double> R, Y0, Xs, Wc, Dc, work;
+    LGH_TRY (R.alloc ((size_t) n * ldm));
+    LGH_TRY (Y0.alloc ((size_t) n * ldm));
+    LGH_TRY (Xs.alloc ((size_t) n * ldm));
+    LGH_TRY (Wc.alloc ((size_t) std::max (kept, 1) * m));
+    LGH_TRY (Dc.alloc ((size_t) std::max (kept, 1) * m));
+    LGH_TRY (work.alloc (std::max<size_t> (gemm_tn_work_elems (n, std::max (kept, 1), m), 64)));
+    LGH_TRY (launch_colmajor_to_rowmajor (n, m, rhs, ldr, R.p, ldm, nullptr, s));
+    if (kind == 0) {
+      /* r2 = M^{1/2} Z^{-1} r (into R) */
+      LGH_TRY (glr_zsolve (g, m, R.p, ldm, nullptr, Xs.p, ldm, ms));
+      R.swap (Xs);
+    }
     LGH_TRY (launch_gemm_tn<double> (n, kept, m, g->U.p, g->ldu, R.p, ldm, Wc.p,
                                      kept, 0, work.p, work.n, s));
-  if (direct) {
     /* t = f(c) r2 + U diag(f(lam + c) - f(c)) U^T r2, x = Z^{-1} M^{1/2} t */
     const double cs = ch[0];
     const double fc = (kind == 0) ? 1. / cs : 1. / sqrt (cs);
@@ -683,23 +681,48 @@ batch_op (lgh_glr_t *g, int kind, int nshift, const double *c, int m,
     LGH_CUDA (cudaStreamSynchronize (s));
     return 0;
   }
-  LGH_TRY (glr_zsolve (g, m, R.p, ldm, ms, Y0.p, ldm, nullptr));
-  for (int si = 0; si < nshift; si++) {
-    const double cs = ch[si];
-    const double fc = (kind == 0) ? 1. / cs : 1. / sqrt (cs);
-    if (kept > 0) {
-      k_shift_coef<<<sgrid ((int64_t) kept * m), 256, 0, s>>> (kept, m, g->lam_d.p,
-                                                              cs, kind, Wc.p, Dc.p);
-      LGH_LAUNCH_CHECK ();
-      LGH_TRY (launch_gemm_nn<double> (n, kept, m, 1.0, g->Wz.p, g->ldu, Dc.p,
-                                       kept, fc, Y0.p, ldm, Xs.p, ldm, s));
-    } else {
-      LGH_TRY (launch_rowscale<double> (n, m, nullptr, Y0.p, ldm, Xs.p, ldm, s));
-      LGH_TRY (launch_vec_scale ((int64_t) n * ldm, Xs.p, nullptr, fc, Xs.p, s));
-    }
-    LGH_TRY (launch_rowmajor_to_colmajor (n, m, Xs.p, ldm, x + (size_t) si * m * ldx,
-                                          ldx, nullptr, s));
+  /* the shift-independent part: r2 (solve: M^{1/2} Z^{-1} r; sample: xi),
+   * C = U^T r2 and y0 = Z^{-1} M^{1/2} r2, in the object's batch plan */
+  ShiftPlan *P = nullptr;
+  LGH_TRY (shift_plan_get (g, n, m, kept, nshift, &P));
+  double *R = shift_plan_R (P), *Xs = shift_plan_Xs (P);
+  double *Y0 = shift_plan_Y0 (P), *Wc = shift_plan_Wc (P);
+  size_t wn = 0;
+  double *work = shift_plan_work (P, &wn);
+  LGH_TRY (launch_colmajor_to_rowmajor (n, m, rhs, ldr, R, ldm, nullptr, s));
+  double *r2 = R;
+  if (kind == 0) {
+    LGH_TRY (glr_zsolve (g, m, R, ldm, nullptr, Xs, ldm, ms));
+    r2 = Xs;
   }
+  if (kept > 0)
+    LGH_TRY (launch_gemm_tn<double> (n, kept, m, g->U.p, g->ldu, r2, ldm, Wc,
+                                     kept, 0, work, wn, s));
+  LGH_TRY (glr_zsolve (g, m, r2, ldm, ms, Y0, ldm, nullptr));
+  /* every shift in one fused launch (a captured graph after the first
+   * call of a shape); the tile variant is the autotuner's */
+  struct Trial
+  {
+    ShiftPlan *P;
+    lgh_glr_t *g;
+    int kind, nshift, m;
+    const double *c;
+    double *x;
+    int64_t ldx;
+    static int run (int v, void *ctx)
+    {
+      Trial *t = (Trial *) ctx;
+      return shift_plan_run_eager (t->P, t->g, t->kind, t->nshift, t->c, t->m,
+                                   t->x, t->ldx, v);
+    }
+  } trial{ P, g, kind, nshift, m, ch.data (), x, ldx };
+  int variant = 0, measured = 0;
+  LGH_TRY (tune_pick ("shift_combine", n, kept, m, nshift, kShiftVariants,
+                      &Trial::run, &trial, &variant, &measured));
+  /* a measured first call has its result from the trials already */
+  if (!measured)
+    LGH_TRY (shift_plan_combine (P, g, kind, nshift, ch.data (), m, x, ldx,
+                                 variant));
   LGH_CUDA (cudaStreamSynchronize (s));
   return 0;
 }
@@ -818,9 +841,26 @@ void
 lgh_glr_destroy (lgh_glr_t *glr)
 {
   if (glr == NULL) return;
+  shift_plan_free (glr->splan);
+  glr->splan = nullptr;
   if (glr->B) mat_release (glr->B);
   lgh_prior_destroy (glr->prior);
   delete glr;
+}
+
+int
+lgh_glr_batch_info (const lgh_glr_t *glr, long *graph_captures,
+                    long *graph_replays, int *tile_variant, int *tuned_shapes)
+{
+  LGH_CHECK (glr, LGH_ERR_ARG_NULL, "lgh_glr_batch_info: NULL");
+  long c = 0, r = 0;
+  int v = -1;
+  shift_plan_stats (glr->splan, &c, &r, &v);
+  if (graph_captures) *graph_captures = c;
+  if (graph_replays) *graph_replays = r;
+  if (tile_variant) *tile_variant = v;
+  if (tuned_shapes) *tuned_shapes = tune_table_size ();
+  return 0;
 }
 
 int

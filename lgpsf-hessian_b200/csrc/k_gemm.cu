@@ -25,6 +25,7 @@
 
 #include <algorithm>
 
+#include "lgh_batch.h"
 #include "lgh_device.cuh"
 #include "lgh_internal.h"
 
@@ -296,6 +297,139 @@ k_gemm_nn (int64_t n, int k, int m2, double alpha, const T *__restrict__ X,
           Y[i * ldy + j] = (T) v;
         }
       }
+}
+
+/* The Woodbury combination of many shifts in one launch (the batched
+ * solve / sample of the shift-independent form x_c = f(c) y0 + W D_c U^T r,
+ * glr_common_impl.h:910-929 applied per shift):
+ *   out[:, J] = fc[si] Y0[:, j] + W (g[si, :] .* C[:, j]),  J = si m + j,
+ * W n x kept row-major (the shift-independent W = Z^{-1} M^{1/2} U), C
+ * kept x m column-major (U^T r), g kept x nshift column-major (g[k, si] =
+ * f(lam_k + c_si) - f(c_si)), Y0 n x m row-major, out column-major with
+ * leading dimension *ldo at *out (the output pointer is read from device
+ * memory so that a captured graph serves every call).  One GEMM of n x
+ * (nshift m) x kept on the FP64 tensor cores: the shift coefficient is
+ * folded into the staging of the B operand, and the epilogue adds f(c) y0
+ * and writes the caller's column-major result directly.  Column tiles run
+ * fastest, so the CTAs resident at once share a band of W rows in L2. */
+/* one staged k block of a BM-row A tile (row stride BM + 4) */
+template <int BM>
+__device__ __forceinline__ void
+dmma_block_rows (const double (*As)[BM + 4], const double (*Bs)[SLD], int wm,
+                 int wn, int lane, double (&acc)[4][4][2])
+{
+#pragma unroll
+  for (int kk = 0; kk < GK; kk += 4) {
+    double a[4], b[4];
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      a[t] = As[kk + (lane & 3)][wm * 32 + t * 8 + (lane >> 2)];
+      b[t] = Bs[kk + (lane & 3)][wn * 32 + t * 8 + (lane >> 2)];
+    }
+#pragma unroll
+    for (int ti = 0; ti < 4; ti++)
+#pragma unroll
+      for (int tj = 0; tj < 4; tj++)
+        asm volatile ("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 "
+                      "{%0, %1}, {%2}, {%3}, {%0, %1};"
+                      : "+d"(acc[ti][tj][0]), "+d"(acc[ti][tj][1])
+                      : "d"(a[ti]), "d"(b[tj]));
+  }
+}
+
+/* BM = 64 (4 warps, 2 x 2 quarters of 32 x 32) or 128 (8 warps, 4 x 2) */
+template <typename T, int BM>
+__global__ void __launch_bounds__ (BM * 2)
+k_shift_combine (int64_t n, int kept, int m, int nshift,
+                 const T *__restrict__ W, int ldw, const double *__restrict__ C,
+                 const double *__restrict__ g, const double *__restrict__ fc,
+                 const T *__restrict__ Y0, int ldy0,
+                 double *const *__restrict__ out, const int64_t *__restrict__ ldo)
+{
+  __shared__ double As[GK][BM + 4], Bs[GK][SLD];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  const int ncol = nshift * m;
+  const int64_t i0 = (int64_t) blockIdx.y * BM;
+  const int j0 = blockIdx.x * GB;
+  double acc[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) acc[a][b][0] = acc[a][b][1] = 0.;
+  /* staging: thread -> A tile row tid / 2 (all threads) and B tile column
+   * tid / 2 (the first 128 threads), 8 consecutive k each */
+  const int lr = tid >> 1, lk = (tid & 1) * 8;
+  const bool bthr = lr < GB;
+  const int Jr = j0 + lr;
+  const bool bcol = bthr && Jr < ncol;
+  const int sr = bcol ? Jr / m : 0, jr = bcol ? Jr - sr * m : 0;
+  double ra[8], rb[8];
+  auto fetch = [&] (int k0) {
+    const int64_t gi = i0 + lr;
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      const int kk = k0 + lk + e;
+      ra[e] = (gi < n && kk < kept) ? (double) W[gi * ldw + kk] : 0.;
+      rb[e] = (bcol && kk < kept)
+              ? g[kk + (size_t) sr * kept] * C[kk + (size_t) jr * kept] : 0.;
+    }
+  };
+  if (kept > 0) fetch (0);
+  for (int k0 = 0; k0 < kept; k0 += GK) {
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      As[lk + e][lr] = ra[e];
+      if (bthr) Bs[lk + e][lr] = rb[e];
+    }
+    __syncthreads ();
+    if (k0 + GK < kept) fetch (k0 + GK);
+    dmma_block_rows<BM> (As, Bs, wm, wn, lane, acc);
+    __syncthreads ();
+  }
+  double *const o = *out;
+  const int64_t ld = *ldo;
+#pragma unroll
+  for (int tj = 0; tj < 4; tj++)
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+      const int J = j0 + dmma_col (wn, tj, c, lane);
+      if (J >= ncol) continue;
+      const int si = J / m, j = J - si * m;
+      const double f = fc[si];
+#pragma unroll
+      for (int ti = 0; ti < 4; ti++) {
+        const int64_t i = i0 + dmma_row (wm, ti, lane);
+        if (i < n)
+          o[i + (int64_t) J * ld] = acc[ti][tj][c] + f * (double) Y0[i * ldy0 + j];
+      }
+    }
+}
+
+int
+launch_shift_combine_variant (int variant, int64_t n, int kept, int m,
+                              int nshift, const double *W, int ldw,
+                              const double *C, const double *g,
+                              const double *fc, const double *Y0, int ldy0,
+                              double *const *out, const int64_t *ldo,
+                              cudaStream_t s)
+{
+  if (n == 0 || m == 0 || nshift == 0) return 0;
+  const int BM = variant == 1 ? 128 : 64;
+  const int64_t ncol = (int64_t) nshift * m;
+  const int64_t rt = (n + BM - 1) / BM;
+  LGH_CHECK (ncol < INT32_MAX && rt < 65536, LGH_ERR_ARG_OUTOFRANGE,
+             "shift combine: %lld rows x %lld columns exceed the grid",
+             (long long) n, (long long) ncol);
+  dim3 grid ((unsigned) ((ncol + GB - 1) / GB), (unsigned) rt);
+  if (variant == 1)
+    k_shift_combine<double, 128><<<grid, 256, 0, s>>> (
+        n, kept, m, nshift, W, ldw, C, g, fc, Y0, ldy0, out, ldo);
+  else
+    k_shift_combine<double, 64><<<grid, 128, 0, s>>> (
+        n, kept, m, nshift, W, ldw, C, g, fc, Y0, ldy0, out, ldo);
+  LGH_LAUNCH_CHECK ();
+  return 0;
 }
 
 /* Y = A^{-1} B on the dense coarse level: A^{-1} n0 x n0 column-major,

@@ -233,6 +233,7 @@ int launch_gemm_nn (int64_t n, int k, int m2, double alpha, const T *X,
                     int ldx, const double *M, int ldm, double beta,
                     const T *Y0, int ldy0, T *Y, int ldy, cudaStream_t s);
 size_t gemm_tn_work_elems (int64_t n, int m1, int m2);
+
 /* partial-sum elements enough for every gemm_tn shape up to m1max x m2max */
 size_t gemm_tn_work_max (int m1max, int m2max);
 /* Y = A^{-1} B for a dense n0 x n0 column-major A^{-1} and row-major B, Y

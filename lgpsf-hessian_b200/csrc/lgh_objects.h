@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "lgh_internal.h"
+#include "lgh_batch.h"
 #include "lgh_strip.h"
 
 /* Mat: a device CSR operator (kind 0) or a dense column-block view handed
@@ -89,6 +90,8 @@ struct lgh_glr
    * W = Z^{-1} M^{1/2} U (n x kept, row-major, ld ldu) */
   lgh::DBuf<double> Wz;
   int have_wz = 0;
+  /* workspace and captured graph of the many-shift combination (batch.cu) */
+  lgh::ShiftPlan *splan = nullptr;
   lgh_glr_stats_t stats{};
 };
 

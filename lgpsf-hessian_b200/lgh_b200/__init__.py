@@ -279,6 +279,7 @@ SIGNATURES = {
                                        ctypes.c_int, P]),
     "lgh_test_rng_state": (ctypes.c_int, [ctypes.c_uint64, I64, I64,
                                           ctypes.c_int, P]),
+    "lgh_glr_batch_info": (ctypes.c_int, [P, P, P, P, P]),
     "lgh_test_spmm": (ctypes.c_int, [P, ctypes.c_int, P, P, ctypes.c_int]),
     "lgh_test_spmm_strip": (ctypes.c_int, [P, ctypes.c_int, P, P, ctypes.c_int,
                                            ctypes.c_int, P]),
@@ -654,6 +655,19 @@ class Glr:
                                          out.ctypes.data_as(c_dbl_p)),
              "lgh_glr_logdet_batch")
         return out
+
+    def batch_info(self):
+        """Graph captures / replays of the batched operations, the tile
+        variant of the last combination and the autotuner's table size."""
+        c, r = ctypes.c_long(), ctypes.c_long()
+        v, t = ctypes.c_int(), ctypes.c_int()
+        _chk(load().lgh_glr_batch_info(self.h, ctypes.addressof(c),
+                                       ctypes.addressof(r),
+                                       ctypes.addressof(v),
+                                       ctypes.addressof(t)),
+             "lgh_glr_batch_info")
+        return dict(captures=c.value, replays=r.value, variant=v.value,
+                    tuned_shapes=t.value)
 
     def _batch(self, fname, cs, R):
         cs = np.ascontiguousarray(cs, dtype=np.float64)

@@ -231,6 +231,34 @@ def test_batch_matches_single():
         assert abs(ld[si] - g.logdet(c)) <= 1e-14 * abs(ld[si])
 
 
+def test_many_shift_batch_graph_replay():
+    """Many shifts in one fused combination, captured as a graph on the
+    first call of a shape and replayed on the next: the replay writes the
+    new call's output buffer with the new call's shifts.  Both calls match
+    the single-vector operations."""
+    cfg, keep = _c1()
+    B, Z, pr = keep
+    g = L.Glr(B, pr, L.glr_opts(ell=40, seed=0, check=0))
+    rng = np.random.default_rng(12)
+    R = rng.standard_normal((cfg["N"], 5))
+    cs1 = np.logspace(-3, 3, 7)
+    cs2 = np.logspace(-2, 2, 7) * 1.5
+    X1 = g.solve_batch(cs1, R)
+    info1 = g.batch_info()
+    X2 = g.solve_batch(cs2, R)
+    info2 = g.batch_info()
+    assert info1["tuned_shapes"] >= 1 and info1["variant"] in (0, 1)
+    assert info2["captures"] == max(info1["captures"], 1)
+    assert info2["replays"] == info1["replays"] + 1
+    for cs, X in ((cs1, X1), (cs2, X2)):
+        for si in (0, 3, 6):
+            for j in (0, 4):
+                assert _rd(X[si][:, j], g.solve(cs[si], R[:, j])) < 1e-8
+    S = g.sample_batch(cs2, R)
+    for si in (0, 6):
+        assert _rd(S[si][:, 1], g.sample(cs2[si], R[:, 1])) < 1e-8
+
+
 def test_single_shift_batch_before_and_after_w():
     """One shift on an object without W = Z^{-1} M^{1/2} U takes the
     per-call formula (no W); once W exists (a multi-shift call builds it)
