@@ -716,15 +716,32 @@ batch_op (lgh_glr_t *g, int kind, int nshift, const double *c, int m,
                                    t->x, t->ldx, v);
     }
   } trial{ P, g, kind, nshift, m, ch.data (), x, ldx };
-  int variant = 0, measured = 0;
-  LGH_TRY (tune_pick ("shift_combine", n, kept, m, nshift, kShiftVariants,
-                      &Trial::run, &trial, &variant, &measured));
+  /* mixed-precision objects: the tcgen05 (TF32 x 3) form; FP64 objects:
+   * the FP64 tensor-core form */
+  const bool tc = g->exec.precision == LGH_PREC_MIXED && kept > 0
+                  && umma_supported ();
+  if (tc) LGH_TRY (shift_plan_prepare_umma (P, g, nshift, m));
+  struct Offset
+  {
+    Trial *t;
+    int base;
+    static int run (int v, void *ctx)
+    {
+      Offset *o = (Offset *) ctx;
+      return Trial::run (o->base + v, o->t);
+    }
+  } off{ &trial, tc ? kShiftVariants : 0 };
+  int v = 0, measured = 0;
+  LGH_TRY (tune_pick (tc ? "shift_combine_tf32x3" : "shift_combine_f64", n,
+                      kept, m, nshift, tc ? kUmmaVariants : kShiftVariants,
+                      &Offset::run, &off, &v, &measured));
+  const int variant = off.base + v;
   /* a measured first call has its result from the trials already */
   if (!measured)
     LGH_TRY (shift_plan_combine (P, g, kind, nshift, ch.data (), m, x, ldx,
                                  variant));
   LGH_CUDA (cudaStreamSynchronize (s));
-  return 0;
+  return shift_plan_check (P);
 }
 
 } /* namespace lgh */

@@ -82,6 +82,15 @@ struct ShiftPlan
   const double *g_W = nullptr, *g_lam = nullptr;
   long replays = 0, captures = 0;
   int last_variant = -1;
+  /* the tensor-core form (mixed-precision objects): W split once, the
+   * coefficient block split per call, tensor maps of both tile widths */
+  int kpad = 0, ncolp = 0;
+  DBuf<float> Ah, Al, Bh, Bl;
+  DBuf<int> err;
+  const double *a_W = nullptr;
+  int a_kept = -1;
+  UmmaMaps maps[2];
+  bool maps_ok = false;
 
   ~ShiftPlan ()
   {
@@ -131,6 +140,63 @@ struct ShiftPlan
   }
 };
 
+/* the tensor-core operands of a mixed-precision object: A from W (when
+ * W or kept changed), B's buffers for nshift x m columns, the tensor maps */
+int
+shift_plan_prepare_umma (ShiftPlan *P, lgh_glr_t *g, int nshift, int m)
+{
+  cudaStream_t s = stream ();
+  const int kpad = std::max (32, (P->kept + 31) / 32 * 32);
+  const int ncolp = (nshift * m + 255) / 256 * 256;
+  bool remap = false;
+  if (!P->err.p) {
+    LGH_TRY (P->err.alloc (1));
+    LGH_CUDA (cudaMemsetAsync (P->err.p, 0, sizeof (int), s));
+  }
+  if (kpad != P->kpad || P->a_W != g->Wz.p || P->a_kept != P->kept) {
+    P->drop_graph ();
+    P->kpad = kpad;
+    LGH_TRY (P->Ah.alloc ((size_t) P->n * kpad));
+    LGH_TRY (P->Al.alloc ((size_t) P->n * kpad));
+    LGH_TRY (umma_split_rows (P->n, P->kept, kpad, g->Wz.p, g->ldu, P->Ah.p,
+                              P->Al.p, s));
+    P->a_W = g->Wz.p;
+    P->a_kept = P->kept;
+    remap = true;
+  }
+  if (ncolp > P->ncolp) {
+    P->drop_graph ();
+    P->ncolp = ncolp;
+    LGH_TRY (P->Bh.alloc ((size_t) ncolp * kpad));
+    LGH_TRY (P->Bl.alloc ((size_t) ncolp * kpad));
+    remap = true;
+  }
+  if (remap || !P->maps_ok) {
+    P->maps_ok = false;
+    LGH_TRY (umma_encode (&P->maps[0], P->Ah.p, P->Al.p, P->n, P->Bh.p, P->Bl.p,
+                          P->ncolp, P->kpad, 128));
+    LGH_TRY (umma_encode (&P->maps[1], P->Ah.p, P->Al.p, P->n, P->Bh.p, P->Bl.p,
+                          P->ncolp, P->kpad, 256));
+    P->maps_ok = true;
+  }
+  return 0;
+}
+
+/* a failed pipeline wait in the tensor-core kernel since the last check */
+int
+shift_plan_check (ShiftPlan *P)
+{
+  if (!P->err.p) return 0;
+  int e = 0;
+  LGH_CUDA (cudaMemcpy (&e, P->err.p, sizeof (int), cudaMemcpyDeviceToHost));
+  if (e) {
+    LGH_CUDA (cudaMemset (P->err.p, 0, sizeof (int)));
+    return set_error (LGH_ERR_GPU, "batched combination: a tensor-core "
+                      "pipeline wait ran out (code %d)", e);
+  }
+  return 0;
+}
+
 /* the fixed-shape tail: parameters up, coefficient table, combination */
 static int
 enqueue_tail (ShiftPlan &P, lgh_glr_t *g, int kind, int nshift, int variant,
@@ -145,6 +211,15 @@ enqueue_tail (ShiftPlan &P, lgh_glr_t *g, int kind, int nshift, int variant,
   k_shift_table<<<std::max (grid, 1), 256, 0, s>>> (P.kept, nshift, g->lam_d.p,
                                                     P.cdev.p, kind, P.g.p, P.fc.p);
   LGH_LAUNCH_CHECK ();
+  if (variant >= kShiftVariants) {
+    LGH_CHECK (P.maps_ok, LGH_ERR_ARG_WRONGSTATE, "batch: tensor maps missing");
+    LGH_TRY (umma_split_coef (P.kept, P.kpad, m, nshift, P.ncolp, P.g.p, P.Wc.p,
+                              P.Bh.p, P.Bl.p, s));
+    return launch_shift_combine_umma (P.maps[variant - kShiftVariants], P.n,
+                                      P.kpad, m, nshift, P.fc.p, P.Y0.p,
+                                      round_ld (m), &pd->out, &pd->ldo,
+                                      P.err.p, s);
+  }
   return launch_shift_combine_variant (variant, P.n, P.kept, m, nshift, g->Wz.p,
                                        g->ldu, P.Wc.p, P.g.p, P.fc.p, P.Y0.p,
                                        round_ld (m), &pd->out, &pd->ldo, s);

@@ -33,16 +33,44 @@ int shift_plan_run_eager (ShiftPlan *P, lgh_glr *g, int kind, int nshift,
 void shift_plan_stats (const ShiftPlan *P, long *captures, long *replays,
                        int *last_variant);
 void shift_plan_free (ShiftPlan *P);
+/* mixed-precision objects: the tensor-core operands and tensor maps */
+int shift_plan_prepare_umma (ShiftPlan *P, lgh_glr *g, int nshift, int m);
+/* the error flag of the tensor-core kernel (nonzero: a wait ran out) */
+int shift_plan_check (ShiftPlan *P);
+/* whether this device runs the tensor-core form (sm_100, tensor maps) */
+bool umma_supported ();
 
-/* tile variants of the combination kernel: 0 = 64 x 64 (4 warps),
- * 1 = 128 x 64 (8 warps) */
+/* tile variants of the combination kernel: FP64 objects 0 = 64 x 64 (4
+ * warps), 1 = 128 x 64 (8 warps) on the FP64 mma.sync path; mixed objects
+ * 2 = 128 x 128, 3 = 128 x 256 on tcgen05 (TF32 x 3) */
 constexpr int kShiftVariants = 2;
+constexpr int kUmmaVariants = 2;
 int launch_shift_combine_variant (int variant, int64_t n, int kept, int m,
                                   int nshift, const double *W, int ldw,
                                   const double *C, const double *g,
                                   const double *fc, const double *Y0,
                                   int ldy0, double *const *out,
                                   const int64_t *ldo, cudaStream_t s);
+
+/* the tensor-core (tcgen05) form of the combination for mixed-precision
+ * objects (k_umma.cu): TF32 operands split in two parts, four TMA tensor
+ * maps (A hi / lo: n x kpad, B hi / lo: columns x kpad, FP32, K-major) */
+struct UmmaMaps
+{
+  alignas (64) unsigned char raw[4 * 128];
+  int tn = 0;
+};
+int umma_split_rows (int64_t n, int kept, int kpad, const double *W, int ldw,
+                     float *Ah, float *Al, cudaStream_t s);
+int umma_split_coef (int kept, int kpad, int m, int nshift, int ncolp,
+                     const double *g, const double *C, float *Bh, float *Bl,
+                     cudaStream_t s);
+int umma_encode (UmmaMaps *M, const float *Ah, const float *Al, int64_t n,
+                 const float *Bh, const float *Bl, int ncolp, int kpad, int tn);
+int launch_shift_combine_umma (const UmmaMaps &M, int64_t n, int kpad, int m,
+                               int nshift, const double *fc, const double *Y0,
+                               int ldy0, double *const *out, const int64_t *ldo,
+                               int *err, cudaStream_t s);
 
 /* the autotuner: the fastest variant for a shape key, measured once per
  * process (and kept in the cache file named by LGH_TUNE_CACHE, when set);
