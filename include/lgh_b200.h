@@ -292,8 +292,21 @@ typedef struct lgh_exec_opts
   int    verbose;
   int    rank_cap;     /* keep at most rank_cap modes ("rank r,
                           oversample p" = ell r + p, rank_cap r); 0 = off */
+  int    check_form;   /* the residual check (opts.check): LGH_CHECK_PROJ
+                          (default) or LGH_CHECK_APPLY                    */
 }
 lgh_exec_opts_t;
+
+/* Two forms of the same residual check max_j ||F u_j - lam_j u_j||
+ * (glr_common_impl.h:576-600).  The reference applies F to the kept U
+ * again (LGH_CHECK_APPLY: one more F-apply of kept columns, a quarter of
+ * the build).  Since U = Q C and F is linear, F U = (F Q) C, and F Q is
+ * the block the Rayleigh-Ritz projection has just formed: LGH_CHECK_PROJ
+ * forms F U as one product of that block with C.  The two differ by the
+ * Z-solve tolerance (F through inexact solves is linear to that
+ * accuracy).                                                              */
+#define LGH_CHECK_PROJ  0
+#define LGH_CHECK_APPLY 1
 
 lgh_exec_opts_t lgh_exec_opts_default (void);
 
@@ -301,6 +314,52 @@ int lgh_glr_compute_ex (lgh_Mat B, lgh_prior_t *prior,
                         const lgh_glr_opts_t *opts,
                         const lgh_exec_opts_t *exec, lgh_glr_t **glr,
                         lgh_glr_report_t *report);
+
+/* ---- several GPUs: the sketch's columns sharded over ranks --------------
+ * The reference distributes the build over MPI row slabs
+ * (docs/glr-woodbury-formulas.tex:76-98).  Here every rank (one process or
+ * thread per GPU) holds B, Z and the whole N x ell blocks, and applies F
+ * only to its own contiguous range of sketch columns (lgh_cols_range; the
+ * hashed sketch does not depend on the split).  After each F-apply one
+ * all-gather rebuilds the full block on every rank; CholQR2, the
+ * Rayleigh-Ritz step and the selection then run identically on all ranks,
+ * so every rank ends with the same object (U, lambda), which serves
+ * solves / samples / logdet locally.  The F-applies (Z-solves and B
+ * products, nearly all of the build) split evenly; no halo exchange is
+ * needed.  The residual check and lgh_glr_extend shard the same way.
+ *
+ * allgather: make recv[r * len, (r + 1) * len) equal rank r's send[0, len)
+ * on every rank, for device buffers, and return 0 (nonzero: the build
+ * fails with LGH_ERR_GPU).  All ranks call it the same number of times
+ * with the same len.  send / recv: caller-owned device buffers of `bytes`
+ * and size * bytes (bytes >= lgh_cols_exchange_bytes), or NULL for
+ * buffers the library allocates; the callback receives the buffers in use.
+ * The communicator must stay valid for the object's lifetime (extend).   */
+typedef struct lgh_comm
+{
+  int    rank, size;
+  void  *send, *recv;
+  size_t bytes;
+  int  (*allgather) (const void *send, void *recv, size_t len, void *ctx);
+  void  *ctx;
+}
+lgh_comm_t;
+
+/* columns [c0, c1) of a width-w block owned by `rank` of `size` (groups of
+ * 4 columns, contiguous, in rank order) */
+void lgh_cols_range (int w, int rank, int size, int *c0, int *c1);
+/* exchange buffer bytes one rank needs for an n-row build at width ell   */
+size_t lgh_cols_exchange_bytes (int64_t n, int ell, int size);
+int lgh_glr_compute_cols (lgh_Mat B, lgh_prior_t *prior,
+                          const lgh_glr_opts_t *opts,
+                          const lgh_exec_opts_t *exec, const lgh_comm_t *comm,
+                          lgh_glr_t **glr, lgh_glr_report_t *report);
+/* `size` communicators for ranks run as threads of one process on one
+ * device (testing the sharded path where fewer GPUs than ranks exist): the
+ * all-gather meets on a host barrier (120 s limit, then LGH_ERR_GPU) and
+ * copies device to device; no kernel waits for another rank.             */
+int lgh_comm_local_create (int size, lgh_comm_t *comms);
+void lgh_comm_local_destroy (lgh_comm_t *comms);
 
 typedef struct lgh_glr_stats
 {

@@ -364,17 +364,74 @@ rayleigh_ritz (lgh_glr_t *g, int ell, const T *Q, int ldq, const double *Araw,
   return 0;
 }
 
-/* max_j || F u_j - lam_raw_j u_j || (glr_common_impl.h:576-600) */
+/* Y = F X over w columns on a column-sharded object: this rank applies F
+ * to its own columns, then one all-gather of the packed column blocks
+ * rebuilds all w columns of Y on every rank (one device: plain apply_F) */
 template <typename T>
 static int
-residual_check (lgh_glr_t *g, T *Ubuf, T *FU, T *Wk, lgh_glr_report_t *rep)
+apply_F_cols (lgh_glr_t *g, int w, const T *X, int ldx, T *Y, int ldy, T *W,
+              int ldw)
+{
+  const lgh_comm_t &cm = g->comm;
+  if (cm.size <= 1) return apply_F<T> (g, w, X, ldx, Y, ldy, W, ldw);
+  cudaStream_t s = stream ();
+  const int64_t n = g->n;
+  int c0, c1, wmax = 0;
+  for (int r = 0; r < cm.size; r++) {
+    lgh_cols_range (w, r, cm.size, &c0, &c1);
+    wmax = std::max (wmax, c1 - c0);
+  }
+  lgh_cols_range (w, cm.rank, cm.size, &c0, &c1);
+  if (c1 > c0)
+    LGH_TRY (apply_F<T> (g, c1 - c0, X + c0, ldx, Y + c0, ldy, W + c0, ldw));
+  const int ldp = round_ld (std::max (wmax, 1));
+  const size_t len = (size_t) n * ldp * sizeof (T);
+  char *snd = (char *) cm.send, *rcv = (char *) cm.recv;
+  if (!snd || !rcv || cm.bytes < len) {
+    LGH_TRY (g->xsend.alloc (len));
+    LGH_TRY (g->xrecv.alloc (len * cm.size));
+    snd = g->xsend.p;
+    rcv = g->xrecv.p;
+  }
+  if (c1 > c0)
+    LGH_TRY (launch_copy_block<T> (n, c1 - c0, Y + c0, ldy, (T *) snd, ldp, s));
+  LGH_CUDA (cudaStreamSynchronize (s));
+  LGH_CHECK (cm.allgather (snd, rcv, len, cm.ctx) == 0, LGH_ERR_GPU,
+             "column-sharded build: the all-gather failed (rank %d of %d)",
+             cm.rank, cm.size);
+  for (int r = 0; r < cm.size; r++) {
+    if (r == cm.rank) continue;
+    int r0, r1;
+    lgh_cols_range (w, r, cm.size, &r0, &r1);
+    if (r1 > r0)
+      LGH_TRY (launch_copy_block<T> (n, r1 - r0, (const T *) (rcv + r * len),
+                                     ldp, Y + r0, ldy, s));
+  }
+  LGH_CUDA (cudaStreamSynchronize (s));
+  return 0;
+}
+
+/* max_j || F u_j - lam_raw_j u_j || (glr_common_impl.h:576-600).  FY, C
+ * (nullable): the projection pass's block F Q (n x ell, ld ldf) and the
+ * kept Ritz coefficients (ell x kept, column-major): F U = (F Q) C, one
+ * product, instead of another F-apply of U (check_form) */
+template <typename T>
+static int
+residual_check (lgh_glr_t *g, T *Ubuf, T *FU, T *Wk, lgh_glr_report_t *rep,
+                const T *FY = nullptr, int ldf = 0, const double *C = nullptr,
+                int ell = 0)
 {
   if (!g->opts.check || g->kept == 0) return 0;
   cudaStream_t s = stream ();
   const int kept = g->kept, ldu = g->ldu;
   double t0 = wall ();
-  LGH_TRY (apply_F<T> (g, kept, Ubuf, ldu, FU, ldu, Wk, ldu));
-  rep->t_operator += wall () - t0;
+  if (FY && C && g->exec.check_form == LGH_CHECK_PROJ) {
+    LGH_TRY (launch_gemm_nn<T> (g->n, ell, kept, 1.0, FY, ldf, C, ell, 0.,
+                                FU, ldu, FU, ldu, s));
+  } else {
+    LGH_TRY (apply_F_cols<T> (g, kept, Ubuf, ldu, FU, ldu, Wk, ldu));
+    rep->t_operator += wall () - t0;
+  }
   DBuf<double> norms, part;
   DBuf<unsigned> cnt;
   LGH_TRY (norms.alloc (kept));
@@ -423,7 +480,7 @@ build (lgh_glr_t *g, lgh_glr_report_t *rep)
 
   /* Y = F Omega; power passes with re-orthonormalisation */
   t0 = wall ();
-  LGH_TRY (apply_F<T> (g, ell, Q.p, ld, Y.p, ld, W.p, ld));
+  LGH_TRY (apply_F_cols<T> (g, ell, Q.p, ld, Y.p, ld, W.p, ld));
   rep->t_operator += wall () - t0;
   for (int p = 0; p < g->opts.q_power; p++) {
     t0 = wall ();
@@ -434,7 +491,7 @@ build (lgh_glr_t *g, lgh_glr_report_t *rep)
     g->stats.t_orth += dt;
     Q.swap (Y);
     t0 = wall ();
-    LGH_TRY (apply_F<T> (g, ell, Q.p, ld, Y.p, ld, W.p, ld));
+    LGH_TRY (apply_F_cols<T> (g, ell, Q.p, ld, Y.p, ld, W.p, ld));
     rep->t_operator += wall () - t0;
   }
   t0 = wall ();
@@ -449,7 +506,7 @@ build (lgh_glr_t *g, lgh_glr_report_t *rep)
 
   /* T = Q^T F Q */
   t0 = wall ();
-  LGH_TRY (apply_F<T> (g, ell, Q.p, ld, Y.p, ld, W.p, ld));
+  LGH_TRY (apply_F_cols<T> (g, ell, Q.p, ld, Y.p, ld, W.p, ld));
   rep->t_operator += wall () - t0;
   DBuf<double> A;
   LGH_TRY (A.alloc ((size_t) ell * ell));
@@ -459,10 +516,16 @@ build (lgh_glr_t *g, lgh_glr_report_t *rep)
 
   /* residual check on the kept columns (U in FP64 or FP32 blocks) */
   if (g->opts.check && g->kept > 0) {
+    /* Y still holds F Q and sm.C the kept coefficients: the projection
+     * form writes F U = Y C into W; the apply form overwrites Y with F U
+     * and uses W as its scratch */
+    T *FU = g->exec.check_form == LGH_CHECK_PROJ ? W.p : Y.p;
     if constexpr (std::is_same<T, double>::value)
-      LGH_TRY (residual_check<double> (g, g->U.p, Y.p, W.p, rep));
+      LGH_TRY (residual_check<double> (g, g->U.p, FU, W.p, rep, Y.p, ld,
+                                       sm.C.p, ell));
     else
-      LGH_TRY (residual_check<float> (g, g->U32.p, Y.p, W.p, rep));
+      LGH_TRY (residual_check<float> (g, g->U32.p, FU, W.p, rep, Y.p, ld,
+                                      sm.C.p, ell));
   }
 
   /* keep the sketch state for the incremental extension */
@@ -513,7 +576,7 @@ extend_incremental (lgh_glr_t *g, int k_new, lgh_glr_report_t *rep)
 
   /* power passes on the new block (internal orthonormalisation only) */
   t0 = wall ();
-  LGH_TRY (apply_F<T> (g, k_new, Qn.p, ldk, Yn.p, ldk, Wn.p, ldk));
+  LGH_TRY (apply_F_cols<T> (g, k_new, Qn.p, ldk, Yn.p, ldk, Wn.p, ldk));
   rep->t_operator += wall () - t0;
   for (int p = 0; p < g->opts.q_power; p++) {
     t0 = wall ();
@@ -522,7 +585,7 @@ extend_incremental (lgh_glr_t *g, int k_new, lgh_glr_report_t *rep)
     rep->t_dense += wall () - t0;
     Qn.swap (Yn);
     t0 = wall ();
-    LGH_TRY (apply_F<T> (g, k_new, Qn.p, ldk, Yn.p, ldk, Wn.p, ldk));
+    LGH_TRY (apply_F_cols<T> (g, k_new, Qn.p, ldk, Yn.p, ldk, Wn.p, ldk));
     rep->t_operator += wall () - t0;
   }
   /* F^{q+1} Omega_new into Qb's new columns; BCGS2 vs old + internal */
@@ -534,7 +597,7 @@ extend_incremental (lgh_glr_t *g, int k_new, lgh_glr_report_t *rep)
   /* F Q_new, border columns Cnew = Q_all^T (F Q_new) */
   LGH_TRY (launch_copy_block<T> (n, k_new, Qb.p + l1, ld2, Qn.p, ldk, s));
   t0 = wall ();
-  LGH_TRY (apply_F<T> (g, k_new, Qn.p, ldk, Yn.p, ldk, Wn.p, ldk));
+  LGH_TRY (apply_F_cols<T> (g, k_new, Qn.p, ldk, Yn.p, ldk, Wn.p, ldk));
   rep->t_operator += wall () - t0;
   DBuf<double> Cn, A2;
   LGH_TRY (Cn.alloc ((size_t) l2 * k_new));
@@ -779,8 +842,12 @@ lgh_exec_opts_default (void)
   e.inner_rtol = 0.;
   e.verbose = 0;
   e.rank_cap = 0;
+  e.check_form = LGH_CHECK_PROJ;
   return e;
 }
+
+/* the communicator of the lgh_glr_compute_cols call on this thread */
+static thread_local const lgh_comm_t *t_comm = nullptr;
 
 int
 lgh_glr_compute_ex (lgh_Mat B, lgh_prior_t *prior, const lgh_glr_opts_t *opts,
@@ -807,6 +874,7 @@ lgh_glr_compute_ex (lgh_Mat B, lgh_prior_t *prior, const lgh_glr_opts_t *opts,
   B->refs++;
   g->prior = prior;
   prior_ref (prior);
+  if (t_comm) g->comm = *t_comm;
   lgh_glr_report_t rep;
   int rc = (g->exec.precision == LGH_PREC_MIXED) ? build<float> (g, &rep)
                                                  : build<double> (g, &rep);
@@ -824,6 +892,42 @@ lgh_glr_compute (lgh_Mat B, lgh_prior_t *prior, const lgh_glr_opts_t *opts,
                  lgh_glr_t **glr, lgh_glr_report_t *report)
 {
   return lgh_glr_compute_ex (B, prior, opts, nullptr, glr, report);
+}
+
+void
+lgh_cols_range (int w, int rank, int size, int *c0, int *c1)
+{
+  const int groups = (w + 3) / 4;
+  const int g0 = (int) ((int64_t) groups * rank / size);
+  const int g1 = (int) ((int64_t) groups * (rank + 1) / size);
+  *c0 = std::min (w, 4 * g0);
+  *c1 = std::min (w, 4 * g1);
+}
+
+size_t
+lgh_cols_exchange_bytes (int64_t n, int ell, int size)
+{
+  int wmax = 0, c0, c1;
+  for (int r = 0; r < size; r++) {
+    lgh_cols_range (ell, r, size, &c0, &c1);
+    wmax = std::max (wmax, c1 - c0);
+  }
+  return (size_t) n * round_ld (std::max (wmax, 1)) * sizeof (double);
+}
+
+int
+lgh_glr_compute_cols (lgh_Mat B, lgh_prior_t *prior, const lgh_glr_opts_t *opts,
+                      const lgh_exec_opts_t *exec, const lgh_comm_t *comm,
+                      lgh_glr_t **glr, lgh_glr_report_t *report)
+{
+  LGH_CHECK (comm && comm->allgather && comm->size >= 1 && comm->rank >= 0
+             && comm->rank < comm->size, LGH_ERR_ARG_WRONG,
+             "lgh_glr_compute_cols: need a communicator with 0 <= rank < size "
+             "and an all-gather");
+  t_comm = comm;
+  const int rc = lgh_glr_compute_ex (B, prior, opts, exec, glr, report);
+  t_comm = nullptr;
+  return rc;
 }
 
 int

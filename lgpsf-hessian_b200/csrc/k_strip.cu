@@ -129,7 +129,7 @@ k_scan_counts (int64_t m, const int64_t *__restrict__ counts,
  * at pack 32 CH blockIdx.y.  Each entry: one gathered X pack per owned
  * pack, applied to the R rows. */
 template <typename T, typename TV, int R, int CH>
-__global__ void __launch_bounds__ (256)
+__global__ void __launch_bounds__ (256, 2)
 k_strip_spmm (int64_t n, int64_t nstrips, const int64_t *__restrict__ sptr,
               const int32_t *__restrict__ scol, const TV *__restrict__ sval,
               const T *__restrict__ X, int ldx, T *__restrict__ Y, int ldy,
@@ -148,30 +148,53 @@ k_strip_spmm (int64_t n, int64_t nstrips, const int64_t *__restrict__ sptr,
 #pragma unroll
       for (int e = 0; e < W; e++) acc[r][h][e] = T (0);
   const int64_t k0 = sptr[s], k1 = sptr[s + 1];
+  /* two-deep software pipeline: the next entry's X packs and values are
+   * loaded before the current entry's FMAs, so each warp keeps two
+   * gathers in flight */
+  T va[R], vb[R];
+  Pack<T> xa[CH], xb[CH];
+  auto fetch = [&] (int64_t k, int c, T (&v)[R], Pack<T> (&x)[CH]) {
+    const TV *vp = sval + k * R;
+    if constexpr (sizeof (TV) == 8 && R % 2 == 0) {
+#pragma unroll
+      for (int r = 0; r < R; r += 2) {
+        const double2 d = __ldg (reinterpret_cast<const double2 *> (vp + r));
+        v[r] = (T) d.x;
+        v[r + 1] = (T) d.y;
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; r++) v[r] = (T) __ldg (vp + r);
+    }
+    const T *xr = X + (int64_t) c * ldx;
+#pragma unroll
+    for (int h = 0; h < CH; h++) {
+      const int vi = pbase + lane + 32 * h;
+      x[h] = vi < nvec ? ldp_nc (xr + vi * W) : pzero<T> ();
+    }
+  };
+  auto apply = [&] (const T (&v)[R], const Pack<T> (&x)[CH]) {
+#pragma unroll
+    for (int h = 0; h < CH; h++)
+#pragma unroll
+      for (int r = 0; r < R; r++)
+#pragma unroll
+        for (int e = 0; e < W; e++)
+          acc[r][h][e] = fma (v[r], x[h].v[e], acc[r][h][e]);
+  };
   for (int64_t kb = k0; kb < k1; kb += 32) {
     const int cnt = (int) ((k1 - kb) < 32 ? (k1 - kb) : 32);
     const int mycol = lane < cnt ? scol[kb + lane] : 0;
-#pragma unroll 2
-    for (int t = 0; t < cnt; t++) {
-      const int c = __shfl_sync (0xffffffffu, mycol, t);
-      const TV *vp = sval + (kb + t) * R;
-      T v[R];
-#pragma unroll
-      for (int r = 0; r < R; r++) v[r] = (T) __ldg (vp + r);
-      const T *xr = X + (int64_t) c * ldx;
-#pragma unroll
-      for (int h = 0; h < CH; h++) {
-        const int vi = pbase + lane + 32 * h;
-        if (vi < nvec) {
-          const Pack<T> x = ldp_nc (xr + vi * W);
-#pragma unroll
-          for (int r = 0; r < R; r++)
-#pragma unroll
-            for (int e = 0; e < W; e++)
-              acc[r][h][e] = fma (v[r], x.v[e], acc[r][h][e]);
-        }
-      }
+    fetch (kb, __shfl_sync (0xffffffffu, mycol, 0), va, xa);
+    int t = 0;
+    for (; t + 1 < cnt; t += 2) {
+      fetch (kb + t + 1, __shfl_sync (0xffffffffu, mycol, t + 1), vb, xb);
+      apply (va, xa);
+      if (t + 2 < cnt)
+        fetch (kb + t + 2, __shfl_sync (0xffffffffu, mycol, t + 2), va, xa);
+      apply (vb, xb);
     }
+    if (t < cnt) apply (va, xa);
   }
   const int64_t r0 = s * R;
 #pragma unroll
@@ -297,9 +320,10 @@ static int
 strip_dispatch (const StripForm &S, const TV *sval, const T *X, int ldx, T *Y,
                 int ldy, int nvec, cudaStream_t s)
 {
-  /* one warp per strip and slice of 32 CH packs; CH = 2 keeps the R x CH
-   * accumulators in registers at R = 8 */
-  constexpr int CH = (R >= 8) ? 2 : 4;
+  /* one warp per strip and slice of 32 CH packs; R x CH = 8 keeps the
+   * accumulators and the two pipeline stages within 128 registers (two
+   * CTAs of 8 warps per SM) */
+  constexpr int CH = 8 / R;
   const int slices = (nvec + 32 * CH - 1) / (32 * CH);
   const int64_t ctas = (S.nstrips + 7) / 8;
   LGH_CHECK (ctas < (int64_t) INT32_MAX && slices < 65536, LGH_ERR_ARG_OUTOFRANGE,

@@ -92,6 +92,10 @@ struct lgh_glr
   int have_wz = 0;
   /* workspace and captured graph of the many-shift combination (batch.cu) */
   lgh::ShiftPlan *splan = nullptr;
+  /* the communicator of a column-sharded build (size 0: one device) and
+   * its library-owned exchange buffers */
+  lgh_comm_t comm{};
+  lgh::DBuf<char> xsend, xrecv;
   lgh_glr_stats_t stats{};
 };
 

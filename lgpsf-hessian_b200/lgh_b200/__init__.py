@@ -21,6 +21,7 @@ c_dbl_p = ctypes.POINTER(ctypes.c_double)
 
 LGH_MEM_HOST, LGH_MEM_DEVICE = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
+CHECK_PROJ, CHECK_APPLY = 0, 1
 PC_AMG, PC_JACOBI = 0, 1
 ERR_NAMES = {0: "SUCCESS", 55: "ERR_MEM", 56: "ERR_SUP", 58: "ERR_ORDER",
              60: "ERR_ARG_SIZ", 62: "ERR_ARG_WRONG",
@@ -78,7 +79,20 @@ class PriorMatOpts(ctypes.Structure):
 class ExecOpts(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int),
                 ("inner_rtol", ctypes.c_double),
-                ("verbose", ctypes.c_int), ("rank_cap", ctypes.c_int)]
+                ("verbose", ctypes.c_int), ("rank_cap", ctypes.c_int),
+                ("check_form", ctypes.c_int)]
+
+
+ALLGATHER_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_size_t, ctypes.c_void_p)
+
+
+class Comm(ctypes.Structure):
+    """lgh_comm_t: the communicator of a column-sharded build."""
+    _fields_ = [("rank", ctypes.c_int), ("size", ctypes.c_int),
+                ("send", ctypes.c_void_p), ("recv", ctypes.c_void_p),
+                ("bytes", ctypes.c_size_t), ("allgather", ALLGATHER_FN),
+                ("ctx", ctypes.c_void_p)]
 
 
 class ServerOpts(ctypes.Structure):
@@ -217,6 +231,16 @@ SIGNATURES = {
     "lgh_glr_eigs": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_int),
                                     ctypes.POINTER(c_dbl_p)]),
     "lgh_exec_opts_default": (ExecOpts, []),
+    "lgh_cols_range": (None, [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P]),
+    "lgh_cols_exchange_bytes": (ctypes.c_size_t, [I64, ctypes.c_int,
+                                                  ctypes.c_int]),
+    "lgh_glr_compute_cols": (ctypes.c_int, [P, P, ctypes.POINTER(GlrOpts),
+                                            ctypes.POINTER(ExecOpts),
+                                            ctypes.POINTER(Comm),
+                                            ctypes.POINTER(P),
+                                            ctypes.POINTER(GlrReport)]),
+    "lgh_comm_local_create": (ctypes.c_int, [ctypes.c_int, P]),
+    "lgh_comm_local_destroy": (None, [P]),
     "lgh_glr_compute_ex": (ctypes.c_int, [P, P, ctypes.POINTER(GlrOpts),
                                           ctypes.POINTER(ExecOpts),
                                           ctypes.POINTER(P),
@@ -522,13 +546,21 @@ class Prior:
 class Glr:
     """lgh_glr_t: build, extend and the downstream operations."""
 
-    def __init__(self, B, prior, opts=None, exec=None):
+    def __init__(self, B, prior, opts=None, exec=None, comm=None):
         L = load()
         self.h = P()
         self.B, self.prior = B, prior
         o = opts if opts is not None else glr_opts()
         rep = GlrReport()
-        if exec is None:
+        if comm is not None:
+            e = exec if exec is not None else L.lgh_exec_opts_default()
+            self._comm = comm
+            _chk(L.lgh_glr_compute_cols(B.h, prior.h, ctypes.byref(o),
+                                        ctypes.byref(e), ctypes.byref(comm),
+                                        ctypes.byref(self.h),
+                                        ctypes.byref(rep)),
+                 "lgh_glr_compute_cols")
+        elif exec is None:
             _chk(L.lgh_glr_compute(B.h, prior.h, ctypes.byref(o),
                                    ctypes.byref(self.h), ctypes.byref(rep)),
                  "lgh_glr_compute")
@@ -889,6 +921,26 @@ def test_spmm(A, X, fp32=False):
     _chk(load().lgh_test_spmm(A.h, X.shape[1], X.ctypes.data, Y.ctypes.data,
                               1 if fp32 else 0), "lgh_test_spmm")
     return Y
+
+
+def cols_range(w, rank, size):
+    """Columns [c0, c1) of a width-w block owned by rank of size."""
+    c0, c1 = ctypes.c_int(), ctypes.c_int()
+    load().lgh_cols_range(w, rank, size, ctypes.addressof(c0),
+                          ctypes.addressof(c1))
+    return c0.value, c1.value
+
+
+def local_comms(size):
+    """size in-process communicators (ranks as threads on one device)."""
+    arr = (Comm * size)()
+    _chk(load().lgh_comm_local_create(size, ctypes.addressof(arr)),
+         "lgh_comm_local_create")
+    return arr
+
+
+def free_local_comms(arr):
+    load().lgh_comm_local_destroy(ctypes.addressof(arr))
 
 
 def test_spmm_strip(A, X, fp32=False, R=0):

@@ -53,7 +53,8 @@ def test_struct_layouts_match_c_compiler(tmp_path):
                "lgh_glr_correct_opts_t": lgh_b200.CorrectOpts,
                "lgh_glr_correct_report_t": lgh_b200.CorrectReport,
                "lgh_server_opts_t": lgh_b200.ServerOpts,
-               "lgh_server_stats_t": lgh_b200.ServerStats}
+               "lgh_server_stats_t": lgh_b200.ServerStats,
+               "lgh_comm_t": lgh_b200.Comm}
     lines = ['#include <stdio.h>', '#include <stddef.h>',
              '#include "lgh_b200.h"', 'int main(void){']
     for cname, py in structs.items():

@@ -64,3 +64,54 @@ def test_sketch_rows_partition_independent(cuda_device):
         y = Y.cpu().numpy()
         assert np.array_equal(y[:, :k], full[i0:i0 + n])
         assert not y[:, k:].any()
+
+
+def test_cols_sharded_build_two_ranks_on_one_device(cuda_device):
+    """The column-sharded build with two ranks run as threads on one GPU
+    (the in-process communicator: a host barrier and device copies, no
+    kernel waits on another rank).  Each rank owns half of the sketch
+    columns; after the build both ranks hold the same object, equal to
+    the one-device build on the same inputs (same hashed sketch), and the
+    sharded extension equals the one-device extension."""
+    import threading
+    cfg = P.grid_problem("c1")
+    o = L.glr_opts(ell=60, seed=0, trunc_rel=1e-3, check=1)
+    one = {}
+
+    def objs():
+        B, Z = L.Mat(cfg["B"]), L.Mat(cfg["Z"])
+        pr = L.Prior(Z=Z, mass=cfg["mass"], opts=L.prior_opts(ksp_rtol=1e-12))
+        return B, Z, pr
+
+    keep1 = objs()
+    g1 = L.Glr(keep1[0], keep1[2], o)
+    comms = L.local_comms(2)
+    res, errs = [None, None], []
+
+    def rank(r):
+        try:
+            keep = objs()
+            g = L.Glr(keep[0], keep[2], o, comm=comms[r])
+            rep0 = dict(g.report)
+            g.extend(20)
+            res[r] = (g.eigs(), g.U(), rep0, keep, g)
+        except Exception as e:             # reported below
+            errs.append(repr(e))
+
+    th = [threading.Thread(target=rank, args=(r,)) for r in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(timeout=600)
+    assert not errs, errs
+    (l0, U0, rep0, _, _), (l1, U1, rep1, _, _) = res
+    assert np.array_equal(l0, l1) and np.array_equal(U0, U1)
+    lo = g1.eigs()
+    assert len(lo) == rep0["kept"]
+    assert abs(rep0["resid_max"] - g1.report["resid_max"]) \
+        < 1e-3 * g1.report["resid_max"]
+    g1.extend(20)
+    l1x = g1.eigs()
+    assert len(l1x) == len(l0)
+    assert np.max(np.abs(l0 - l1x) / l1x) < 1e-10
+    L.free_local_comms(comms)
