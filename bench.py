@@ -71,7 +71,7 @@ def parse():
     ap.add_argument("--serve-rates", default="",
                     help="comma-separated request rates for --config c5")
     ap.add_argument("--kernel-case", default="",
-                    choices=["", "zsolve", "spmm", "build"],
+                    choices=["", "zsolve", "spmm", "build", "batch"],
                     help="run one device case and print the library's "
                          "per-kernel event timing (for ncu captures of "
                          "single kernels): zsolve = a blocked Z-solve of a "
@@ -81,6 +81,10 @@ def parse():
     ap.add_argument("--kc-width", type=int, default=220)
     ap.add_argument("--kc-rtol", type=float, default=1e-10)
     ap.add_argument("--kc-fp32", action="store_true")
+    ap.add_argument("--kc-shifts", type=int, default=8,
+                    help="batch case: shifts (log-spaced in [1e-3, 1e3])")
+    ap.add_argument("--kc-rank", type=int, default=200,
+                    help="batch case: ell (rank cap = ell - 20)")
     ap.add_argument("--config", default="c2", choices=["c2", "c3", "c4", "c5"],
                     help="c2: the headline job (default); c3 / c4: the "
                          "mixed-precision 3D extend and the batched-shift "
@@ -951,6 +955,38 @@ def run_kernel_case(args):
         X = np.random.default_rng(0).standard_normal((N, w))
         L.test_spmm(B, X, fp32=args.kc_fp32)
         info = {}
+    elif args.kernel_case == "batch":
+        # many-shift batched solves (w right-hand sides, --kc-shifts
+        # shifts) on an FP64 and a mixed object: the fused combination
+        # kernels, timed per call after a tuning call and a graph capture
+        import torch
+        B, Z = L.Mat(cfg["B"]), L.Mat(cfg["Z"])
+        pr = L.Prior(Z=Z, mass=cfg["mass"],
+                     opts=L.prior_opts(ksp_rtol=args.kc_rtol))
+        ell = args.kc_rank
+        cs = np.logspace(-3, 3, args.kc_shifts)
+        R = L.DeviceBlock(N, w, np.random.default_rng(8).standard_normal(
+            (N, w)))
+        Xo = L.DeviceBlock(N, w * len(cs))
+        Lb = L.load()
+        info = {}
+        for name, prec in (("fp64", L.PREC_FP64), ("mixed", L.PREC_MIXED)):
+            g = L.Glr(B, pr, L.glr_opts(ell=ell, seed=0, trunc_rel=0.0,
+                                        check=0),
+                      exec=L.exec_opts(precision=prec, rank_cap=ell - 20))
+            ts = []
+            for _ in range(4):
+                ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+                ev[0].record()
+                L._chk(Lb.lgh_glr_solve_batch(
+                    g.h, len(cs), cs.ctypes.data_as(L.c_dbl_p), w, R.ptr(),
+                    N, Xo.ptr(), N), "solve_batch")
+                ev[1].record()
+                torch.cuda.synchronize()
+                ts.append(ev[0].elapsed_time(ev[1]))
+            info[name] = {"call_ms": [round(t, 3) for t in ts],
+                          "batch": g.batch_info()}
+            del g
     else:
         B, Z = L.Mat(cfg["B"]), L.Mat(cfg["Z"])
         pr = L.Prior(Z=Z, mass=cfg["mass"],

@@ -623,6 +623,11 @@ long lgh_launch_count (void);
  * kernel launches.                                                        */
 int lgh_runtime_counters (double *out);
 
+/* Throughput probes (the roofline denominators beside the measured copy
+ * bandwidth): out[0..3] = FP64 FMA TFLOP/s, FP32 FMA TFLOP/s, FP64
+ * mma.sync TFLOP/s, L2-resident read GB/s.                                */
+int lgh_probe_peaks (double *out);
+
 /* Last error message of the calling thread (empty if none).              */
 const char *lgh_last_error (void);
 

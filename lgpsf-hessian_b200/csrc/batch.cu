@@ -77,9 +77,14 @@ struct ShiftPlan
   double *cph = nullptr;  /* pinned shifts */
   /* the captured sequence and what it was captured for */
   cudaStream_t cs = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  int g_kind = -1, g_nshift = 0, g_m = 0, g_variant = -1;
-  const double *g_W = nullptr, *g_lam = nullptr;
+  /* one captured tail per kind (0 solve, 1 sample) and what it was
+   * captured for */
+  struct Captured
+  {
+    cudaGraphExec_t exec = nullptr;
+    int nshift = 0, m = 0, variant = -1;
+    const double *W = nullptr, *lam = nullptr;
+  } cap[2];
   long replays = 0, captures = 0;
   int last_variant = -1;
   /* the tensor-core form (mixed-precision objects): W split once, the
@@ -94,7 +99,7 @@ struct ShiftPlan
 
   ~ShiftPlan ()
   {
-    if (exec) cudaGraphExecDestroy (exec);
+    drop_graph ();
     if (cs) cudaStreamDestroy (cs);
     if (ph) cudaFreeHost (ph);
     if (cph) cudaFreeHost (cph);
@@ -102,9 +107,10 @@ struct ShiftPlan
 
   void drop_graph ()
   {
-    if (exec) cudaGraphExecDestroy (exec);
-    exec = nullptr;
-    g_kind = -1;
+    for (auto &c : cap) {
+      if (c.exec) cudaGraphExecDestroy (c.exec);
+      c = Captured ();
+    }
   }
 
   int ensure (int64_t n_, int m_, int kept_, int nshift)
@@ -259,10 +265,11 @@ shift_plan_combine (ShiftPlan *P, lgh_glr_t *g, int kind, int nshift,
   P->ph->out = x;
   P->ph->ldo = ldx;
   memcpy (P->cph, c_host, nshift * sizeof (double));
-  if (P->exec == nullptr || P->g_kind != kind || P->g_nshift != nshift
-      || P->g_m != m || P->g_variant != variant || P->g_W != g->Wz.p
-      || P->g_lam != g->lam_d.p) {
-    P->drop_graph ();
+  ShiftPlan::Captured &C = P->cap[kind & 1];
+  if (C.exec == nullptr || C.nshift != nshift || C.m != m
+      || C.variant != variant || C.W != g->Wz.p || C.lam != g->lam_d.p) {
+    if (C.exec) cudaGraphExecDestroy (C.exec);
+    C = ShiftPlan::Captured ();
     /* captured on the plan's own stream; the instantiated graph is then
      * launched on the library's stream, after the work queued there */
     cudaGraph_t gr = nullptr;
@@ -271,26 +278,25 @@ shift_plan_combine (ShiftPlan *P, lgh_glr_t *g, int kind, int nshift,
       rc = enqueue_tail (*P, g, kind, nshift, variant, m, P->cs);
       const cudaError_t ce = cudaStreamEndCapture (P->cs, &gr);
       if (!rc && (ce != cudaSuccess || gr == nullptr
-                  || cudaGraphInstantiate (&P->exec, gr, 0) != cudaSuccess)) {
-        P->exec = nullptr;
+                  || cudaGraphInstantiate (&C.exec, gr, 0) != cudaSuccess)) {
+        C.exec = nullptr;
       }
       if (gr) cudaGraphDestroy (gr);
     }
     cudaGetLastError ();
     if (rc) return rc;
-    if (P->exec) {
-      P->g_kind = kind;
-      P->g_nshift = nshift;
-      P->g_m = m;
-      P->g_variant = variant;
-      P->g_W = g->Wz.p;
-      P->g_lam = g->lam_d.p;
+    if (C.exec) {
+      C.nshift = nshift;
+      C.m = m;
+      C.variant = variant;
+      C.W = g->Wz.p;
+      C.lam = g->lam_d.p;
       P->captures++;
     }
   }
   P->last_variant = variant;
-  if (P->exec) {
-    LGH_CUDA (cudaGraphLaunch (P->exec, s));
+  if (C.exec) {
+    LGH_CUDA (cudaGraphLaunch (C.exec, s));
     P->replays++;
   } else {
     /* capture unavailable: the same sequence, eagerly */

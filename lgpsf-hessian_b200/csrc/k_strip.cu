@@ -126,8 +126,11 @@ k_scan_counts (int64_t m, const int64_t *__restrict__ counts,
 
 /* Y (rows r0 .. r0 + R) = strip s times X over the packs of this warp's
  * column slice: lane l owns packs l + 32 h, h < CH, of the slice starting
- * at pack 32 CH blockIdx.y.  Each entry: one gathered X pack per owned
- * pack, applied to the R rows. */
+ * at pack 32 CH blockIdx.y.  The gathers are latency-bound, so the kernel
+ * is built for bytes in flight: a warp stages the columns and values of 32
+ * union entries in shared memory with coalesced loads, then issues the X
+ * gathers of D entries (D CH = 8 packs per lane) before any of their FMAs,
+ * reading the values back as shared-memory broadcasts. */
 template <typename T, typename TV, int R, int CH>
 __global__ void __launch_bounds__ (256, 2)
 k_strip_spmm (int64_t n, int64_t nstrips, const int64_t *__restrict__ sptr,
@@ -136,8 +139,11 @@ k_strip_spmm (int64_t n, int64_t nstrips, const int64_t *__restrict__ sptr,
               int nvec)
 {
   constexpr int W = Pack<T>::W;
-  const int lane = threadIdx.x & 31;
-  const int64_t s = (int64_t) blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  constexpr int D = 8 / CH;
+  __shared__ TV sv_s[8][32 * R];
+  __shared__ int sc_s[8][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int64_t s = (int64_t) blockIdx.x * (blockDim.x >> 5) + wid;
   if (s >= nstrips) return;
   const int pbase = blockIdx.y * 32 * CH;
   T acc[R][CH][W];
@@ -148,53 +154,45 @@ k_strip_spmm (int64_t n, int64_t nstrips, const int64_t *__restrict__ sptr,
 #pragma unroll
       for (int e = 0; e < W; e++) acc[r][h][e] = T (0);
   const int64_t k0 = sptr[s], k1 = sptr[s + 1];
-  /* two-deep software pipeline: the next entry's X packs and values are
-   * loaded before the current entry's FMAs, so each warp keeps two
-   * gathers in flight */
-  T va[R], vb[R];
-  Pack<T> xa[CH], xb[CH];
-  auto fetch = [&] (int64_t k, int c, T (&v)[R], Pack<T> (&x)[CH]) {
-    const TV *vp = sval + k * R;
-    if constexpr (sizeof (TV) == 8 && R % 2 == 0) {
-#pragma unroll
-      for (int r = 0; r < R; r += 2) {
-        const double2 d = __ldg (reinterpret_cast<const double2 *> (vp + r));
-        v[r] = (T) d.x;
-        v[r + 1] = (T) d.y;
-      }
-    } else {
-#pragma unroll
-      for (int r = 0; r < R; r++) v[r] = (T) __ldg (vp + r);
-    }
-    const T *xr = X + (int64_t) c * ldx;
-#pragma unroll
-    for (int h = 0; h < CH; h++) {
-      const int vi = pbase + lane + 32 * h;
-      x[h] = vi < nvec ? ldp_nc (xr + vi * W) : pzero<T> ();
-    }
-  };
-  auto apply = [&] (const T (&v)[R], const Pack<T> (&x)[CH]) {
-#pragma unroll
-    for (int h = 0; h < CH; h++)
-#pragma unroll
-      for (int r = 0; r < R; r++)
-#pragma unroll
-        for (int e = 0; e < W; e++)
-          acc[r][h][e] = fma (v[r], x[h].v[e], acc[r][h][e]);
-  };
+  TV *sv = sv_s[wid];
+  int *sc = sc_s[wid];
   for (int64_t kb = k0; kb < k1; kb += 32) {
     const int cnt = (int) ((k1 - kb) < 32 ? (k1 - kb) : 32);
-    const int mycol = lane < cnt ? scol[kb + lane] : 0;
-    fetch (kb, __shfl_sync (0xffffffffu, mycol, 0), va, xa);
-    int t = 0;
-    for (; t + 1 < cnt; t += 2) {
-      fetch (kb + t + 1, __shfl_sync (0xffffffffu, mycol, t + 1), vb, xb);
-      apply (va, xa);
-      if (t + 2 < cnt)
-        fetch (kb + t + 2, __shfl_sync (0xffffffffu, mycol, t + 2), va, xa);
-      apply (vb, xb);
+    /* stage: lane l takes entry kb + l (its column and R values) */
+    sc[lane] = lane < cnt ? scol[kb + lane] : 0;
+#pragma unroll
+    for (int r = 0; r < R; r++)
+      sv[lane * R + r] = lane < cnt ? __ldg (sval + (kb + lane) * R + r) : TV (0);
+    __syncwarp ();
+    for (int t0 = 0; t0 < cnt; t0 += D) {
+      Pack<T> x[D][CH];
+#pragma unroll
+      for (int d = 0; d < D; d++) {
+        const int t = t0 + d;
+        const T *xr = X + (int64_t) sc[t < cnt ? t : 0] * ldx;
+#pragma unroll
+        for (int h = 0; h < CH; h++) {
+          const int vi = pbase + lane + 32 * h;
+          x[d][h] = (t < cnt && vi < nvec) ? ldp_nc (xr + vi * W) : pzero<T> ();
+        }
+      }
+#pragma unroll
+      for (int d = 0; d < D; d++) {
+        const int t = t0 + d;
+        if (t < cnt) {
+#pragma unroll
+          for (int r = 0; r < R; r++) {
+            const T v = (T) sv[t * R + r];
+#pragma unroll
+            for (int h = 0; h < CH; h++)
+#pragma unroll
+              for (int e = 0; e < W; e++)
+                acc[r][h][e] = fma (v, x[d][h].v[e], acc[r][h][e]);
+          }
+        }
+      }
     }
-    if (t < cnt) apply (va, xa);
+    __syncwarp ();
   }
   const int64_t r0 = s * R;
 #pragma unroll

@@ -304,6 +304,7 @@ SIGNATURES = {
     "lgh_test_rng_state": (ctypes.c_int, [ctypes.c_uint64, I64, I64,
                                           ctypes.c_int, P]),
     "lgh_glr_batch_info": (ctypes.c_int, [P, P, P, P, P]),
+    "lgh_probe_peaks": (ctypes.c_int, [P]),
     "lgh_test_spmm": (ctypes.c_int, [P, ctypes.c_int, P, P, ctypes.c_int]),
     "lgh_test_spmm_strip": (ctypes.c_int, [P, ctypes.c_int, P, P, ctypes.c_int,
                                            ctypes.c_int, P]),
@@ -921,6 +922,14 @@ def test_spmm(A, X, fp32=False):
     _chk(load().lgh_test_spmm(A.h, X.shape[1], X.ctypes.data, Y.ctypes.data,
                               1 if fp32 else 0), "lgh_test_spmm")
     return Y
+
+
+def probe_peaks():
+    """FP64 / FP32 FMA, FP64 mma.sync TFLOP/s and L2 read GB/s."""
+    out = np.zeros(4)
+    _chk(load().lgh_probe_peaks(out.ctypes.data), "lgh_probe_peaks")
+    return dict(fp64_fma_tflops=out[0], fp32_fma_tflops=out[1],
+                fp64_mma_tflops=out[2], l2_read_gbs=out[3])
 
 
 def cols_range(w, rank, size):
