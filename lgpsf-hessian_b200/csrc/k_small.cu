@@ -332,9 +332,14 @@ launch_syev_jacobi (int n, double *A, double *V, double *w, double *A2,
    * needs): a round's element updates are the larger part of its time, so
    * more CTAs shorten it despite the wider barrier (measured at n = 220:
    * 15.7 ms on 48 CTAs, 11.6 ms on 296; at n = 520: 65 ms on 148 CTAs,
-   * 51 ms on 296); the result does not depend on the grid */
-  int grid = (int) std::min<int64_t> (2 * (int64_t) num_sms (),
-                                      (int64_t) num_sms () * per_sm);
+   * 51 ms on 296); the result does not depend on the grid.  Small
+   * problems keep about one CTA per 128 matrix entries (n = 220 still
+   * gets 296), so that a 10 x 10 eigensolve does not pay a 296-CTA
+   * barrier every round. */
+  const int64_t by_size = std::max<int64_t> (1, ((int64_t) n * n + 127) / 128);
+  int grid = (int) std::min<int64_t> (std::min<int64_t> (2 * (int64_t) num_sms (),
+                                                         (int64_t) num_sms () * per_sm),
+                                      by_size);
   JacobiCtl *ctl;
   LGH_TRY (dalloc ((void **) &ctl, sizeof (JacobiCtl)));
   cudaMemsetAsync (ctl, 0, sizeof (JacobiCtl), s);
