@@ -559,16 +559,23 @@ mat_release (lgh_Mat A)
   delete A;
 }
 
+int
+mat_prepare_block (lgh_Mat A, int w)
+{
+  if (w >= 8 && !A->strips_built) {
+    LGH_TRY (strip_build (A->csr, A->strip_R, A->strips));
+    A->strips_built = 1;
+  }
+  return 0;
+}
+
 template <typename T>
 int
 mat_mult_block (lgh_Mat A, const T *X, int ldx, T *Y, int ldy, int w,
                 cudaStream_t s)
 {
   if (w >= 8) {
-    if (!A->strips_built) {
-      LGH_TRY (strip_build (A->csr, A->strip_R, A->strips));
-      A->strips_built = 1;
-    }
+    LGH_TRY (mat_prepare_block (A, w));
     return launch_strip_spmm<T> (A->strips, X, ldx, Y, ldy, w, s);
   }
   return launch_spmm<T> (A->csr, X, ldx, Y, ldy, w, s);

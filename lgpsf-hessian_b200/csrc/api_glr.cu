@@ -208,6 +208,7 @@ apply_F (lgh_glr_t *g, int w, const T *X, int ldx, T *Y, int ldy, T *W,
   double t1 = wall ();
   static thread_local EventRing ring;
   const bool timing = ktime_on ();
+  LGH_TRY (mat_prepare_block (g->B, w));   /* once per operator */
   if (timing) LGH_TRY (ring.record (s));
   LGH_TRY (mat_mult_block<T> (g->B, W, ldw, Y, ldy, w, s));
   if (timing) LGH_TRY (ring.record (s));

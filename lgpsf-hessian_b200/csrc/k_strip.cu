@@ -139,8 +139,8 @@ k_strip_spmm (int64_t n, int64_t nstrips, const int64_t *__restrict__ sptr,
               int nvec)
 {
   constexpr int W = Pack<T>::W;
-  constexpr int D = 8 / CH;
-  __shared__ TV sv_s[8][32 * R];
+  constexpr int D = (8 / CH) > 0 ? 8 / CH : 1;
+  __shared__ __align__ (16) TV sv_s[8][32 * R];
   __shared__ int sc_s[8][32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int64_t s = (int64_t) blockIdx.x * (blockDim.x >> 5) + wid;
@@ -180,15 +180,35 @@ k_strip_spmm (int64_t n, int64_t nstrips, const int64_t *__restrict__ sptr,
       for (int d = 0; d < D; d++) {
         const int t = t0 + d;
         if (t < cnt) {
+          /* the entry's R values as 16-byte shared broadcasts */
+          T v[R];
+          if constexpr (sizeof (TV) == 8) {
 #pragma unroll
-          for (int r = 0; r < R; r++) {
-            const T v = (T) sv[t * R + r];
+            for (int r = 0; r < R; r += 2) {
+              const double2 u = *reinterpret_cast<const double2 *> (sv + t * R + r);
+              v[r] = (T) u.x;
+              v[r + 1] = (T) u.y;
+            }
+          } else if constexpr (R % 4 == 0) {
+#pragma unroll
+            for (int r = 0; r < R; r += 4) {
+              const float4 u = *reinterpret_cast<const float4 *> (sv + t * R + r);
+              v[r] = (T) u.x;
+              v[r + 1] = (T) u.y;
+              v[r + 2] = (T) u.z;
+              v[r + 3] = (T) u.w;
+            }
+          } else {
+#pragma unroll
+            for (int r = 0; r < R; r++) v[r] = (T) sv[t * R + r];
+          }
+#pragma unroll
+          for (int r = 0; r < R; r++)
 #pragma unroll
             for (int h = 0; h < CH; h++)
 #pragma unroll
               for (int e = 0; e < W; e++)
-                acc[r][h][e] = fma (v, x[d][h].v[e], acc[r][h][e]);
-          }
+                acc[r][h][e] = fma (v[r], x[d][h].v[e], acc[r][h][e]);
         }
       }
     }
@@ -275,12 +295,13 @@ strip_build (const Csr &A, int force_R, StripForm &S)
   DBuf<unsigned long long> tot;
   LGH_TRY (tot.alloc (4));
   LGH_CUDA (cudaMemsetAsync (tot.p, 0, 4 * sizeof (unsigned long long), s));
-  DBuf<int64_t> counts;
-  LGH_TRY (counts.alloc ((size_t) (n + 1) / 2 + 1));
+  DBuf<int64_t> cnt[3];
+  for (int c = 0; c < 3; c++)
+    LGH_TRY (cnt[c].alloc ((size_t) (n + cand[c] - 1) / cand[c] + 1));
   int R = force_R;
   if (R <= 0) {
     for (int c = 0; c < 3; c++)
-      LGH_TRY (merge_any (cand[c], A, (n + cand[c] - 1) / cand[c], counts.p,
+      LGH_TRY (merge_any (cand[c], A, (n + cand[c] - 1) / cand[c], cnt[c].p,
                           tot.p + c, nullptr, s));
     unsigned long long th[3];
     LGH_CUDA (cudaMemcpyAsync (th, tot.p, sizeof (th), cudaMemcpyDeviceToHost, s));
@@ -295,10 +316,12 @@ strip_build (const Csr &A, int force_R, StripForm &S)
   S.n = n;
   S.nstrips = (n + R - 1) / R;
   S.nnz = A.nnz;
-  /* the chosen height's union lengths (the candidates share one array) */
-  LGH_TRY (merge_any (R, A, S.nstrips, counts.p, tot.p + 3, nullptr, s));
+  const int ci = R == 2 ? 0 : (R == 4 ? 1 : 2);
+  int64_t *counts = cnt[ci].p;
+  if (force_R > 0)   /* only the forced height was not counted above */
+    LGH_TRY (merge_any (R, A, S.nstrips, counts, tot.p + ci, nullptr, s));
   unsigned long long nent = 0;
-  LGH_CUDA (cudaMemcpyAsync (&nent, tot.p + 3, sizeof (nent),
+  LGH_CUDA (cudaMemcpyAsync (&nent, tot.p + ci, sizeof (nent),
                              cudaMemcpyDeviceToHost, s));
   LGH_CUDA (cudaStreamSynchronize (s));
   S.nent = (int64_t) nent;
@@ -306,7 +329,7 @@ strip_build (const Csr &A, int force_R, StripForm &S)
   LGH_TRY (dalloc ((void **) &S.scol, (size_t) S.nent * sizeof (int32_t) + 16));
   LGH_TRY (dalloc ((void **) &S.sval, (size_t) S.nent * R * sizeof (double) + 16));
   LGH_TRY (dalloc ((void **) &S.sval32, (size_t) S.nent * R * sizeof (float) + 16));
-  k_scan_counts<<<1, 1024, 0, s>>> (S.nstrips, counts.p, S.sptr);
+  k_scan_counts<<<1, 1024, 0, s>>> (S.nstrips, counts, S.sptr);
   LGH_LAUNCH_CHECK ();
   LGH_TRY (merge_any (R, A, S.nstrips, nullptr, nullptr, &S, s));
   LGH_CUDA (cudaStreamSynchronize (s));
@@ -318,10 +341,10 @@ static int
 strip_dispatch (const StripForm &S, const TV *sval, const T *X, int ldx, T *Y,
                 int ldy, int nvec, cudaStream_t s)
 {
-  /* one warp per strip and slice of 32 CH packs; R x CH = 8 keeps the
-   * accumulators and the two pipeline stages within 128 registers (two
-   * CTAs of 8 warps per SM) */
-  constexpr int CH = 8 / R;
+  /* one warp per strip and slice of 32 CH packs: R x CH = 16 accumulator
+   * packs and 8 packs of gathers in flight per lane within 128 registers
+   * (two CTAs of 8 warps per SM) */
+  constexpr int CH = 16 / R;
   const int slices = (nvec + 32 * CH - 1) / (32 * CH);
   const int64_t ctas = (S.nstrips + 7) / 8;
   LGH_CHECK (ctas < (int64_t) INT32_MAX && slices < 65536, LGH_ERR_ARG_OUTOFRANGE,

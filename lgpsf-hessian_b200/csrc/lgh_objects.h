@@ -108,6 +108,8 @@ int mat_mult_vec (lgh_Mat A, const double *x, double *y);
 template <typename T>
 int mat_mult_block (lgh_Mat A, const T *X, int ldx, T *Y, int ldy, int w,
                     cudaStream_t s);
+/* build the strip form of A now if a width-w product will use it */
+int mat_prepare_block (lgh_Mat A, int w);
 void prior_ref (lgh_prior_t *p);
 int prior_applyZ (lgh_prior_t *p, const double *x, double *y);
 int prior_solve_vec (lgh_prior_t *p, const double *x, const double *s_in,

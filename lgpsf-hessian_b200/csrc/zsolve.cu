@@ -422,13 +422,17 @@ k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ vdv,
 
 /* ---- PCG with an explicit preconditioner z = V(r) (the AMG V-cycle):
  * p_new = z + beta p_old on the fly at neighbours, q = Z p_new, (p, q) ---- */
-template <typename T, int CH>
+template <typename T, int CH, bool GIVEN = false>
 __global__ void __launch_bounds__ (ZS_THREADS, (CH * (16 / sizeof (T)) <= 8 ? 4 : 2))
 k_pcgx_pq (ZK z, const T *__restrict__ vals, const T *__restrict__ Zb,
            const T *__restrict__ Pold, T *__restrict__ Pnew,
            T *__restrict__ Qv, int ld, int nvec, int glog, int first,
            double *partA, unsigned *counter, double *scal, int *ival, int cap)
 {
+  /* GIVEN: the direction p_new is already in Pnew (formed by the
+   * streaming k_pcgx_pform); the product gathers p alone and Pnew is only
+   * read.  Otherwise p_new = z + beta p_old is formed at every neighbour
+   * row (first: p = z). */
   /* the next row's bounds and first G (column, value) pairs are loaded
    * while the current row's neighbours are gathered (software pipeline).
    * The per-column beta and each lane's running (p, q) sums live in
@@ -492,12 +496,19 @@ k_pcgx_pq (ZK z, const T *__restrict__ vals, const T *__restrict__ Zb,
         for (int h = 0; h < CH; h++) {
           const int vi = lane + h * G;
           if (vi < nvec) {
-            Pack<T> zj = ldp (Zb + (int64_t) c * ld + vi * W);
-            Pack<T> pj = first ? pzero<T> () : ldp (Pold + (int64_t) c * ld + vi * W);
-            const Pack<T> bt = *reinterpret_cast<const Pack<T> *> (bsm + vi * W);
+            if constexpr (GIVEN) {
+              const Pack<T> pj = ldp (Pnew + (int64_t) c * ld + vi * W);
 #pragma unroll
-            for (int e = 0; e < W; e++)
-              acc[h][e] = fma (v, fma (bt.v[e], pj.v[e], zj.v[e]), acc[h][e]);
+              for (int e = 0; e < W; e++)
+                acc[h][e] = fma (v, pj.v[e], acc[h][e]);
+            } else {
+              Pack<T> zj = ldp (Zb + (int64_t) c * ld + vi * W);
+              Pack<T> pj = first ? pzero<T> () : ldp (Pold + (int64_t) c * ld + vi * W);
+              const Pack<T> bt = *reinterpret_cast<const Pack<T> *> (bsm + vi * W);
+#pragma unroll
+              for (int e = 0; e < W; e++)
+                acc[h][e] = fma (v, fma (bt.v[e], pj.v[e], zj.v[e]), acc[h][e]);
+            }
           }
         }
       }
@@ -512,17 +523,22 @@ k_pcgx_pq (ZK z, const T *__restrict__ vals, const T *__restrict__ Zb,
     for (int h = 0; h < CH; h++) {
       const int vi = lane + h * G;
       if (vi < nvec) {
-        Pack<T> zi = ldp (Zb + i * ld + vi * W);
-        Pack<T> pi = first ? pzero<T> () : ldp (Pold + i * ld + vi * W);
         Pack<T> pn, q;
-        const Pack<T> bt = *reinterpret_cast<const Pack<T> *> (bsm + vi * W);
+        if constexpr (GIVEN) {
+          pn = ldp (Pnew + i * ld + vi * W);
+        } else {
+          Pack<T> zi = ldp (Zb + i * ld + vi * W);
+          Pack<T> pi = first ? pzero<T> () : ldp (Pold + i * ld + vi * W);
+          const Pack<T> bt = *reinterpret_cast<const Pack<T> *> (bsm + vi * W);
+#pragma unroll
+          for (int e = 0; e < W; e++) pn.v[e] = fma (bt.v[e], pi.v[e], zi.v[e]);
+        }
 #pragma unroll
         for (int e = 0; e < W; e++) {
-          pn.v[e] = fma (bt.v[e], pi.v[e], zi.v[e]);
           q.v[e] = acc[h][e];
           apq[vi * W + e] += (double) pn.v[e] * (double) q.v[e];
         }
-        stp (Pnew + i * ld + vi * W, pn);
+        if constexpr (!GIVEN) stp (Pnew + i * ld + vi * W, pn);
         stp (Qv + i * ld + vi * W, q);
       }
     }
@@ -574,6 +590,80 @@ k_pcgx_upd (int64_t n, int ld, T *__restrict__ X, T *__restrict__ R,
     }
     stp (X + o, x);
     stp (R + o, r);
+  }
+}
+
+/* the direction, streamed: p_new = z + beta p_old; with it the previous
+ * iteration's deferred x += alpha p_old (x is read by nothing inside an
+ * iteration, so the update moves here from k_pcgx_upd; the same FMA, so
+ * the same bits) */
+template <typename T>
+__global__ void
+k_pcgx_pform (int64_t n, int ld, const T *__restrict__ Zb,
+              const T *__restrict__ Pold, T *__restrict__ Pnew,
+              T *__restrict__ X, const double *beta, const double *alpha)
+{
+  constexpr int W = Pack<T>::W;
+  const int nvec = ld / W;
+  const int64_t total = n * nvec;
+  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t) gridDim.x * blockDim.x) {
+    const int64_t i = e / nvec;
+    const int vi = (int) (e - i * nvec);
+    const int64_t o = i * ld + vi * W;
+    const Pack<T> z = ldp (Zb + o), p = ldp (Pold + o);
+    Pack<T> x = ldp (X + o), pn;
+#pragma unroll
+    for (int k = 0; k < W; k++) {
+      pn.v[k] = fma ((T) beta[vi * W + k], p.v[k], z.v[k]);
+      x.v[k] = fma ((T) alpha[vi * W + k], p.v[k], x.v[k]);
+    }
+    stp (Pnew + o, pn);
+    stp (X + o, x);
+  }
+}
+
+/* r -= alpha q (the x half of the update is deferred to k_pcgx_pform) */
+template <typename T>
+__global__ void
+k_pcgx_updr (int64_t n, int ld, T *__restrict__ R, const T *__restrict__ Qv,
+             const double *alpha)
+{
+  constexpr int W = Pack<T>::W;
+  const int nvec = ld / W;
+  const int64_t total = n * nvec;
+  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t) gridDim.x * blockDim.x) {
+    const int64_t i = e / nvec;
+    const int vi = (int) (e - i * nvec);
+    const int64_t o = i * ld + vi * W;
+    Pack<T> r = ldp (R + o);
+    const Pack<T> q = ldp (Qv + o);
+#pragma unroll
+    for (int k = 0; k < W; k++) r.v[k] = fma (-(T) alpha[vi * W + k], q.v[k], r.v[k]);
+    stp (R + o, r);
+  }
+}
+
+/* the last iteration's deferred x += alpha p */
+template <typename T>
+__global__ void
+k_pcgx_xfin (int64_t n, int ld, T *__restrict__ X, const T *__restrict__ P,
+             const double *alpha)
+{
+  constexpr int W = Pack<T>::W;
+  const int nvec = ld / W;
+  const int64_t total = n * nvec;
+  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t) gridDim.x * blockDim.x) {
+    const int64_t i = e / nvec;
+    const int vi = (int) (e - i * nvec);
+    const int64_t o = i * ld + vi * W;
+    Pack<T> x = ldp (X + o);
+    const Pack<T> p = ldp (P + o);
+#pragma unroll
+    for (int k = 0; k < W; k++) x.v[k] = fma ((T) alpha[vi * W + k], p.v[k], x.v[k]);
+    stp (X + o, x);
   }
 }
 
