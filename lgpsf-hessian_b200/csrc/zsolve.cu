@@ -1106,22 +1106,41 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
       LGH_LAUNCH_CHECK ();
       T *Pold = bP0, *Pnew = bP1;
       int h_nact = 1;
+      const double *alpha = ws.scal.p + S_ALPHA * cap;
+      const double *betap = ws.scal.p + S_BETA * cap;
       for (int it = 0; it < cfg.maxit; it++) {
-        if (tr) LGH_TRY (tr->begin (K_PCGX_PQ, zbytes + (it == 0 ? 3. : 4.) * bw, s));
+        /* iteration 0: p = z inside the product; later iterations: the
+         * direction p = z + beta p_old by a streaming pass, which also
+         * applies the previous iteration's x += alpha p_old, then the
+         * product gathers p alone */
+        if (it > 0) {
+          if (tr) LGH_TRY (tr->begin (K_PCGX_PFORM, 5. * bw, s));
+          k_pcgx_pform<T><<<egrid, 256, 0, s>>> (n, ldt, bZ, Pold, Pnew, bX,
+                                                betap, alpha);
+          LGH_LAUNCH_CHECK ();
+          if (tr) LGH_TRY (tr->end (s));
+        }
+        if (tr) LGH_TRY (tr->begin (K_PCGX_PQ, zbytes + (it == 0 ? 3. : 2.) * bw, s));
         ZS_DISPATCH (ch, {
-          auto k1 = k_pcgx_pq<T, CH_>;
           const int psm = zs_pq_smem_bytes (glog, ldt);
-          set_smem_attr (k1, psm);
-          k1<<<fit_grid (k1, grid, ZS_THREADS, psm), ZS_THREADS, psm, s>>> (zk, vals, bZ, Pold, Pnew, bQ, ldt,
-                                             nvec, glog, it == 0, ws.partA.p,
-                                             ws.counters.p, ws.scal.p,
-                                             ws.ival.p, cap);
+          if (it == 0) {
+            auto k1 = k_pcgx_pq<T, CH_, false>;
+            set_smem_attr (k1, psm);
+            k1<<<fit_grid (k1, grid, ZS_THREADS, psm), ZS_THREADS, psm, s>>> (
+                zk, vals, bZ, Pold, Pnew, bQ, ldt, nvec, glog, 1, ws.partA.p,
+                ws.counters.p, ws.scal.p, ws.ival.p, cap);
+          } else {
+            auto k1 = k_pcgx_pq<T, CH_, true>;
+            set_smem_attr (k1, psm);
+            k1<<<fit_grid (k1, grid, ZS_THREADS, psm), ZS_THREADS, psm, s>>> (
+                zk, vals, bZ, Pold, Pnew, bQ, ldt, nvec, glog, 0, ws.partA.p,
+                ws.counters.p, ws.scal.p, ws.ival.p, cap);
+          }
         });
         LGH_LAUNCH_CHECK ();
         if (tr) LGH_TRY (tr->end (s));
-        if (tr) LGH_TRY (tr->begin (K_PCGX_UPD, 6. * bw, s));
-        k_pcgx_upd<T><<<egrid, 256, 0, s>>> (n, ldt, bX, bR, Pnew, bQ,
-                                            ws.scal.p + S_ALPHA * cap);
+        if (tr) LGH_TRY (tr->begin (K_PCGX_UPD, 3. * bw, s));
+        k_pcgx_updr<T><<<egrid, 256, 0, s>>> (n, ldt, bR, bQ, alpha);
         LGH_LAUNCH_CHECK ();
         if (tr) LGH_TRY (tr->end (s));
         LGH_TRY (precond ());
@@ -1147,6 +1166,10 @@ zsolve_block (const Csr &Z, const ZsolveCfg &cfg, Hierarchy *mg, ZWork &ws,
           if (h_nact == 0) break;
         }
       }
+      /* the last iteration's deferred x += alpha p (its direction is in
+       * Pold after the swap) */
+      k_pcgx_xfin<T><<<egrid, 256, 0, s>>> (n, ldt, bX, Pold, alpha);
+      LGH_LAUNCH_CHECK ();
       if (tr && !tr->ids.empty ()) {
         LGH_CUDA (cudaStreamSynchronize (s));
         LGH_TRY (tr->drain ());
