@@ -723,10 +723,12 @@ k_pcgx_dots (ZK z, const T *__restrict__ R, const T *__restrict__ Zb, int ld,
         }
         rz[c] = srz;
         be[c] = b;
+        /* a converged column keeps its alpha: its x update may still be
+         * pending (k_pcgx_pform or k_pcgx_xfin applies it), and the next
+         * product zeroes alpha for inactive columns */
         if (sqrt (szz) <= rtol * n0[c] || srz == 0.) {
           act[c] = 0;
           be[c] = 0.;
-          al_g[c] = 0.;
           its[c] = iter + 1;
         }
       });
