@@ -221,8 +221,9 @@ enqueue_tail (ShiftPlan &P, lgh_glr_t *g, int kind, int nshift, int variant,
     LGH_CHECK (P.maps_ok, LGH_ERR_ARG_WRONGSTATE, "batch: tensor maps missing");
     LGH_TRY (umma_split_coef (P.kept, P.kpad, m, nshift, P.ncolp, P.g.p, P.Wc.p,
                               P.Bh.p, P.Bl.p, s));
-    return launch_shift_combine_umma (P.maps[variant - kShiftVariants], P.n,
-                                      P.kpad, m, nshift, P.fc.p, P.Y0.p,
+    const int u = variant - kShiftVariants;
+    return launch_shift_combine_umma (P.maps[u & 1], umma_variant_stages (u),
+                                      P.n, P.kpad, m, nshift, P.fc.p, P.Y0.p,
                                       round_ld (m), &pd->out, &pd->ldo,
                                       P.err.p, s);
   }

@@ -15,7 +15,9 @@
  *   - the split operands live in global memory K-major (A: n x kpad from
  *     W, once per object; B: columns x kpad from g .* C, once per call),
  *     kpad a multiple of 32;
- *   - thread 0 drives a two-stage pipeline: TMA tile loads
+ *   - thread 0 drives an NS-stage pipeline (NS = 2 with one CTA per SM,
+ *     or NS = 1 with two or three CTAs per SM that overlap one another's
+ *     loads, MMAs and epilogues): TMA tile loads
  *     (cp.async.bulk.tensor.2d, 128-byte swizzle, no multicast) of 32 K
  *     values of A_hi, A_lo, B_hi, B_lo into a stage, completing on the
  *     stage's mbarrier; then 3 x 4 tcgen05.mma kind::tf32 (M = 128,
@@ -118,8 +120,8 @@ tf32_hi (float x)
   return __uint_as_float (r);
 }
 
-template <int TN>
-__global__ void __launch_bounds__ (128, 1)
+template <int TN, int NS>
+__global__ void __launch_bounds__ (128, NS == 1 ? 2 : 1)
 k_shift_combine_umma (const __grid_constant__ CUtensorMap mAh,
                       const __grid_constant__ CUtensorMap mAl,
                       const __grid_constant__ CUtensorMap mBh,
@@ -136,18 +138,19 @@ k_shift_combine_umma (const __grid_constant__ CUtensorMap mAh,
   const uint32_t raw = su32 (smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
   uint8_t *const gbase = smem_raw + (base - raw);
-  uint64_t *bars = (uint64_t *) (gbase + 2 * STAGE); /* full 0,1 empty 0,1 done */
-  uint32_t *holder = (uint32_t *) (bars + 5);
+  /* barriers: full[NS], empty[NS], done */
+  uint64_t *bars = (uint64_t *) (gbase + NS * STAGE);
+  uint32_t *holder = (uint32_t *) (bars + 2 * NS + 1);
   int *failed = (int *) (holder + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t row0 = (int64_t) blockIdx.y * UM;
   const int col0 = blockIdx.x * TN;
   const int ncol = nshift * m;
-  const uint32_t bfull = su32 (bars), bempty = su32 (bars + 2),
-                 bdone = su32 (bars + 4);
+  const uint32_t bfull = su32 (bars), bempty = su32 (bars + NS),
+                 bdone = su32 (bars + 2 * NS);
 
   if (tid == 0) {
-    for (int i = 0; i < 5; i++)
+    for (int i = 0; i < 2 * NS + 1; i++)
       asm volatile ("mbarrier.init.shared::cta.b64 [%0], 1;"
                     :: "r"(su32 (bars + i)));
     *failed = 0;
@@ -169,47 +172,51 @@ k_shift_combine_umma (const __grid_constant__ CUtensorMap mAh,
                            | ((uint32_t) (TN >> 3) << 17)
                            | ((uint32_t) (UM >> 4) << 24);
     bool ok = true;
-    int issued = 0;          /* stages loaded */
-    for (int a = 0; a <= natoms && ok; a++) {
-      if (a < natoms) {
-        const int s = a & 1;
-        if (a >= 2) ok = mbar_wait (bempty + 8 * s, ((a - 2) >> 1) & 1);
-        if (!ok) break;
-        const uint32_t st = base + s * STAGE;
-        asm volatile ("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                      :: "r"(bfull + 8 * s), "r"(STAGE) : "memory");
-        tma_load_2d (st, &mAh, a * UKA, (int) row0, bfull + 8 * s);
-        tma_load_2d (st + A_BYTES, &mAl, a * UKA, (int) row0, bfull + 8 * s);
-        tma_load_2d (st + 2 * A_BYTES, &mBh, a * UKA, col0, bfull + 8 * s);
-        tma_load_2d (st + 2 * A_BYTES + B_BYTES, &mBl, a * UKA, col0,
-                     bfull + 8 * s);
-        issued = a + 1;
-      }
-      if (a >= 1) {
-        const int b = a - 1, s = b & 1;
-        ok = mbar_wait (bfull + 8 * s, (b >> 1) & 1);
-        if (!ok) break;
-        asm volatile ("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t st = base + s * STAGE;
+    int issued = 0;          /* atoms whose loads were issued */
+    auto load = [&] (int a) {
+      const int s = a % NS;
+      const uint32_t st = base + s * STAGE;
+      asm volatile ("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                    :: "r"(bfull + 8 * s), "r"(STAGE) : "memory");
+      tma_load_2d (st, &mAh, a * UKA, (int) row0, bfull + 8 * s);
+      tma_load_2d (st + A_BYTES, &mAl, a * UKA, (int) row0, bfull + 8 * s);
+      tma_load_2d (st + 2 * A_BYTES, &mBh, a * UKA, col0, bfull + 8 * s);
+      tma_load_2d (st + 2 * A_BYTES + B_BYTES, &mBl, a * UKA, col0,
+                   bfull + 8 * s);
+      issued = a + 1;
+    };
+    /* the first NS atoms go straight into their stages; atom b + NS
+     * reuses atom b's stage once the MMAs of atom b have drained it */
+    for (int a = 0; a < NS && a < natoms; a++) load (a);
+    for (int b = 0; b < natoms; b++) {
+      const int s = b % NS;
+      ok = mbar_wait (bfull + 8 * s, (b / NS) & 1);
+      if (!ok) break;
+      asm volatile ("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t st = base + s * STAGE;
 #pragma unroll
-        for (int kk = 0; kk < 4; kk++) {
-          const uint64_t ah = sdesc (st + 32 * kk);
-          const uint64_t al = sdesc (st + A_BYTES + 32 * kk);
-          const uint64_t bh = sdesc (st + 2 * A_BYTES + 32 * kk);
-          const uint64_t bl = sdesc (st + 2 * A_BYTES + B_BYTES + 32 * kk);
-          umma_tf32 (tmem, ah, bh, idesc, (b > 0 || kk > 0) ? 1u : 0u);
-          umma_tf32 (tmem, ah, bl, idesc, 1u);
-          umma_tf32 (tmem, al, bh, idesc, 1u);
-        }
-        umma_commit (bempty + 8 * s);
+      for (int kk = 0; kk < 4; kk++) {
+        const uint64_t ah = sdesc (st + 32 * kk);
+        const uint64_t al = sdesc (st + A_BYTES + 32 * kk);
+        const uint64_t bh = sdesc (st + 2 * A_BYTES + 32 * kk);
+        const uint64_t bl = sdesc (st + 2 * A_BYTES + B_BYTES + 32 * kk);
+        umma_tf32 (tmem, ah, bh, idesc, (b > 0 || kk > 0) ? 1u : 0u);
+        umma_tf32 (tmem, ah, bl, idesc, 1u);
+        umma_tf32 (tmem, al, bh, idesc, 1u);
+      }
+      umma_commit (bempty + 8 * s);
+      if (b + NS < natoms) {
+        ok = mbar_wait (bempty + 8 * s, (b / NS) & 1);
+        if (!ok) break;
+        load (b + NS);
       }
     }
     if (!ok) {
       *failed = 1;
       atomicExch (err, 1);
       /* loads still in flight complete on their stage barriers */
-      for (int b = std::max (0, issued - 2); b < issued; b++)
-        mbar_wait (bfull + 8 * (b & 1), (b >> 1) & 1);
+      for (int b = std::max (0, issued - NS); b < issued; b++)
+        mbar_wait (bfull + 8 * (b % NS), (b / NS) & 1);
     }
     /* one commit after every MMA issued: the accumulator is final (or,
      * after a failure, no MMA is in flight) when it arrives */
@@ -355,11 +362,31 @@ encode_kmajor (CUtensorMap *map, const float *base, int64_t rows, int kpad,
   return 0;
 }
 
-template <int TN>
+template <int TN, int NS>
 constexpr int
 umma_smem ()
 {
-  return 2 * (2 * UM * 128 + 2 * TN * 128) + 64 + 1024;
+  return NS * (2 * UM * 128 + 2 * TN * 128) + 64 + 1024;
+}
+
+template <int TN, int NS>
+int
+launch_umma_shape (const CUtensorMap *mp, dim3 grid, int64_t n, int kpad,
+                   int m, int nshift, const double *fc, const double *Y0,
+                   int ldy0, double *const *out, const int64_t *ldo, int *err,
+                   cudaStream_t s)
+{
+  auto k = k_shift_combine_umma<TN, NS>;
+  constexpr int sm = umma_smem<TN, NS> ();
+  static bool set = false;
+  if (!set) {
+    LGH_CUDA (cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    set = true;
+  }
+  k<<<grid, 128, sm, s>>> (mp[0], mp[1], mp[2], mp[3], n, kpad, m, nshift, fc,
+                           Y0, ldy0, out, ldo, err);
+  LGH_LAUNCH_CHECK ();
+  return 0;
 }
 
 } /* namespace */
@@ -417,10 +444,10 @@ umma_encode (UmmaMaps *M, const float *Ah, const float *Al, int64_t n,
 }
 
 int
-launch_shift_combine_umma (const UmmaMaps &M, int64_t n, int kpad, int m,
-                           int nshift, const double *fc, const double *Y0,
-                           int ldy0, double *const *out, const int64_t *ldo,
-                           int *err, cudaStream_t s)
+launch_shift_combine_umma (const UmmaMaps &M, int stages, int64_t n, int kpad,
+                           int m, int nshift, const double *fc,
+                           const double *Y0, int ldy0, double *const *out,
+                           const int64_t *ldo, int *err, cudaStream_t s)
 {
   if (n == 0 || m == 0 || nshift == 0) return 0;
   const CUtensorMap *mp = (const CUtensorMap *) M.raw;
@@ -428,30 +455,16 @@ launch_shift_combine_umma (const UmmaMaps &M, int64_t n, int kpad, int m,
   const int64_t rt = (n + UM - 1) / UM;
   LGH_CHECK (rt < 65536 && ncol < INT32_MAX, LGH_ERR_ARG_OUTOFRANGE,
              "tensor-core shift combine: grid too large");
-  dim3 grid ((unsigned) ((ncol + M.tn - 1) / M.tn), (unsigned) rt);
-  if (M.tn == 256) {
-    auto k = k_shift_combine_umma<256>;
-    const int sm = umma_smem<256> ();
-    static bool set = false;
-    if (!set) {
-      LGH_CUDA (cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-      set = true;
-    }
-    k<<<grid, 128, sm, s>>> (mp[0], mp[1], mp[2], mp[3], n, kpad, m, nshift, fc,
-                             Y0, ldy0, out, ldo, err);
-  } else {
-    auto k = k_shift_combine_umma<128>;
-    const int sm = umma_smem<128> ();
-    static bool set = false;
-    if (!set) {
-      LGH_CUDA (cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-      set = true;
-    }
-    k<<<grid, 128, sm, s>>> (mp[0], mp[1], mp[2], mp[3], n, kpad, m, nshift, fc,
-                             Y0, ldy0, out, ldo, err);
-  }
-  LGH_LAUNCH_CHECK ();
-  return 0;
+  LGH_CHECK ((M.tn == 128 || M.tn == 256) && (stages == 1 || stages == 2),
+             LGH_ERR_ARG_WRONG, "tensor-core shift combine: no such tile");
+  const dim3 grid ((unsigned) ((ncol + M.tn - 1) / M.tn), (unsigned) rt);
+  if (M.tn == 256)
+    return stages == 1
+        ? launch_umma_shape<256, 1> (mp, grid, n, kpad, m, nshift, fc, Y0, ldy0, out, ldo, err, s)
+        : launch_umma_shape<256, 2> (mp, grid, n, kpad, m, nshift, fc, Y0, ldy0, out, ldo, err, s);
+  return stages == 1
+      ? launch_umma_shape<128, 1> (mp, grid, n, kpad, m, nshift, fc, Y0, ldy0, out, ldo, err, s)
+      : launch_umma_shape<128, 2> (mp, grid, n, kpad, m, nshift, fc, Y0, ldy0, out, ldo, err, s);
 }
 
 } /* namespace lgh */

@@ -42,9 +42,15 @@ bool umma_supported ();
 
 /* tile variants of the combination kernel: FP64 objects 0 = 64 x 64 (4
  * warps), 1 = 128 x 64 (8 warps) on the FP64 mma.sync path; mixed objects
- * 2 = 128 x 128, 3 = 128 x 256 on tcgen05 (TF32 x 3) */
+ * on tcgen05 (TF32 x 3): 2 = 128 x 128 and 3 = 128 x 256 with a two-stage
+ * load pipeline (one CTA per SM), 4 = 128 x 128 and 5 = 128 x 256 with one
+ * stage (three and two CTAs per SM, whose loads, MMAs and epilogues
+ * overlap one another) */
 constexpr int kShiftVariants = 2;
-constexpr int kUmmaVariants = 2;
+constexpr int kUmmaVariants = 4;
+/* tcgen05 variant u = variant - kShiftVariants: tile width and stages */
+inline int umma_variant_tn (int u) { return (u & 1) ? 256 : 128; }
+inline int umma_variant_stages (int u) { return u >= 2 ? 1 : 2; }
 int launch_shift_combine_variant (int variant, int64_t n, int kept, int m,
                                   int nshift, const double *W, int ldw,
                                   const double *C, const double *g,
@@ -67,7 +73,8 @@ int umma_split_coef (int kept, int kpad, int m, int nshift, int ncolp,
                      cudaStream_t s);
 int umma_encode (UmmaMaps *M, const float *Ah, const float *Al, int64_t n,
                  const float *Bh, const float *Bl, int ncolp, int kpad, int tn);
-int launch_shift_combine_umma (const UmmaMaps &M, int64_t n, int kpad, int m,
+int launch_shift_combine_umma (const UmmaMaps &M, int stages, int64_t n,
+                               int kpad, int m,
                                int nshift, const double *fc, const double *Y0,
                                int ldy0, double *const *out, const int64_t *ldo,
                                int *err, cudaStream_t s);

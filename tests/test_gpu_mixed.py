@@ -113,7 +113,7 @@ def test_mixed_many_shift_batch_on_tensor_cores(c1):
         X = g.solve_batch(cs, R)
         S = g.sample_batch(cs, R)
         info = g.batch_info()
-        assert info["variant"] in (2, 3), info
+        assert info["variant"] in (2, 3, 4, 5), info
         for si in (0, 4, 8):
             for j in (0, 63):
                 ref = g.solve(cs[si], R[:, j])
