@@ -606,6 +606,74 @@ void lgh_shard_destroy (lgh_shard_t *shard);
 int lgh_sketch_rows (uint64_t seed, int64_t i0, int64_t n, int64_t j0, int k,
                      double *Y, int64_t ld);
 
+/* ---- a build over row slabs (one rank per GPU) ---------------------------
+ * The reference's MPI layout (docs/glr-woodbury-formulas.tex:76-98): B, Z,
+ * the mass lumps and every N-row block are split into contiguous row slabs
+ * (rank r owns rows lgh_shard_range (N, size, r)).  A row-sharded Mat
+ * (lgh_mat_create_rows) carries its halo plan and the communicator; a
+ * prior made from a row-sharded Z (lgh_prior_create_mat / _pc, with the
+ * rank's mass lumps) is a row-sharded prior, and lgh_glr_compute on a
+ * row-sharded B and prior builds over the slabs:
+ *   - B X and Z X exchange the ghost rows of X once per product (one
+ *     all-to-all of the rows each peer references) and multiply the local
+ *     rows by [owned rows; ghost rows];
+ *   - Z-solves run blocked PCG with two all-reduces of 2 w scalars per
+ *     iteration; the preconditioner is rank-local (block Jacobi: the
+ *     multigrid V-cycle on the rank's diagonal block of Z, or Jacobi),
+ *     so iteration counts grow slowly with the number of ranks and the
+ *     solution matches the one-rank solve to the solve tolerance;
+ *   - every Gram, Q^T F Q, U^T X and residual norm is the local product
+ *     plus one all-reduce (glr_common_impl.h:363, 487, 769, 851); the
+ *     small eigenproblem runs replicated, so every rank keeps the same
+ *     spectrum and its own rows of U.
+ * The sketch is partition-independent (hashed per global row).  Vectors
+ * and blocks passed to the object's operations (solve, sample, apply,
+ * factor, lgh_glr_get_U) hold the rank's rows; logdet and eigs are
+ * replicated.  The batched shift operations, the request loop, the
+ * deflation correction and persistence return LGH_ERR_SUP on a
+ * row-sharded object.
+ *
+ * allreduce: buf[0, count) (device, FP64) becomes the elementwise sum over
+ * ranks, identical on every rank.  alltoallv: for each peer p, the
+ * send_bytes[p] bytes at offset sum_{q<p} send_bytes[q] of send go to p,
+ * and the recv_bytes[p] bytes from p land at offset sum_{q<p}
+ * recv_bytes[q] of recv (device buffers; recv_bytes[p] equals what p
+ * sends here; entries for this rank are 0).  The library synchronises
+ * its stream before each call; the callback returns once the data is in
+ * place (0), or nonzero to fail the operation with LGH_ERR_GPU.  Every
+ * rank makes the same calls in the same order.  The communicator must
+ * stay valid for the lifetime of the objects made with it.              */
+typedef struct lgh_rows_comm
+{
+  int    rank, size;
+  int  (*allreduce) (double *buf, size_t count, void *ctx);
+  int  (*alltoallv) (const void *send, const size_t *send_bytes, void *recv,
+                     const size_t *recv_bytes, void *ctx);
+  void  *ctx;
+}
+lgh_rows_comm_t;
+
+/* This rank's rows [row0, row1) = lgh_shard_range (N, size, rank) of a
+ * symmetric N x N CSR operator: rowptr (row1 - row0 + 1 entries,
+ * rowptr[0] = 0), global column indices, values; host arrays, copied.
+ * Collective: every rank calls it with its own rows.                     */
+int lgh_mat_create_rows (int64_t N, const lgh_rows_comm_t *comm,
+                         const int64_t *rowptr, const int32_t *colidx,
+                         const double *vals, lgh_Mat *A);
+/* rows of a row-sharded Mat (0 / N / 0 ghosts for an ordinary Mat)       */
+int lgh_mat_rows_info (lgh_Mat A, int64_t *row0, int64_t *row1,
+                       int64_t *nghost);
+/* halo traffic of a row-sharded Mat since its creation: exchanges, bytes
+ * this rank sent, seconds in the exchange callback                       */
+int lgh_mat_rows_traffic (lgh_Mat A, long *exchanges, int64_t *bytes_sent,
+                          double *seconds);
+/* `size` communicators for ranks run as threads of one process on one
+ * device: the collectives meet on a host barrier (120 s limit, then
+ * LGH_ERR_GPU), sum in rank order on the host and copy device to device;
+ * no kernel waits for another rank.                                      */
+int lgh_rows_local_create (int size, lgh_rows_comm_t *comms);
+void lgh_rows_local_destroy (lgh_rows_comm_t *comms);
+
 /* Per-kernel CUDA-event timing of the hot kernels: switch on (1) / off (0)
  * (either resets the figures); read accumulated device milliseconds,
  * launches and algorithmic bytes of kernel id 0 k_pcg_pq, 1 k_pcg_upd,

@@ -556,6 +556,7 @@ mat_release (lgh_Mat A)
   if (!A || --A->refs > 0) return;
   if (A->kind == 0) csr_free (A->csr);
   strip_free (A->strips);
+  rows_plan_free (A->rows);
   delete A;
 }
 
@@ -574,6 +575,7 @@ int
 mat_mult_block (lgh_Mat A, const T *X, int ldx, T *Y, int ldy, int w,
                 cudaStream_t s)
 {
+  if (A->rows) return rows_mult_block<T> (A, X, ldx, Y, ldy, w, s);
   if (w >= 8) {
     LGH_TRY (mat_prepare_block (A, w));
     return launch_strip_spmm<T> (A->strips, X, ldx, Y, ldy, w, s);
@@ -589,6 +591,7 @@ template int mat_mult_block<float> (lgh_Mat, const float *, int, float *, int,
 int
 mat_mult_vec (lgh_Mat A, const double *x, double *y)
 {
+  if (A->rows) return rows_mult_block<double> (A, x, 1, y, 1, 1, stream ());
   return launch_spmm<double> (A->csr, x, 1, y, 1, 1, stream ());
 }
 
@@ -596,7 +599,7 @@ mat_mult_vec (lgh_Mat A, const double *x, double *y)
 int
 prior_applyZ (lgh_prior_t *p, const double *x, double *y)
 {
-  if (p->is_mat) return launch_spmm<double> (p->Z->csr, x, 1, y, 1, 1, stream ());
+  if (p->is_mat) return mat_mult_vec (p->Z, x, y);
   lgh_vec_s vx, vy;
   vx.d = (double *) x; vx.n = p->n; vx.owns = 0;
   vy.d = y; vy.n = p->n; vy.owns = 0;
@@ -620,6 +623,8 @@ prior_solve_vec (lgh_prior_t *p, const double *x, const double *s_in,
                  double *y, const double *s_out)
 {
   cudaStream_t s = stream ();
+  if (p->rows)
+    return rows_zsolve<double> (p, 1, x, 1, s_in, y, 1, s_out, p->zcfg.rtol);
   if (p->is_mat) {
     ZsolveCfg cfg;
     prior_zcfg (p, cfg);
@@ -653,6 +658,9 @@ prior_solve_rows (lgh_prior_t *p, int w, const T *X, int ldx,
 {
   cudaStream_t s = stream ();
   if (w == 0) return 0;
+  if (p->rows)
+    return rows_zsolve<T> (p, w, X, ldx, s_in, Y, ldy, s_out,
+                           rtol_override > 0. ? rtol_override : p->zcfg.rtol);
   if (p->is_mat) {
     ZsolveCfg cfg;
     prior_zcfg (p, cfg);
@@ -735,7 +743,7 @@ prior_solve_pc32 (lgh_prior_t *p, int w, const double *X, int ldx,
                   double rtol_override)
 {
   if (w == 0) return 0;
-  if (!p->is_mat || p->mg == nullptr || p->zcfg.mode > 1)
+  if (p->rows || !p->is_mat || p->mg == nullptr || p->zcfg.mode > 1)
     return prior_solve_rows<double> (p, w, X, ldx, s_in, Y, ldy, s_out,
                                      rtol_override);
   ZsolveCfg cfg;
@@ -860,6 +868,9 @@ lgh_prior_create_mat_pc (lgh_Mat Z, lgh_Vec mass,
   LGH_CHECK (o.blocked_mode != 3 || pc_type == LGH_PC_AMG, LGH_ERR_ARG_WRONG,
              "lgh_prior_create_mat: blocked_mode 3 needs the multigrid "
              "preconditioner");
+  LGH_CHECK (!Z->rows || o.blocked_mode <= 1, LGH_ERR_SUP,
+             "lgh_prior_create_mat: a row-sharded Z solves with PCG "
+             "(blocked_mode 0 or 1)");
   lgh_prior_t *p;
   LGH_TRY (prior_init_common (mass, &p));
   p->is_mat = 1;
@@ -867,7 +878,16 @@ lgh_prior_create_mat_pc (lgh_Mat Z, lgh_Vec mass,
   Z->refs++;
   p->mopts = o;
   p->pc_type = pc_type;
-  if (pc_type == LGH_PC_AMG) {
+  if (Z->rows) {
+    /* the rank-local block-Jacobi preconditioner on the diagonal block */
+    p->rows = new RowsPrior ();
+    int rc = rows_prior_setup (p);
+    if (rc) { lgh_prior_destroy (p); return rc; }
+    if (o.verbose && p->mg)
+      printf ("lgh_prior: rank %d multigrid %d levels (coarse %d) setup "
+              "%.3f s\n", Z->rows->comm.rank, (int) p->mg->lev.size (),
+              p->mg->n0, p->mg->setup_s);
+  } else if (pc_type == LGH_PC_AMG) {
     const int nu = o.nu_force > 0 ? o.nu_force : 2;
     int rc = mg_build (Z->csr, o.tile, o.smoother_top, nu, &p->mg);
     if (rc) { lgh_prior_destroy (p); return rc; }
@@ -946,7 +966,9 @@ void
 lgh_prior_destroy (lgh_prior_t *prior)
 {
   if (prior == NULL || --prior->refs > 0) return;
+  /* the hierarchy borrows the finest operator's arrays: it goes first */
   if (prior->mg) mg_destroy (prior->mg);
+  rows_prior_free (prior->rows);
   if (prior->Z) mat_release (prior->Z);
   delete prior;
 }

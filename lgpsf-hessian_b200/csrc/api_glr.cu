@@ -228,11 +228,13 @@ apply_F (lgh_glr_t *g, int w, const T *X, int ldx, T *Y, int ldy, T *W,
 }
 
 /* X <- X L^{-T}, twice (CholQR2, glr_common_impl.h:370-407); the result
- * returns to X, Tmp is scratch.  jitter_mode 0 = replicated rule. */
+ * returns to X, Tmp is scratch.  jitter_mode 0 = replicated rule.  rc
+ * (row slabs): the Gram of the local rows is all-reduced before the
+ * factorisation, which every rank then repeats identically. */
 template <typename T>
 static int
 cholqr2 (int64_t n, int w, T *X, int ldx, T *Tmp, int ldt, Small &sm,
-         int jitter_mode, int *jittered)
+         int jitter_mode, int *jittered, const lgh_rows_comm_t *rc = nullptr)
 {
   cudaStream_t s = stream ();
   for (int pass = 0; pass < 2; pass++) {
@@ -241,6 +243,7 @@ cholqr2 (int64_t n, int w, T *X, int ldx, T *Tmp, int ldt, Small &sm,
     const int lds = pass == 0 ? ldx : ldt, ldd = pass == 0 ? ldt : ldx;
     LGH_TRY (launch_gemm_tn<T> (n, w, w, src, lds, src, lds, sm.G.p, w, 0,
                                 sm.work.p, sm.work.n, s));
+    if (rc) LGH_TRY (rows_allreduce (*rc, sm.G.p, (size_t) w * w, s));
     LGH_TRY (launch_potrf (w, sm.G.p, sm.G0.p, jitter_mode, sm.info.p, s));
     int info[2];
     LGH_CUDA (cudaMemcpyAsync (info, sm.info.p, 2 * sizeof (int),
@@ -259,9 +262,10 @@ cholqr2 (int64_t n, int w, T *X, int ldx, T *Tmp, int ldt, Small &sm,
  * (glr_scalapack_impl.h:110-148), in place via Tmp (>= n x bw) */
 template <typename T>
 static int
-panel_cholqr (int64_t n, int bw, T *P, int ldp, T *Tmp, int ldt, Small &sm)
+panel_cholqr (int64_t n, int bw, T *P, int ldp, T *Tmp, int ldt, Small &sm,
+              const lgh_rows_comm_t *rc)
 {
-  LGH_TRY (cholqr2<T> (n, bw, P, ldp, Tmp, ldt, sm, 1, nullptr));
+  LGH_TRY (cholqr2<T> (n, bw, P, ldp, Tmp, ldt, sm, 1, nullptr, rc));
   return 0;
 }
 
@@ -270,7 +274,7 @@ panel_cholqr (int64_t n, int bw, T *P, int ldp, T *Tmp, int ldt, Small &sm)
 template <typename T>
 static int
 bcgs2 (int64_t n, T *Y, int ld, int ell, int b, int p_start, T *Tmp,
-       int ldt, Small &sm)
+       int ldt, Small &sm, const lgh_rows_comm_t *rc)
 {
   cudaStream_t s = stream ();
   for (int p0 = p_start; p0 < ell; p0 += b) {
@@ -281,10 +285,11 @@ bcgs2 (int64_t n, T *Y, int ld, int ell, int b, int p_start, T *Tmp,
         /* C = Y(:, 0:p0)^T P ; P -= Y(:, 0:p0) C */
         LGH_TRY (launch_gemm_tn<T> (n, p0, bw, Y, ld, pa, ld, sm.C.p, p0, 0,
                                     sm.work.p, sm.work.n, s));
+        if (rc) LGH_TRY (rows_allreduce (*rc, sm.C.p, (size_t) p0 * bw, s));
         LGH_TRY (launch_gemm_nn<T> (n, p0, bw, -1.0, Y, ld, sm.C.p, p0, 1.0,
                                     pa, ld, pa, ld, s));
       }
-      LGH_TRY (panel_cholqr<T> (n, bw, pa, ld, Tmp, ldt, sm));
+      LGH_TRY (panel_cholqr<T> (n, bw, pa, ld, Tmp, ldt, sm, rc));
     }
   }
   return 0;
@@ -445,6 +450,16 @@ residual_check (lgh_glr_t *g, T *Ubuf, T *FU, T *Wk, lgh_glr_report_t *rep,
   LGH_CUDA (cudaMemcpyAsync (h.data (), norms.p, kept * sizeof (double),
                              cudaMemcpyDeviceToHost, s));
   LGH_CUDA (cudaStreamSynchronize (s));
+  if (g->rows) {
+    /* row slabs: the squared local norms summed over ranks */
+    for (double &v : h) v *= v;
+    LGH_CUDA (cudaMemcpy (norms.p, h.data (), kept * sizeof (double),
+                          cudaMemcpyHostToDevice));
+    LGH_TRY (rows_allreduce (*g->rows, norms.p, kept, s));
+    LGH_CUDA (cudaMemcpy (h.data (), norms.p, kept * sizeof (double),
+                          cudaMemcpyDeviceToHost));
+    for (double &v : h) v = sqrt (v);
+  }
   double mx = 0.;
   for (double v : h) mx = std::max (mx, v);
   rep->resid_max = mx;
@@ -473,9 +488,9 @@ build (lgh_glr_t *g, lgh_glr_report_t *rep)
   /* Omega, hashed per (seed, global row, column) */
   double t0 = wall ();
   if constexpr (std::is_same<T, double>::value)
-    LGH_TRY (launch_sketch (g->opts.seed, n, 0, ell, Q.p, ld, s));
+    LGH_TRY (launch_sketch (g->opts.seed, n, 0, ell, Q.p, ld, s, g->row0));
   else
-    LGH_TRY (launch_sketch_f32 (g->opts.seed, n, 0, ell, Q.p, ld, s));
+    LGH_TRY (launch_sketch_f32 (g->opts.seed, n, 0, ell, Q.p, ld, s, g->row0));
   LGH_CUDA (cudaStreamSynchronize (s));
   g->stats.t_sketch += wall () - t0;
 
@@ -485,7 +500,7 @@ build (lgh_glr_t *g, lgh_glr_report_t *rep)
   rep->t_operator += wall () - t0;
   for (int p = 0; p < g->opts.q_power; p++) {
     t0 = wall ();
-    LGH_TRY (cholqr2<T> (n, ell, Y.p, ld, W.p, ld, sm, 0, nullptr));
+    LGH_TRY (cholqr2<T> (n, ell, Y.p, ld, W.p, ld, sm, 0, nullptr, g->rows));
     LGH_CUDA (cudaStreamSynchronize (s));
     double dt = wall () - t0;
     rep->t_dense += dt;
@@ -496,7 +511,7 @@ build (lgh_glr_t *g, lgh_glr_report_t *rep)
     rep->t_operator += wall () - t0;
   }
   t0 = wall ();
-  LGH_TRY (cholqr2<T> (n, ell, Y.p, ld, W.p, ld, sm, 0, nullptr));
+  LGH_TRY (cholqr2<T> (n, ell, Y.p, ld, W.p, ld, sm, 0, nullptr, g->rows));
   LGH_CUDA (cudaStreamSynchronize (s));
   {
     double dt = wall () - t0;
@@ -513,6 +528,7 @@ build (lgh_glr_t *g, lgh_glr_report_t *rep)
   LGH_TRY (A.alloc ((size_t) ell * ell));
   LGH_TRY (launch_gemm_tn<T> (n, ell, ell, Q.p, ld, Y.p, ld, A.p, ell, 0,
                               sm.work.p, sm.work.n, s));
+  if (g->rows) LGH_TRY (rows_allreduce (*g->rows, A.p, (size_t) ell * ell, s));
   LGH_TRY (rayleigh_ritz<T> (g, ell, Q.p, ld, A.p, sm, rep));
 
   /* residual check on the kept columns (U in FP64 or FP32 blocks) */
@@ -569,9 +585,9 @@ extend_incremental (lgh_glr_t *g, int k_new, lgh_glr_report_t *rep)
   LGH_TRY (launch_copy_block<T> (n, l1, Qold, ld1, Qb.p, ld2, s));
   double t0 = wall ();
   if constexpr (std::is_same<T, double>::value)
-    LGH_TRY (launch_sketch (g->opts.seed, n, l1, k_new, Qn.p, ldk, s));
+    LGH_TRY (launch_sketch (g->opts.seed, n, l1, k_new, Qn.p, ldk, s, g->row0));
   else
-    LGH_TRY (launch_sketch_f32 (g->opts.seed, n, l1, k_new, Qn.p, ldk, s));
+    LGH_TRY (launch_sketch_f32 (g->opts.seed, n, l1, k_new, Qn.p, ldk, s, g->row0));
   LGH_CUDA (cudaStreamSynchronize (s));
   g->stats.t_sketch += wall () - t0;
 
@@ -581,7 +597,7 @@ extend_incremental (lgh_glr_t *g, int k_new, lgh_glr_report_t *rep)
   rep->t_operator += wall () - t0;
   for (int p = 0; p < g->opts.q_power; p++) {
     t0 = wall ();
-    LGH_TRY (bcgs2<T> (n, Yn.p, ldk, k_new, panel, 0, Wn.p, ldk, sm));
+    LGH_TRY (bcgs2<T> (n, Yn.p, ldk, k_new, panel, 0, Wn.p, ldk, sm, g->rows));
     LGH_CUDA (cudaStreamSynchronize (s));
     rep->t_dense += wall () - t0;
     Qn.swap (Yn);
@@ -592,7 +608,7 @@ extend_incremental (lgh_glr_t *g, int k_new, lgh_glr_report_t *rep)
   /* F^{q+1} Omega_new into Qb's new columns; BCGS2 vs old + internal */
   LGH_TRY (launch_copy_block<T> (n, k_new, Yn.p, ldk, Qb.p + l1, ld2, s));
   t0 = wall ();
-  LGH_TRY (bcgs2<T> (n, Qb.p, ld2, l2, panel, l1, Wn.p, ld2, sm));
+  LGH_TRY (bcgs2<T> (n, Qb.p, ld2, l2, panel, l1, Wn.p, ld2, sm, g->rows));
   LGH_CUDA (cudaStreamSynchronize (s));
   rep->t_dense += wall () - t0;
   /* F Q_new, border columns Cnew = Q_all^T (F Q_new) */
@@ -605,6 +621,7 @@ extend_incremental (lgh_glr_t *g, int k_new, lgh_glr_report_t *rep)
   LGH_TRY (A2.alloc ((size_t) l2 * l2));
   LGH_TRY (launch_gemm_tn<T> (n, l2, k_new, Qb.p, ld2, Yn.p, ldk, Cn.p, l2, 0,
                               sm.work.p, sm.work.n, s));
+  if (g->rows) LGH_TRY (rows_allreduce (*g->rows, Cn.p, (size_t) l2 * k_new, s));
   k_grow_A<<<sgrid ((int64_t) l2 * l2), 256, 0, s>>> (l1, l2, g->A.p, Cn.p, A2.p);
   LGH_LAUNCH_CHECK ();
   g->opts.ell = l2;
@@ -648,6 +665,7 @@ filter_core (lgh_glr_t *g, int kind, double c, double p, const double *f_user,
   LGH_LAUNCH_CHECK ();
   LGH_TRY (launch_gemm_tn<double> (n, g->kept, 1, g->U.p, g->ldu, in, 1,
                                    g->wk.p, g->kept, 0, g->part.p, g->part.n, s));
+  if (g->rows) LGH_TRY (rows_allreduce (*g->rows, g->wk.p, g->kept, s));
   k_scale_rows_cm<<<1, 256, 0, s>>> (g->kept, 1, g->fk.p, g->wk.p, g->wk.p);
   LGH_LAUNCH_CHECK ();
   LGH_TRY (launch_gemm_nn<double> (n, g->kept, 1, 1.0, g->U.p, g->ldu, g->wk.p,
@@ -706,6 +724,8 @@ batch_op (lgh_glr_t *g, int kind, int nshift, const double *c, int m,
   cudaStream_t s = stream ();
   const int64_t n = g->n;
   LGH_CHECK (g && c && rhs && x, LGH_ERR_ARG_NULL, "batch: NULL argument");
+  LGH_CHECK (!g->rows, LGH_ERR_SUP,
+             "batch: a row-sharded object runs the per-shift operations");
   LGH_CHECK (m > 0 && nshift > 0 && ldr >= n && ldx >= n, LGH_ERR_ARG_SIZ, "batch: size");
   std::vector<double> ch (nshift);
   LGH_CUDA (cudaMemcpy (ch.data (), c, nshift * sizeof (double), cudaMemcpyDefault));
@@ -859,10 +879,23 @@ lgh_glr_compute_ex (lgh_Mat B, lgh_prior_t *prior, const lgh_glr_opts_t *opts,
   LGH_CHECK (B && prior && glr, LGH_ERR_ARG_NULL, "lgh_glr_compute: NULL argument");
   LGH_CHECK (B->kind == 0, LGH_ERR_ARG_WRONG, "lgh_glr_compute: B must be a CSR Mat");
   LGH_CHECK (B->csr.n == prior->n, LGH_ERR_ARG_SIZ, "lgh_glr_compute: B and prior sizes differ");
+  /* row slabs: B and the prior's Z sharded by the same communicator */
+  const bool rows = B->rows != nullptr || prior->rows != nullptr;
+  if (rows) {
+    LGH_CHECK (B->rows && prior->rows, LGH_ERR_ARG_WRONG,
+               "lgh_glr_compute: B and the prior must both be row-sharded "
+               "or neither");
+    LGH_CHECK (rows_same_comm (B->rows->comm, prior->Z->rows->comm)
+               && B->rows->N == prior->Z->rows->N, LGH_ERR_ARG_WRONG,
+               "lgh_glr_compute: B and the prior are sharded differently");
+    LGH_CHECK (t_comm == nullptr, LGH_ERR_SUP,
+               "lgh_glr_compute: row slabs and column sharding together");
+  }
+  const int64_t Nglob = rows ? B->rows->N : B->csr.n;
   lgh_glr_opts_t o = opts ? *opts : lgh_glr_opts_default ();
   /* glr_common_impl.h:651-654 */
-  LGH_CHECK (o.ell > 0 && o.ell <= B->csr.n, LGH_ERR_ARG_OUTOFRANGE,
-             "lgh_glr_compute: need 0 < ell (%d) <= N (%d)", o.ell, (int) B->csr.n);
+  LGH_CHECK (o.ell > 0 && o.ell <= Nglob, LGH_ERR_ARG_OUTOFRANGE,
+             "lgh_glr_compute: need 0 < ell (%d) <= N (%d)", o.ell, (int) Nglob);
   LGH_CHECK (o.ell <= 2048, LGH_ERR_SUP, "lgh_glr_compute: ell %d > 2048 on one device", o.ell);
   LGH_CHECK (o.treat >= 0 && o.treat <= 2, LGH_ERR_ARG_OUTOFRANGE, "lgh_glr_compute: treat");
   lgh_glr_t *g = new lgh_glr_t ();
@@ -876,6 +909,11 @@ lgh_glr_compute_ex (lgh_Mat B, lgh_prior_t *prior, const lgh_glr_opts_t *opts,
   g->prior = prior;
   prior_ref (prior);
   if (t_comm) g->comm = *t_comm;
+  g->N = Nglob;
+  if (rows) {
+    g->rows = &B->rows->comm;
+    g->row0 = B->rows->row0;
+  }
   lgh_glr_report_t rep;
   int rc = (g->exec.precision == LGH_PREC_MIXED) ? build<float> (g, &rep)
                                                  : build<double> (g, &rep);
@@ -1011,7 +1049,7 @@ lgh_glr_apply (lgh_glr_t *glr, double c, lgh_Vec v, lgh_Vec y)
   LGH_TRY (glr_scratch (glr));
   lgh_prior_t *p = glr->prior;
   cudaStream_t s = stream ();
-  LGH_TRY (launch_spmm<double> (glr->B->csr, v->d, 1, y->d, 1, 1, s));
+  LGH_TRY (mat_mult_vec (glr->B, v->d, y->d));
   LGH_TRY (prior_applyZ (p, v->d, glr->w1.p));
   LGH_TRY (launch_vec_div (glr->n, glr->w1.p, p->mass.p, glr->w2.p, s));
   LGH_TRY (prior_applyZ (p, glr->w2.p, glr->w1.p));

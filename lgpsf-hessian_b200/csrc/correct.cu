@@ -741,6 +741,8 @@ lgh_glr_correct_probes (lgh_glr_t *glr, int k, const double *V,
   LGH_CHECK (glr && V && HV && hess, LGH_ERR_ARG_NULL,
              "lgh_glr_correct_probes: the object, both probe arrays and the "
              "Hessian callback are required");
+  LGH_CHECK (!glr->rows, LGH_ERR_SUP,
+             "lgh_glr_correct_probes: not on a row-sharded object");
   lgh_glr_correct_report_t rep;
   Deflator dfl{};
   LGH_TRY (start (glr, opts_in, &rep, &dfl.o, "lgh_glr_correct_probes"));
@@ -833,6 +835,8 @@ lgh_glr_correct (lgh_glr_t *glr, lgh_hessian_fn hess, void *ctx,
   LGH_CHECK (glr && hess, LGH_ERR_ARG_NULL,
              "lgh_glr_correct: the object and the Hessian callback are "
              "required");
+  LGH_CHECK (!glr->rows, LGH_ERR_SUP,
+             "lgh_glr_correct: not on a row-sharded object");
   lgh_glr_correct_report_t rep;
   Deflator dfl{};
   LGH_TRY (start (glr, opts_in, &rep, &dfl.o, "lgh_glr_correct"));

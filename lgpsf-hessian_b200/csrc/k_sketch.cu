@@ -51,20 +51,20 @@ grid_for (int64_t total)
 
 int
 launch_sketch (uint64_t seed, int64_t n, int64_t j0, int k, double *Y,
-               int ld, cudaStream_t s)
+               int ld, cudaStream_t s, int64_t i0)
 {
   if (n == 0) return 0;
-  k_sketch<double><<<grid_for (n * ld), 256, 0, s>>> (seed, 0, n, j0, k, Y, ld);
+  k_sketch<double><<<grid_for (n * ld), 256, 0, s>>> (seed, i0, n, j0, k, Y, ld);
   LGH_LAUNCH_CHECK ();
   return 0;
 }
 
 int
 launch_sketch_f32 (uint64_t seed, int64_t n, int64_t j0, int k, float *Y,
-                   int ld, cudaStream_t s)
+                   int ld, cudaStream_t s, int64_t i0)
 {
   if (n == 0) return 0;
-  k_sketch<float><<<grid_for (n * ld), 256, 0, s>>> (seed, 0, n, j0, k, Y, ld);
+  k_sketch<float><<<grid_for (n * ld), 256, 0, s>>> (seed, i0, n, j0, k, Y, ld);
   LGH_LAUNCH_CHECK ();
   return 0;
 }

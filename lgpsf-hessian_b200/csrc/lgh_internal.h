@@ -147,11 +147,12 @@ struct Csr
 
 /* ---- kernel launchers (k_*.cu) ------------------------------------------ */
 
-/* sketch: Y[i*ld + j] = randn_at(seed, i, j0 + j), i < n, j < k */
+/* sketch: Y[i*ld + j] = randn_at(seed, i0 + i, j0 + j), i < n, j < k
+ * (i0: the first global row of a row slab) */
 int launch_sketch (uint64_t seed, int64_t n, int64_t j0, int k, double *Y,
-                   int ld, cudaStream_t s);
+                   int ld, cudaStream_t s, int64_t i0 = 0);
 int launch_sketch_f32 (uint64_t seed, int64_t n, int64_t j0, int k,
-                       float *Y, int ld, cudaStream_t s);
+                       float *Y, int ld, cudaStream_t s, int64_t i0 = 0);
 /* the integer xorshift state (testing) */
 int launch_rng_state (uint64_t seed, int64_t n, int64_t j0, int k,
                       uint64_t *S, cudaStream_t s);

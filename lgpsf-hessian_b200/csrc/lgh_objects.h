@@ -8,6 +8,7 @@
 #include "lgh_internal.h"
 #include "lgh_batch.h"
 #include "lgh_strip.h"
+#include "lgh_rows.h"
 
 /* Mat: a device CSR operator (kind 0) or a dense column-block view handed
  * to blocked prior callbacks (kind 1, MATDENSE layout, not owned). */
@@ -25,6 +26,9 @@ struct lgh_mat_s
   lgh::StripForm strips;
   int strips_built = 0;
   int strip_R = 0;
+  /* row-sharded operator: csr holds the owned rows over local columns
+   * [owned; ghosts] (csr.ncols = nloc + nghost) and rows the halo plan */
+  lgh::RowsPlan *rows = nullptr;
 };
 
 /* Vec: a device vector; owns its array unless created with an array. */
@@ -57,6 +61,9 @@ struct lgh_prior
   lgh::ZsolveStats stats;
   long pc32_calls = 0;          /* Z-solves with the FP32 V-cycle (mixed) */
   lgh::DBuf<double> mix_in;     /* FP64 copy of an FP32 block (mixed) */
+  /* row-sharded prior (Z row-sharded): the rank-local preconditioner and
+   * the distributed PCG's workspace; n is the rank's row count */
+  lgh::RowsPrior *rows = nullptr;
 };
 
 /* struct lgh_glr (glr_common_impl.h:252-278), device resident */
@@ -96,6 +103,10 @@ struct lgh_glr
    * its library-owned exchange buffers */
   lgh_comm_t comm{};
   lgh::DBuf<char> xsend, xrecv;
+  /* a build over row slabs: the communicator of B and the prior (null:
+   * not row-sharded), the first global row and the global row count */
+  const lgh_rows_comm_t *rows = nullptr;
+  int64_t row0 = 0, N = 0;
   lgh_glr_stats_t stats{};
 };
 

@@ -102,6 +102,7 @@ lgh_glr_save (const lgh_glr_t *g, const char *path, int with_extension)
 {
   LGH_TRY (ensure_init ());
   LGH_CHECK (g && path, LGH_ERR_ARG_NULL, "lgh_glr_save: NULL argument");
+  LGH_CHECK (!g->rows, LGH_ERR_SUP, "lgh_glr_save: not on a row-sharded object");
   LGH_CUDA (cudaDeviceSynchronize ());
   const int has_q = (g->Q.p != nullptr || g->Q32.p != nullptr) && g->ell > 0;
   LGH_CHECK (!with_extension || has_q, LGH_ERR_ARG_WRONGSTATE,
@@ -163,6 +164,8 @@ lgh_glr_load (lgh_Mat B, lgh_prior_t *prior, const char *path,
              "lgh_glr_load: NULL argument");
   LGH_CHECK (B->kind == 0 && B->csr.n == prior->n, LGH_ERR_ARG_SIZ,
              "lgh_glr_load: B and prior sizes differ");
+  LGH_CHECK (!B->rows && !prior->rows, LGH_ERR_SUP,
+             "lgh_glr_load: not onto row-sharded operators");
   Source in;
   in.f = fopen (path, "rb");
   LGH_CHECK (in.f != nullptr, LGH_ERR_ARG_WRONG, "lgh_glr_load: cannot open %s",

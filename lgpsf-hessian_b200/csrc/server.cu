@@ -863,6 +863,9 @@ lgh_server_create (lgh_glr_t *glr, const lgh_server_opts_t *opts,
   LGH_CHECK (glr && out, LGH_ERR_ARG_NULL, "lgh_server_create: NULL");
   LGH_CHECK (glr->prior->is_mat, LGH_ERR_SUP,
              "lgh_server_create: needs a Mat-path prior (device Z-solves)");
+  LGH_CHECK (!glr->rows, LGH_ERR_SUP,
+             "lgh_server_create: a row-sharded object is served by its "
+             "per-call operations");
   lgh_server_opts_t o = opts ? *opts : lgh_server_opts_default ();
   LGH_CHECK (o.slots >= 1 && o.slots <= Harvest::MAXS, LGH_ERR_ARG_OUTOFRANGE,
              "lgh_server_create: slots %d", o.slots);

@@ -95,6 +95,22 @@ class Comm(ctypes.Structure):
                 ("ctx", ctypes.c_void_p)]
 
 
+ROWS_ALLREDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p,
+                                     ctypes.c_size_t, ctypes.c_void_p)
+ROWS_ALLTOALLV_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p,
+                                     ctypes.POINTER(ctypes.c_size_t),
+                                     ctypes.c_void_p,
+                                     ctypes.POINTER(ctypes.c_size_t),
+                                     ctypes.c_void_p)
+
+
+class RowsComm(ctypes.Structure):
+    """lgh_rows_comm_t: the communicator of a build over row slabs."""
+    _fields_ = [("rank", ctypes.c_int), ("size", ctypes.c_int),
+                ("allreduce", ROWS_ALLREDUCE_FN),
+                ("alltoallv", ROWS_ALLTOALLV_FN), ("ctx", ctypes.c_void_p)]
+
+
 class ServerOpts(ctypes.Structure):
     _fields_ = [("slots", ctypes.c_int), ("hbm_reserve", ctypes.c_double),
                 ("verbose", ctypes.c_int)]
@@ -293,6 +309,12 @@ SIGNATURES = {
     "lgh_shard_destroy": (None, [P]),
     "lgh_sketch_rows": (ctypes.c_int, [ctypes.c_uint64, I64, I64, I64,
                                        ctypes.c_int, P, I64]),
+    "lgh_mat_create_rows": (ctypes.c_int, [I64, P, P, P, P,
+                                           ctypes.POINTER(P)]),
+    "lgh_mat_rows_info": (ctypes.c_int, [P, P, P, P]),
+    "lgh_mat_rows_traffic": (ctypes.c_int, [P, P, P, P]),
+    "lgh_rows_local_create": (ctypes.c_int, [ctypes.c_int, P]),
+    "lgh_rows_local_destroy": (None, [P]),
     "lgh_launch_count": (ctypes.c_long, []),
     "lgh_runtime_counters": (ctypes.c_int, [c_dbl_p]),
     "lgh_kernel_timing": (ctypes.c_int, [ctypes.c_int]),
@@ -434,11 +456,26 @@ class DeviceBlock:
 
 
 class Mat:
-    """Device CSR operator (the reference's Mat for B and Z)."""
+    """Device CSR operator (the reference's Mat for B and Z).  With rows =
+    (N, comm): this rank's row slab of an N x N operator (csr holds the
+    rank's rows with global column indices), sharded over the row-slab
+    communicator comm (a RowsComm)."""
 
-    def __init__(self, csr=None, dense=None):
+    def __init__(self, csr=None, dense=None, rows=None):
         L = load()
         self.h = P()
+        if rows is not None:
+            N, comm = rows
+            rp = np.ascontiguousarray(csr["rowptr"], dtype=np.int64)
+            ci = np.ascontiguousarray(csr["colidx"], dtype=np.int32)
+            va = np.ascontiguousarray(csr["vals"], dtype=np.float64)
+            self._comm = comm
+            _chk(L.lgh_mat_create_rows(int(N), ctypes.addressof(comm),
+                                       rp.ctypes.data, ci.ctypes.data,
+                                       va.ctypes.data, ctypes.byref(self.h)),
+                 "lgh_mat_create_rows")
+            self.n = len(rp) - 1
+            return
         if dense is not None:
             D = np.asfortranarray(dense, dtype=np.float64)
             _chk(L.lgh_mat_create_dense(D.shape[0], D.ctypes.data, D.shape[0],
@@ -460,6 +497,24 @@ class Mat:
         _chk(load().lgh_mat_get_info(self.h, ctypes.byref(n),
                                      ctypes.byref(nnz)), "lgh_mat_get_info")
         return n.value, nnz.value
+
+    def rows_info(self):
+        """(row0, row1, nghost) of a row-sharded Mat."""
+        a, b, g = I64(), I64(), I64()
+        _chk(load().lgh_mat_rows_info(self.h, ctypes.addressof(a),
+                                      ctypes.addressof(b),
+                                      ctypes.addressof(g)),
+             "lgh_mat_rows_info")
+        return a.value, b.value, g.value
+
+    def rows_traffic(self):
+        """(exchanges, bytes sent, seconds) of a row-sharded Mat's halo."""
+        e, b, t = ctypes.c_long(), I64(), ctypes.c_double()
+        _chk(load().lgh_mat_rows_traffic(self.h, ctypes.addressof(e),
+                                         ctypes.addressof(b),
+                                         ctypes.addressof(t)),
+             "lgh_mat_rows_traffic")
+        return e.value, b.value, t.value
 
     def mult(self, x):
         vx, vy = Vec(data=x), Vec(len(x))
@@ -950,6 +1005,28 @@ def local_comms(size):
 
 def free_local_comms(arr):
     load().lgh_comm_local_destroy(ctypes.addressof(arr))
+
+
+def local_rows_comms(size):
+    """size in-process row-slab communicators (ranks as threads on one
+    device)."""
+    arr = (RowsComm * size)()
+    _chk(load().lgh_rows_local_create(size, ctypes.addressof(arr)),
+         "lgh_rows_local_create")
+    return arr
+
+
+def free_local_rows_comms(arr):
+    load().lgh_rows_local_destroy(ctypes.addressof(arr))
+
+
+def rows_slab(csr, row0, row1):
+    """Rows [row0, row1) of a host CSR dict (global column indices)."""
+    rp = np.asarray(csr["rowptr"], dtype=np.int64)
+    a, b = int(rp[row0]), int(rp[row1])
+    return dict(n=row1 - row0, rowptr=rp[row0:row1 + 1] - a,
+                colidx=np.asarray(csr["colidx"])[a:b],
+                vals=np.asarray(csr["vals"])[a:b])
 
 
 def test_spmm_strip(A, X, fp32=False, R=0):

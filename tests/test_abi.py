@@ -54,7 +54,8 @@ def test_struct_layouts_match_c_compiler(tmp_path):
                "lgh_glr_correct_report_t": lgh_b200.CorrectReport,
                "lgh_server_opts_t": lgh_b200.ServerOpts,
                "lgh_server_stats_t": lgh_b200.ServerStats,
-               "lgh_comm_t": lgh_b200.Comm}
+               "lgh_comm_t": lgh_b200.Comm,
+               "lgh_rows_comm_t": lgh_b200.RowsComm}
     lines = ['#include <stdio.h>', '#include <stddef.h>',
              '#include "lgh_b200.h"', 'int main(void){']
     for cname, py in structs.items():
