@@ -878,7 +878,6 @@ lgh_glr_compute_ex (lgh_Mat B, lgh_prior_t *prior, const lgh_glr_opts_t *opts,
   LGH_TRY (ensure_init ());
   LGH_CHECK (B && prior && glr, LGH_ERR_ARG_NULL, "lgh_glr_compute: NULL argument");
   LGH_CHECK (B->kind == 0, LGH_ERR_ARG_WRONG, "lgh_glr_compute: B must be a CSR Mat");
-  LGH_CHECK (B->csr.n == prior->n, LGH_ERR_ARG_SIZ, "lgh_glr_compute: B and prior sizes differ");
   /* row slabs: B and the prior's Z sharded by the same communicator */
   const bool rows = B->rows != nullptr || prior->rows != nullptr;
   if (rows) {
@@ -891,6 +890,7 @@ lgh_glr_compute_ex (lgh_Mat B, lgh_prior_t *prior, const lgh_glr_opts_t *opts,
     LGH_CHECK (t_comm == nullptr, LGH_ERR_SUP,
                "lgh_glr_compute: row slabs and column sharding together");
   }
+  LGH_CHECK (B->csr.n == prior->n, LGH_ERR_ARG_SIZ, "lgh_glr_compute: B and prior sizes differ");
   const int64_t Nglob = rows ? B->rows->N : B->csr.n;
   lgh_glr_opts_t o = opts ? *opts : lgh_glr_opts_default ();
   /* glr_common_impl.h:651-654 */

@@ -184,7 +184,10 @@ def test_rows_build_matches_one_rank(cuda_device, c1, size):
     got = _sharded(c1, size, gopts)
     _close(got, want)
     assert got["report"]["kept"] == want["report"]["kept"]
-    assert got["report"]["resid_max"] < 1e-6 * np.abs(want["lam"]).max()
+    # the Rayleigh-Ritz residual (about the first cut eigenvalue) is the
+    # same quantity, computed from all-reduced partial norms
+    rg, rw = got["report"]["resid_max"], want["report"]["resid_max"]
+    assert abs(rg - rw) <= 1e-3 * rw + 1e-10 * np.abs(want["lam"]).max()
     for ex, nbytes, _ in got["traffic"]:
         assert ex > 0 and nbytes > 0
 
