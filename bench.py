@@ -71,7 +71,7 @@ def parse():
     ap.add_argument("--serve-rates", default="",
                     help="comma-separated request rates for --config c5")
     ap.add_argument("--kernel-case", default="",
-                    choices=["", "zsolve", "spmm", "build", "batch"],
+                    choices=["", "zsolve", "spmm", "build", "batch", "rows"],
                     help="run one device case and print the library's "
                          "per-kernel event timing (for ncu captures of "
                          "single kernels): zsolve = a blocked Z-solve of a "
@@ -85,6 +85,11 @@ def parse():
                     help="batch case: shifts (log-spaced in [1e-3, 1e3])")
     ap.add_argument("--kc-rank", type=int, default=200,
                     help="batch case: ell (rank cap = ell - 20)")
+    ap.add_argument("--kc-ranks", type=int, default=2,
+                    help="rows case: row slabs, run as threads of this "
+                         "process on one GPU (the ranks serialise on the "
+                         "device, so the case measures the sharded "
+                         "algorithm's extra work, not multi-GPU time)")
     ap.add_argument("--config", default="c2", choices=["c2", "c3", "c4", "c5"],
                     help="c2: the headline job (default); c3 / c4: the "
                          "mixed-precision 3D extend and the batched-shift "
@@ -932,6 +937,64 @@ def run_c5(args):
     return line
 
 
+def rows_case(L, cfg, ell, rtol, nranks):
+    """The build over row slabs against the one-rank build of the same
+    operators: per-column PCG iterations (the rank-local block-Jacobi
+    preconditioner against the global V-cycle), halo exchanges and bytes,
+    all-reduce count, spectrum agreement, and the wall time with the ranks
+    as threads sharing one GPU."""
+    import threading
+    N = cfg["N"]
+    gopts = L.glr_opts(ell=ell, seed=0, trunc_rel=0.0)
+    popts = L.prior_opts(ksp_rtol=rtol)
+    pr = L.Prior(Z=L.Mat(cfg["Z"]), mass=cfg["mass"], opts=popts)
+    t0 = time.time()
+    g1 = L.Glr(L.Mat(cfg["B"]), pr, gopts)
+    one = {"build_s": round(time.time() - t0, 3),
+           "mean_col_iters": round(pr.info()["mean_col_iters"], 2)}
+    lam1 = g1.eigs().copy()
+    del g1, pr
+    comms = L.local_rows_comms(nranks)
+    res, errs = [None] * nranks, []
+
+    def rank(r):
+        try:
+            a, b = L.shard_range(N, nranks, r)
+            Bm = L.Mat(L.rows_slab(cfg["B"], a, b), rows=(N, comms[r]))
+            Zm = L.Mat(L.rows_slab(cfg["Z"], a, b), rows=(N, comms[r]))
+            p = L.Prior(Z=Zm, mass=cfg["mass"][a:b], opts=popts)
+            g = L.Glr(Bm, p, gopts)
+            res[r] = {"rows": b - a, "ghosts_B": Bm.rows_info()[2],
+                      "ghosts_Z": Zm.rows_info()[2],
+                      "halo_B": Bm.rows_traffic()[:2],
+                      "halo_Z": Zm.rows_traffic()[:2],
+                      "mean_col_iters": p.info()["mean_col_iters"],
+                      "lam": g.eigs().copy()}
+            del g, p, Bm, Zm
+        except Exception as e:
+            errs.append(repr(e))
+
+    t0 = time.time()
+    ts = [threading.Thread(target=rank, args=(r,)) for r in range(nranks)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    wall = time.time() - t0
+    L.free_local_rows_comms(comms)
+    if errs:
+        raise RuntimeError(errs)
+    lam = res[0]["lam"]
+    return {"one_rank": one,
+            "slabs": {"ranks": nranks, "wall_s_threads_one_gpu": round(wall, 3),
+                      "mean_col_iters": round(res[0]["mean_col_iters"], 2),
+                      "per_rank": [{k: v for k, v in r.items() if k != "lam"}
+                                   for r in res],
+                      "lam_max_abs_diff_rel": float(
+                          np.abs(lam - lam1).max() / np.abs(lam1).max()),
+                      "kept": int(len(lam))}}
+
+
 def run_kernel_case(args):
     """One device case through the C ABI with the per-kernel event
     registry on; prints the wall time and each kernel's launches, time and
@@ -987,6 +1050,8 @@ def run_kernel_case(args):
             info[name] = {"call_ms": [round(t, 3) for t in ts],
                           "batch": g.batch_info()}
             del g
+    elif args.kernel_case == "rows":
+        info = rows_case(L, cfg, w, args.kc_rtol, args.kc_ranks)
     else:
         B, Z = L.Mat(cfg["B"]), L.Mat(cfg["Z"])
         pr = L.Prior(Z=Z, mass=cfg["mass"],
