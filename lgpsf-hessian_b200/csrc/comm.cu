@@ -11,11 +11,12 @@
  * communicator of their own (for example over NCCL).
  *
  * lgh_rows_local_create gives the same for the build over row slabs: an
- * all-reduce (host-staged, summed in rank order, so identical on every
- * rank) and the halo all-to-all (device to device copies of each peer's
- * chunk).
+ * all-reduce (every rank sums all ranks' device buffers in rank order, so
+ * the result is identical on every rank) and the halo all-to-all (device
+ * to device copies of each peer's chunk).
  */
 
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <mutex>
@@ -43,7 +44,18 @@ struct RankCtx
 {
   Shared *sh;
   int rank;
+  double *sum = nullptr;        /* row slabs: this rank's all-reduce scratch */
+  size_t sum_n = 0;
 };
+
+/* y[i] += x[i] */
+__global__ void
+k_local_add (size_t n, const double *__restrict__ x, double *__restrict__ y)
+{
+  for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t) gridDim.x * blockDim.x)
+    y[i] += x[i];
+}
 
 /* a reusable barrier with a time limit; false when it ran out */
 bool
@@ -85,31 +97,50 @@ local_allgather (const void *send, void *recv, size_t len, void *ctx)
   return meet (sh) ? 0 : 1;
 }
 
-/* row slabs: every rank stages its buffer on the host, all ranks sum the
- * stages in rank order (the same additions on every rank, so the same
- * result), then wait before a stage may be overwritten */
+/* row slabs: every rank posts its device buffer; each rank sums all
+ * posted buffers in rank order into its scratch on the device (the same
+ * additions on every rank, so the same result), waits until every rank
+ * has read every buffer, and only then overwrites its own */
 int
 local_allreduce (double *buf, size_t count, void *ctx)
 {
   RankCtx *rc = (RankCtx *) ctx;
   Shared *sh = rc->sh;
-  std::vector<double> &mine = sh->stage[rc->rank];
-  mine.resize (count);
-  if (cudaMemcpy (mine.data (), buf, count * sizeof (double),
-                  cudaMemcpyDeviceToHost) != cudaSuccess)
-    return 2;
-  if (!meet (sh)) return 1;
-  std::vector<double> sum (count, 0.);
   int rcode = 0;
-  for (int r = 0; r < sh->size; r++) {
-    if (sh->stage[r].size () != count) rcode = 3;
+  if (rc->sum_n < count) {
+    cudaFree (rc->sum);
+    rc->sum = nullptr;
+    rc->sum_n = 0;
+    if (cudaMalloc ((void **) &rc->sum, count * sizeof (double)) == cudaSuccess)
+      rc->sum_n = count;
     else
-      for (size_t i = 0; i < count; i++) sum[i] += sh->stage[r][i];
+      rcode = 2;
   }
-  if (!rcode && cudaMemcpy (buf, sum.data (), count * sizeof (double),
-                            cudaMemcpyHostToDevice) != cudaSuccess)
-    rcode = 2;
+  {
+    std::lock_guard<std::mutex> lk (sh->mu);
+    sh->posted[rc->rank] = buf;
+    sh->stage[rc->rank].assign (1, (double) count);
+  }
   if (!meet (sh)) return 1;
+  for (int r = 0; r < sh->size && !rcode; r++)
+    if (sh->stage[r].size () != 1 || sh->stage[r][0] != (double) count) rcode = 3;
+  if (!rcode) {
+    const int grid = (int) std::min<size_t> ((count + 255) / 256, 4096);
+    if (cudaMemcpy (rc->sum, sh->posted[0], count * sizeof (double),
+                    cudaMemcpyDeviceToDevice) != cudaSuccess)
+      rcode = 2;
+    for (int r = 1; r < sh->size && !rcode; r++) {
+      k_local_add<<<grid > 0 ? grid : 1, 256>>> (count,
+                                                 (const double *) sh->posted[r],
+                                                 rc->sum);
+      if (cudaGetLastError () != cudaSuccess) rcode = 2;
+    }
+    if (!rcode && cudaDeviceSynchronize () != cudaSuccess) rcode = 2;
+  }
+  if (!meet (sh)) return 1;
+  if (!rcode && cudaMemcpy (buf, rc->sum, count * sizeof (double),
+                            cudaMemcpyDeviceToDevice) != cudaSuccess)
+    rcode = 2;
   return rcode;
 }
 
@@ -216,7 +247,9 @@ lgh_rows_local_destroy (lgh_rows_comm_t *comms)
   const int size = comms[0].size;
   Shared *sh = ((RankCtx *) comms[0].ctx)->sh;
   for (int r = 0; r < size; r++) {
-    delete (RankCtx *) comms[r].ctx;
+    RankCtx *rc = (RankCtx *) comms[r].ctx;
+    if (rc) cudaFree (rc->sum);
+    delete rc;
     comms[r].ctx = nullptr;
   }
   delete sh;

@@ -41,10 +41,21 @@ struct RowsPrior
 {
   Csr diag;
   int ld = 0;
-  DBuf<double> X, R, P, Q, Z;       /* nloc x ld iterates                 */
+  DBuf<double> X, R, P, Q, Z, T;    /* nloc x ld iterates                 */
   DBuf<double> part, sums;          /* column-sum partials and results    */
   DBuf<double> coef;                /* per-column alpha / beta (device)   */
   std::vector<double> h;            /* host mirror of the sums            */
+  /* the global coarse correction (AMG type, hierarchies of two levels or
+   * more): the coarse space is every rank's first-level aggregates (the
+   * local prolongator P_r of the diagonal block's hierarchy), the coarse
+   * operator A_c = P^T Z P of the whole Z (couplings across slabs
+   * included), replicated on every rank with a hierarchy of its own.
+   * coarse: 0 none (block Jacobi), 1 additive, 2 symmetric multiplicative */
+  int coarse = 0;
+  int64_t nc = 0, nc_loc = 0, coff = 0;
+  Csr cA;
+  Hierarchy *cmg = nullptr;
+  DBuf<double> rc, ec;              /* nc x ld coarse blocks              */
 };
 
 /* the same communicator (rank, size, callbacks, context) */

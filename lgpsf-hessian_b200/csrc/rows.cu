@@ -196,6 +196,16 @@ k_rows_dir (int64_t n, int ld, const double *__restrict__ beta,
     P[e] = fma (beta[e % ld], P[e], Z[e]);
 }
 
+/* out = a X + b Y (elementwise; out may alias X or Y) */
+__global__ void
+k_rows_axpby (int64_t total, double a, const double *X, double b,
+              const double *Y, double *out)
+{
+  for (int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t) gridDim.x * blockDim.x)
+    out[e] = a * X[e] + b * Y[e];
+}
+
 /* z = D^{-1} r (the Jacobi type of the rank-local preconditioner) */
 __global__ void
 k_rows_jacobi (int64_t n, int ld, const double *__restrict__ dinv,
@@ -304,6 +314,261 @@ rows_plan_free (RowsPlan *P)
 
 /* ---- the row-sharded prior ---------------------------------------------- */
 
+/* one all-to-all of host int64 arrays through device buffers */
+static int
+rows_exchange_i64 (const lgh_rows_comm_t &c, const std::vector<int64_t> &send,
+                   const std::vector<size_t> &scount,
+                   std::vector<int64_t> &recv,
+                   const std::vector<size_t> &rcount)
+{
+  const int np = c.size;
+  std::vector<size_t> sb (np), rb (np);
+  size_t rtot = 0;
+  for (int p = 0; p < np; p++) {
+    sb[p] = scount[p] * sizeof (int64_t);
+    rb[p] = rcount[p] * sizeof (int64_t);
+    rtot += rcount[p];
+  }
+  DBuf<int64_t> ds, dr;
+  LGH_TRY (ds.alloc (std::max<size_t> (send.size (), 1)));
+  LGH_TRY (dr.alloc (std::max<size_t> (rtot, 1)));
+  if (!send.empty ())
+    LGH_CUDA (cudaMemcpy (ds.p, send.data (), send.size () * sizeof (int64_t),
+                          cudaMemcpyHostToDevice));
+  LGH_CHECK (c.alltoallv (ds.p, sb.data (), dr.p, rb.data (), c.ctx) == 0,
+             LGH_ERR_GPU, "row slabs: the plan exchange failed (rank %d of %d)",
+             c.rank, c.size);
+  recv.resize (rtot);
+  if (rtot)
+    LGH_CUDA (cudaMemcpy (recv.data (), dr.p, rtot * sizeof (int64_t),
+                          cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+template <typename T>
+static int
+host_copy (std::vector<T> &h, const T *d, int64_t count)
+{
+  h.resize (count);
+  if (count)
+    LGH_CUDA (cudaMemcpy (h.data (), d, count * sizeof (T),
+                          cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+static int64_t
+pack_double (double v)
+{
+  int64_t b;
+  memcpy (&b, &v, sizeof b);
+  return b;
+}
+
+static double
+unpack_double (int64_t b)
+{
+  double v;
+  memcpy (&v, &b, sizeof v);
+  return v;
+}
+
+/* The global coarse correction (RowsPrior): the global coarse numbering
+ * (rank r's aggregates after those of ranks < r), the P rows of the Z
+ * halo's ghost rows from their owners, this rank's rows of
+ * A_c = P^T Z P, then every rank's rows to every rank and the coarse
+ * hierarchy.  All ranks compute the same A_c and build the same
+ * hierarchy on it. */
+static int
+rows_coarse_setup (lgh_prior *p, int mode)
+{
+  RowsPrior &W = *p->rows;
+  Hierarchy *h = p->mg;
+  W.coarse = 0;
+  if (mode <= 0 || h == nullptr || h->lev.size () < 2) return 0;
+  const RowsPlan &Zp = *p->Z->rows;
+  const lgh_rows_comm_t &cm = Zp.comm;
+  const int np = cm.size, me = cm.rank;
+  cudaStream_t s = stream ();
+  const Csr &Pd = h->lev[0].P;
+  const int64_t nloc = Pd.n, ncl = h->lev[1].n;
+  std::vector<int64_t> prp, zrp;
+  std::vector<int32_t> pci, zci;
+  std::vector<double> pva, zva;
+  LGH_TRY (host_copy (prp, Pd.rowptr, nloc + 1));
+  LGH_TRY (host_copy (pci, Pd.colidx, Pd.nnz));
+  LGH_TRY (host_copy (pva, Pd.vals, Pd.nnz));
+  const Csr &Zc = p->Z->csr;
+  LGH_TRY (host_copy (zrp, Zc.rowptr, Zc.n + 1));
+  LGH_TRY (host_copy (zci, Zc.colidx, Zc.nnz));
+  LGH_TRY (host_copy (zva, Zc.vals, Zc.nnz));
+
+  /* coarse offsets: each rank's count in its slot, summed */
+  std::vector<double> cnt (np, 0.);
+  cnt[me] = (double) ncl;
+  {
+    DBuf<double> d;
+    LGH_TRY (d.alloc (np));
+    LGH_CUDA (cudaMemcpy (d.p, cnt.data (), np * sizeof (double),
+                          cudaMemcpyHostToDevice));
+    LGH_TRY (rows_allreduce (cm, d.p, np, s));
+    LGH_CUDA (cudaMemcpy (cnt.data (), d.p, np * sizeof (double),
+                          cudaMemcpyDeviceToHost));
+  }
+  std::vector<int64_t> coff (np + 1, 0);
+  for (int q = 0; q < np; q++) coff[q + 1] = coff[q] + (int64_t) llround (cnt[q]);
+  const int64_t nc = coff[np], c0 = coff[me];
+  LGH_CHECK (nc < (int64_t) INT32_MAX, LGH_ERR_ARG_OUTOFRANGE,
+             "row slabs: coarse space of %lld rows", (long long) nc);
+
+  /* the P rows of the Z halo's send rows, to the peers that hold them as
+   * ghosts: per-row counts, then (global coarse column, value) pairs */
+  std::vector<int64_t> sidx;
+  LGH_TRY (host_copy (sidx, Zp.sidx.p, Zp.nsend));
+  std::vector<int64_t> snnz, sent, gnnz, gent;
+  std::vector<size_t> rs (np), rr (np), es (np, 0), er (np, 0);
+  for (int q = 0, k = 0; q < np; q++) {
+    rs[q] = (size_t) Zp.send_rows[q];
+    rr[q] = (size_t) Zp.recv_rows[q];
+    for (int64_t t = 0; t < Zp.send_rows[q]; t++, k++) {
+      const int64_t i = sidx[k];
+      snnz.push_back (prp[i + 1] - prp[i]);
+      for (int64_t e = prp[i]; e < prp[i + 1]; e++) {
+        sent.push_back (c0 + pci[e]);
+        sent.push_back (pack_double (pva[e]));
+      }
+      es[q] += 2 * (size_t) (prp[i + 1] - prp[i]);
+    }
+  }
+  LGH_TRY (rows_exchange_i64 (cm, snnz, rs, gnnz, rr));
+  for (int q = 0, g = 0; q < np; q++)
+    for (int64_t t = 0; t < Zp.recv_rows[q]; t++, g++) er[q] += 2 * (size_t) gnnz[g];
+  LGH_TRY (rows_exchange_i64 (cm, sent, es, gent, er));
+  std::vector<int64_t> grp (Zp.nghost + 1, 0);
+  for (int64_t g = 0; g < Zp.nghost; g++) grp[g + 1] = grp[g] + gnnz[g];
+
+  /* this rank's coarse rows: A_c[I, :] = sum_i P[i, I] (Z P)[i, :] */
+  std::vector<int64_t> tp (ncl + 1, 0), ti (pci.size ());
+  std::vector<double> tv (pci.size ());
+  for (size_t e = 0; e < pci.size (); e++) tp[pci[e] + 1]++;
+  for (int64_t I = 0; I < ncl; I++) tp[I + 1] += tp[I];
+  {
+    std::vector<int64_t> fill (tp.begin (), tp.end () - 1);
+    for (int64_t i = 0; i < nloc; i++)
+      for (int64_t e = prp[i]; e < prp[i + 1]; e++) {
+        const int64_t at = fill[pci[e]]++;
+        ti[at] = i;
+        tv[at] = pva[e];
+      }
+  }
+  std::vector<double> acc (nc, 0.);
+  std::vector<char> mark (nc, 0);
+  std::vector<int64_t> list, arp (ncl + 1, 0), aci;
+  std::vector<double> ava;
+  auto add = [&] (int64_t J, double v) {
+    if (!mark[J]) { mark[J] = 1; list.push_back (J); }
+    acc[J] += v;
+  };
+  for (int64_t I = 0; I < ncl; I++) {
+    list.clear ();
+    for (int64_t t = tp[I]; t < tp[I + 1]; t++) {
+      const int64_t i = ti[t];
+      for (int64_t k = zrp[i]; k < zrp[i + 1]; k++) {
+        const int64_t c = zci[k];
+        const double f = tv[t] * zva[k];
+        if (c < nloc) {
+          for (int64_t e = prp[c]; e < prp[c + 1]; e++)
+            add (c0 + pci[e], f * pva[e]);
+        } else {
+          const int64_t g = c - nloc;
+          for (int64_t e = grp[g]; e < grp[g + 1]; e++)
+            add (gent[2 * e], f * unpack_double (gent[2 * e + 1]));
+        }
+      }
+    }
+    std::sort (list.begin (), list.end ());
+    for (int64_t J : list) {
+      aci.push_back (J);
+      ava.push_back (acc[J]);
+      acc[J] = 0.;
+      mark[J] = 0;
+    }
+    arp[I + 1] = (int64_t) aci.size ();
+  }
+
+  /* every rank's rows to every rank */
+  std::vector<int64_t> mynnz (ncl), myent;
+  for (int64_t I = 0; I < ncl; I++) mynnz[I] = arp[I + 1] - arp[I];
+  for (size_t e = 0; e < aci.size (); e++) {
+    myent.push_back (aci[e]);
+    myent.push_back (pack_double (ava[e]));
+  }
+  std::vector<int64_t> bnnz, bent, rnnz, rent;
+  std::vector<size_t> ns (np, 0), nr (np, 0), xs (np, 0), xr (np, 0);
+  for (int q = 0; q < np; q++) {
+    if (q == me) continue;
+    bnnz.insert (bnnz.end (), mynnz.begin (), mynnz.end ());
+    bent.insert (bent.end (), myent.begin (), myent.end ());
+    ns[q] = (size_t) ncl;
+    nr[q] = (size_t) (coff[q + 1] - coff[q]);
+    xs[q] = myent.size ();
+  }
+  LGH_TRY (rows_exchange_i64 (cm, bnnz, ns, rnnz, nr));
+  {
+    size_t k = 0;
+    for (int q = 0; q < np; q++) {
+      if (q == me) continue;
+      for (size_t t = 0; t < nr[q]; t++, k++) xr[q] += 2 * (size_t) rnnz[k];
+    }
+  }
+  LGH_TRY (rows_exchange_i64 (cm, bent, xs, rent, xr));
+  std::vector<int64_t> crp (nc + 1, 0);
+  std::vector<int32_t> cci;
+  std::vector<double> cva;
+  {
+    size_t kr = 0, ke = 0;
+    for (int q = 0; q < np; q++) {
+      const int64_t rows_q = coff[q + 1] - coff[q];
+      for (int64_t I = 0; I < rows_q; I++) {
+        const int64_t gI = coff[q] + I;
+        if (q == me) {
+          for (int64_t e = arp[I]; e < arp[I + 1]; e++) {
+            cci.push_back ((int32_t) aci[e]);
+            cva.push_back (ava[e]);
+          }
+        } else {
+          const int64_t m = rnnz[kr++];
+          for (int64_t t = 0; t < m; t++, ke++) {
+            cci.push_back ((int32_t) rent[2 * ke]);
+            cva.push_back (unpack_double (rent[2 * ke + 1]));
+          }
+        }
+        crp[gI + 1] = (int64_t) cci.size ();
+      }
+    }
+  }
+  Csr &A = W.cA;
+  A.n = nc;
+  A.nnz = (int64_t) cci.size ();
+  LGH_TRY (dalloc ((void **) &A.rowptr, (size_t) (nc + 1) * sizeof (int64_t)));
+  LGH_TRY (dalloc ((void **) &A.colidx, (size_t) A.nnz * sizeof (int32_t) + 16));
+  LGH_TRY (dalloc ((void **) &A.vals, (size_t) A.nnz * sizeof (double) + 16));
+  LGH_CUDA (cudaMemcpy (A.rowptr, crp.data (), (nc + 1) * sizeof (int64_t),
+                        cudaMemcpyHostToDevice));
+  LGH_CUDA (cudaMemcpy (A.colidx, cci.data (), A.nnz * sizeof (int32_t),
+                        cudaMemcpyHostToDevice));
+  LGH_CUDA (cudaMemcpy (A.vals, cva.data (), A.nnz * sizeof (double),
+                        cudaMemcpyHostToDevice));
+  LGH_TRY (csr_finish (A));
+  const lgh_prior_mat_opts_t &o = p->mopts;
+  LGH_TRY (mg_build (A, o.tile, o.smoother_top, o.nu_force > 0 ? o.nu_force : 2,
+                     &W.cmg));
+  W.coarse = mode;
+  W.nc = nc;
+  W.nc_loc = ncl;
+  W.coff = c0;
+  return 0;
+}
+
 /* diag = Z restricted to the owned rows and columns (local columns below
  * nloc), and its multigrid hierarchy for the AMG type */
 int
@@ -355,6 +620,10 @@ rows_prior_setup (lgh_prior *p)
     const lgh_prior_mat_opts_t &o = p->mopts;
     const int nu = o.nu_force > 0 ? o.nu_force : 2;
     LGH_TRY (mg_build (D, o.tile, o.smoother_top, nu, &p->mg));
+    /* LGH_ROWS_COARSE: 0 block Jacobi alone, 1 additive, 2 symmetric
+     * multiplicative coarse correction (default) */
+    const char *env = getenv ("LGH_ROWS_COARSE");
+    LGH_TRY (rows_coarse_setup (p, env ? atoi (env) : 2));
   }
   return 0;
 }
@@ -363,6 +632,8 @@ void
 rows_prior_free (RowsPrior *R)
 {
   if (!R) return;
+  if (R->cmg) mg_destroy (R->cmg);     /* borrows cA's arrays */
+  csr_free (R->cA);
   csr_free (R->diag);
   delete R;
 }
@@ -414,11 +685,52 @@ rows_zsolve (lgh_prior *p, int w, const T *X, int ldx, const double *s_in,
     LGH_CUDA (cudaStreamSynchronize (s));
     return 0;
   };
-  auto precond = [&] () -> int {
-    if (p->mg) return mg_vcycle<double> (p->mg, W.R.p, W.Z.p, ld, w, s);
-    k_rows_jacobi<<<egrid ((int64_t) nn), 256, 0, s>>> (n, ld, W.diag.dinv,
-                                                         W.R.p, W.Z.p);
+  if (W.coarse) {
+    LGH_TRY (W.rc.alloc ((size_t) W.nc * ld));
+    LGH_TRY (W.ec.alloc ((size_t) W.nc * ld));
+    if (W.coarse == 2) LGH_TRY (W.T.alloc (nn));
+  }
+  /* t = r - Z z (the symmetric multiplicative form's residuals) */
+  auto resid = [&] (const double *z) -> int {
+    LGH_TRY (rows_mult_block<double> (p->Z, z, ld, W.T.p, ld, w, s));
+    k_rows_axpby<<<egrid ((int64_t) nn), 256, 0, s>>> ((int64_t) nn, 1., W.R.p,
+                                                        -1., W.T.p, W.T.p);
     LGH_LAUNCH_CHECK ();
+    return 0;
+  };
+  /* z += P V_c (P^T t): the coarse rows of every rank summed into one
+   * zero-filled nc-row block (exact: the other slots add zeros) */
+  auto coarse = [&] (const double *t) -> int {
+    const MgLevel &l0 = p->mg->lev[0];
+    LGH_CUDA (cudaMemsetAsync (W.rc.p, 0, (size_t) W.nc * ld * sizeof (double), s));
+    LGH_TRY (launch_spmm<double> (l0.R, t, ld, W.rc.p + (size_t) W.coff * ld,
+                                  ld, w, s));
+    LGH_TRY (rows_allreduce (cm, W.rc.p, (size_t) W.nc * ld, s));
+    LGH_TRY (mg_vcycle<double> (W.cmg, W.rc.p, W.ec.p, ld, w, s));
+    return launch_spmm_mode<double> (l0.P, W.ec.p + (size_t) W.coff * ld, ld,
+                                     W.Z.p, ld, w, 1, nullptr, 0, s);
+  };
+  auto precond = [&] () -> int {
+    if (!p->mg) {
+      k_rows_jacobi<<<egrid ((int64_t) nn), 256, 0, s>>> (n, ld, W.diag.dinv,
+                                                           W.R.p, W.Z.p);
+      LGH_LAUNCH_CHECK ();
+      return 0;
+    }
+    LGH_TRY (mg_vcycle<double> (p->mg, W.R.p, W.Z.p, ld, w, s));
+    if (W.coarse == 1) return coarse (W.R.p);
+    if (W.coarse == 2) {
+      /* z1 = V r; z2 = z1 + P V_c P^T (r - Z z1); z = z2 + V (r - Z z2),
+       * the last V-cycle's output in Q (free between products) */
+      LGH_TRY (resid (W.Z.p));
+      LGH_TRY (coarse (W.T.p));
+      LGH_TRY (resid (W.Z.p));
+      LGH_TRY (mg_vcycle<double> (p->mg, W.T.p, W.Q.p, ld, w, s));
+      k_rows_axpby<<<egrid ((int64_t) nn), 256, 0, s>>> ((int64_t) nn, 1.,
+                                                          W.Z.p, 1., W.Q.p,
+                                                          W.Z.p);
+      LGH_LAUNCH_CHECK ();
+    }
     return 0;
   };
 
@@ -532,37 +844,6 @@ rows_agree (const lgh_rows_comm_t &c, int local_rc, const char *who)
   if (local_rc) return local_rc;
   LGH_CHECK (sum == 0., LGH_ERR_ARG_WRONG, "%s: %g other rank(s) failed", who,
              sum);
-  return 0;
-}
-
-/* one all-to-all of host int64 arrays through device buffers */
-int
-rows_exchange_i64 (const lgh_rows_comm_t &c, const std::vector<int64_t> &send,
-                   const std::vector<size_t> &scount,
-                   std::vector<int64_t> &recv,
-                   const std::vector<size_t> &rcount)
-{
-  const int np = c.size;
-  std::vector<size_t> sb (np), rb (np);
-  size_t rtot = 0;
-  for (int p = 0; p < np; p++) {
-    sb[p] = scount[p] * sizeof (int64_t);
-    rb[p] = rcount[p] * sizeof (int64_t);
-    rtot += rcount[p];
-  }
-  DBuf<int64_t> ds, dr;
-  LGH_TRY (ds.alloc (std::max<size_t> (send.size (), 1)));
-  LGH_TRY (dr.alloc (std::max<size_t> (rtot, 1)));
-  if (!send.empty ())
-    LGH_CUDA (cudaMemcpy (ds.p, send.data (), send.size () * sizeof (int64_t),
-                          cudaMemcpyHostToDevice));
-  LGH_CHECK (c.alltoallv (ds.p, sb.data (), dr.p, rb.data (), c.ctx) == 0,
-             LGH_ERR_GPU, "row slabs: the plan exchange failed (rank %d of %d)",
-             c.rank, c.size);
-  recv.resize (rtot);
-  if (rtot)
-    LGH_CUDA (cudaMemcpy (recv.data (), dr.p, rtot * sizeof (int64_t),
-                          cudaMemcpyDeviceToHost));
   return 0;
 }
 
