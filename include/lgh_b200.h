@@ -609,7 +609,7 @@ int lgh_sketch_rows (uint64_t seed, int64_t i0, int64_t n, int64_t j0, int k,
 /* ---- a build over row slabs (one rank per GPU) ---------------------------
  * The reference's MPI layout (docs/glr-woodbury-formulas.tex:76-98): B, Z,
  * the mass lumps and every N-row block are split into contiguous row slabs
- * (rank r owns rows lgh_shard_range (N, size, r)).  A row-sharded Mat
+ * (rank r owns a contiguous range of rows, ranks in order).  A row-sharded Mat
  * (lgh_mat_create_rows) carries its halo plan and the communicator; a
  * prior made from a row-sharded Z (lgh_prior_create_mat / _pc, with the
  * rank's mass lumps) is a row-sharded prior, and lgh_glr_compute on a
@@ -653,13 +653,17 @@ typedef struct lgh_rows_comm
 }
 lgh_rows_comm_t;
 
-/* This rank's rows [row0, row1) = lgh_shard_range (N, size, rank) of a
- * symmetric N x N CSR operator: rowptr (row1 - row0 + 1 entries,
- * rowptr[0] = 0), global column indices, values; host arrays, copied.
- * Collective: every rank calls it with its own rows.                     */
+/* This rank's rows [row0, row0 + nrows) of a symmetric N x N CSR
+ * operator (MatGetOwnershipRange of an MPIAIJ): rowptr (nrows + 1
+ * entries, rowptr[0] = 0), global column indices, values; host arrays,
+ * copied.  Ranks own contiguous rows in rank order covering [0, N), at
+ * least one each (any split: PETSc's layout, or lgh_shard_range's);
+ * B and Z of one build must be split alike.  Collective: every rank calls
+ * it with its own rows, and all ranks fail together on a bad split.      */
 int lgh_mat_create_rows (int64_t N, const lgh_rows_comm_t *comm,
-                         const int64_t *rowptr, const int32_t *colidx,
-                         const double *vals, lgh_Mat *A);
+                         int64_t row0, int64_t nrows, const int64_t *rowptr,
+                         const int32_t *colidx, const double *vals,
+                         lgh_Mat *A);
 /* rows of a row-sharded Mat (0 / N / 0 ghosts for an ordinary Mat)       */
 int lgh_mat_rows_info (lgh_Mat A, int64_t *row0, int64_t *row1,
                        int64_t *nghost);

@@ -885,7 +885,9 @@ lgh_glr_compute_ex (lgh_Mat B, lgh_prior_t *prior, const lgh_glr_opts_t *opts,
                "lgh_glr_compute: B and the prior must both be row-sharded "
                "or neither");
     LGH_CHECK (rows_same_comm (B->rows->comm, prior->Z->rows->comm)
-               && B->rows->N == prior->Z->rows->N, LGH_ERR_ARG_WRONG,
+               && B->rows->N == prior->Z->rows->N
+               && B->rows->row0 == prior->Z->rows->row0
+               && B->rows->row1 == prior->Z->rows->row1, LGH_ERR_ARG_WRONG,
                "lgh_glr_compute: B and the prior are sharded differently");
     LGH_CHECK (t_comm == nullptr, LGH_ERR_SUP,
                "lgh_glr_compute: row slabs and column sharding together");

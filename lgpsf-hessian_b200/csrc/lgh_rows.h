@@ -58,6 +58,12 @@ struct RowsPrior
   DBuf<double> rc, ec;              /* nc x ld coarse blocks              */
 };
 
+/* the shard plan for rank `rank` of an explicit contiguous partition
+ * (rank r owns [starts[r], starts[r + 1]); shard.cu) */
+int shard_create_ranges (int64_t N, int nranks, int rank,
+                         const int64_t *starts, const int64_t *rowptr,
+                         const int32_t *colidx, lgh_shard_t **out);
+
 /* the same communicator (rank, size, callbacks, context) */
 bool rows_same_comm (const lgh_rows_comm_t &a, const lgh_rows_comm_t &b);
 

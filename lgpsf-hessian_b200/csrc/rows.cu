@@ -12,12 +12,14 @@
  *     rows of an extended block, since ghosts are ascending global rows
  *     and ranks own contiguous ranges) and the local strip / CSR product;
  *   - a row-sharded prior solves with blocked PCG whose dot products are
- *     all-reduced (two all-reduces of up to 2 w doubles per iteration) and
- *     whose preconditioner is rank-local block Jacobi: the smoothed-
- *     aggregation V-cycle on the rank's diagonal block of Z (the role of
- *     PETSc's default parallel block-Jacobi / GAMG-per-process setting),
- *     or Jacobi.  Convergence is decided from the all-reduced sums only,
- *     so every rank takes the same iterations;
+ *     all-reduced (two all-reduces of up to 2 w doubles per iteration);
+ *     its preconditioner is the smoothed-aggregation V-cycle on the rank's
+ *     diagonal block of Z (block Jacobi) with a global coarse correction
+ *     (every rank's first-level aggregates, A_c = P^T Z P with the
+ *     couplings across slabs, replicated), applied symmetric
+ *     multiplicatively by default, or Jacobi.  Convergence is decided
+ *     from the all-reduced sums only, so every rank takes the same
+ *     iterations;
  *   - the in-process communicator runs ranks as threads of one process
  *     on one device: collectives meet on a host barrier with a time limit;
  *     no kernel ever waits for another rank.
@@ -852,9 +854,9 @@ rows_agree (const lgh_rows_comm_t &c, int local_rc, const char *who)
 extern "C" {
 
 int
-lgh_mat_create_rows (int64_t N, const lgh_rows_comm_t *comm,
-                     const int64_t *rowptr, const int32_t *colidx,
-                     const double *vals, lgh_Mat *out)
+lgh_mat_create_rows (int64_t N, const lgh_rows_comm_t *comm, int64_t row0,
+                     int64_t nrows, const int64_t *rowptr,
+                     const int32_t *colidx, const double *vals, lgh_Mat *out)
 {
   LGH_TRY (ensure_init ());
   LGH_CHECK (comm && rowptr && out, LGH_ERR_ARG_NULL,
@@ -865,23 +867,51 @@ lgh_mat_create_rows (int64_t N, const lgh_rows_comm_t *comm,
              comm->size);
   const lgh_rows_comm_t &cm = *comm;
   const int np = cm.size, me = cm.rank;
-  int64_t row0 = 0, row1 = 0;
-  lgh_shard_range (N, np, me, &row0, &row1);
-  const int64_t nloc = row1 - row0;
+  const int64_t nloc = nrows, row1 = row0 + nrows;
+
+  /* every rank's rows: one all-reduce of the (first row, count) slots */
+  std::vector<int64_t> starts (np + 1, 0);
+  int rc = 0;
+  {
+    std::vector<double> sl (2 * np, 0.);
+    sl[2 * me] = (double) row0;
+    sl[2 * me + 1] = (double) nrows;
+    DBuf<double> d;
+    LGH_TRY (d.alloc (2 * np));
+    LGH_CUDA (cudaMemcpy (d.p, sl.data (), 2 * np * sizeof (double),
+                          cudaMemcpyHostToDevice));
+    LGH_TRY (rows_allreduce (cm, d.p, 2 * np, stream ()));
+    LGH_CUDA (cudaMemcpy (sl.data (), d.p, 2 * np * sizeof (double),
+                          cudaMemcpyDeviceToHost));
+    for (int q = 0; q < np && !rc; q++) {
+      const int64_t a = (int64_t) sl[2 * q], m = (int64_t) sl[2 * q + 1];
+      if (a != starts[q] || m < 0)
+        rc = set_error (LGH_ERR_ARG_WRONG,
+                        "lgh_mat_create_rows: rank %d's rows start at %lld, "
+                        "not %lld (ranks own contiguous rows in rank order)",
+                        q, (long long) a, (long long) starts[q]);
+      starts[q + 1] = a + m;
+    }
+    if (!rc && starts[np] != N)
+      rc = set_error (LGH_ERR_ARG_WRONG,
+                      "lgh_mat_create_rows: the ranks' rows cover %lld of "
+                      "%lld", (long long) starts[np], (long long) N);
+  }
 
   /* local checks and the plan; every rank then agrees before exchanging */
-  int rc = 0;
-  if (N < np || N >= (int64_t) INT32_MAX)
+  if (rc) {
+  } else if (N < 1 || N >= (int64_t) INT32_MAX || nloc < 1)
     rc = set_error (LGH_ERR_ARG_OUTOFRANGE,
-                    "lgh_mat_create_rows: N %lld for %d ranks",
-                    (long long) N, np);
+                    "lgh_mat_create_rows: N %lld, %lld rows on rank %d",
+                    (long long) N, (long long) nloc, me);
   else if (rowptr[0] != 0 || rowptr[nloc] < 0
            || (rowptr[nloc] > 0 && (!colidx || !vals)))
     rc = set_error (LGH_ERR_ARG_WRONG,
                     "lgh_mat_create_rows: rowptr[0] must be 0 and the "
                     "arrays non-null");
   lgh_shard_t *sh = nullptr;
-  if (!rc) rc = lgh_shard_create (N, np, me, rowptr, colidx, &sh);
+  if (!rc)
+    rc = shard_create_ranges (N, np, me, starts.data (), rowptr, colidx, &sh);
   struct Guard
   {
     lgh_shard_t *s;

@@ -38,6 +38,7 @@ struct lgh_shard
 {
   int64_t N = 0, row0 = 0, row1 = 0;
   int nranks = 1, rank = 0;
+  std::vector<int64_t> starts;          /* rank r owns [starts[r], starts[r+1]) */
   std::vector<int64_t> ghosts;          /* ascending global rows            */
   std::vector<int64_t> ghost_count;     /* per owner rank                   */
   std::vector<int64_t> ghost_first;     /* offset of each owner's run       */
@@ -59,16 +60,9 @@ shard_range (int64_t N, int P, int r, int64_t *a, int64_t *b)
 static int
 shard_owner (const lgh_shard_t *sh, int64_t g)
 {
-  /* the largest r with row0(r) <= g */
-  int lo = 0, hi = sh->nranks - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) / 2;
-    int64_t a, b;
-    shard_range (sh->N, sh->nranks, mid, &a, &b);
-    if (a <= g) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
+  /* the last r with starts[r] <= g (empty ranks own nothing) */
+  const auto it = std::upper_bound (sh->starts.begin (), sh->starts.end (), g);
+  return (int) (it - sh->starts.begin ()) - 1;
 }
 
 /* rows of X listed in idx -> contiguous buf (count x w, row stride w) */
@@ -108,35 +102,33 @@ shard_grid (int64_t total)
   return (int) (g > 0 ? g : 1);
 }
 
-} /* namespace lgh */
-
-using namespace lgh;
-
-extern "C" {
-
-void
-lgh_shard_range (int64_t N, int nranks, int rank, int64_t *row0, int64_t *row1)
-{
-  if (nranks < 1 || rank < 0 || rank >= nranks) {
-    *row0 = *row1 = 0;
-    return;
-  }
-  shard_range (N, nranks, rank, row0, row1);
-}
-
+/* the plan for an explicit contiguous partition: rank r owns rows
+ * [starts[r], starts[r + 1]), starts[0] = 0, starts[nranks] = N,
+ * non-decreasing */
 int
-lgh_shard_create (int64_t N, int nranks, int rank, const int64_t *rowptr,
-                  const int32_t *colidx, lgh_shard_t **out)
+shard_create_ranges (int64_t N, int nranks, int rank, const int64_t *starts,
+                     const int64_t *rowptr, const int32_t *colidx,
+                     lgh_shard_t **out)
 {
-  LGH_CHECK (rowptr && out, LGH_ERR_ARG_NULL, "lgh_shard_create: NULL argument");
+  LGH_CHECK (rowptr && out && starts, LGH_ERR_ARG_NULL,
+             "lgh_shard_create: NULL argument");
   LGH_CHECK (N >= 1 && nranks >= 1 && rank >= 0 && rank < nranks,
              LGH_ERR_ARG_OUTOFRANGE, "lgh_shard_create: N %lld, rank %d of %d",
              (long long) N, rank, nranks);
+  LGH_CHECK (starts[0] == 0 && starts[nranks] == N, LGH_ERR_ARG_WRONG,
+             "lgh_shard_create: the ranks' rows must cover [0, %lld)",
+             (long long) N);
+  for (int r = 0; r < nranks; r++)
+    LGH_CHECK (starts[r] <= starts[r + 1], LGH_ERR_ARG_WRONG,
+               "lgh_shard_create: rank %d's rows are not contiguous after "
+               "rank %d's", r + 1, r);
   lgh_shard_t *sh = new lgh_shard_t ();
   sh->N = N;
   sh->nranks = nranks;
   sh->rank = rank;
-  shard_range (N, nranks, rank, &sh->row0, &sh->row1);
+  sh->starts.assign (starts, starts + nranks + 1);
+  sh->row0 = starts[rank];
+  sh->row1 = starts[rank + 1];
   const int64_t nloc = sh->row1 - sh->row0;
   const int64_t nnz = rowptr[nloc] - rowptr[0];
   if (nnz > 0 && colidx == nullptr) {
@@ -178,6 +170,40 @@ lgh_shard_create (int64_t N, int nranks, int rank, const int64_t *rowptr,
   sh->dsends.resize (nranks);
   *out = sh;
   return 0;
+}
+
+} /* namespace lgh */
+
+using namespace lgh;
+
+extern "C" {
+
+void
+lgh_shard_range (int64_t N, int nranks, int rank, int64_t *row0, int64_t *row1)
+{
+  if (nranks < 1 || rank < 0 || rank >= nranks) {
+    *row0 = *row1 = 0;
+    return;
+  }
+  shard_range (N, nranks, rank, row0, row1);
+}
+
+int
+lgh_shard_create (int64_t N, int nranks, int rank, const int64_t *rowptr,
+                  const int32_t *colidx, lgh_shard_t **out)
+{
+  LGH_CHECK (N >= 1 && nranks >= 1 && rank >= 0 && rank < nranks,
+             LGH_ERR_ARG_OUTOFRANGE, "lgh_shard_create: N %lld, rank %d of %d",
+             (long long) N, rank, nranks);
+  std::vector<int64_t> st (nranks + 1);
+  for (int r = 0; r < nranks; r++) {
+    int64_t a, b;
+    shard_range (N, nranks, r, &a, &b);
+    st[r] = a;
+    st[r + 1] = b;
+  }
+  return lgh::shard_create_ranges (N, nranks, rank, st.data (), rowptr, colidx,
+                                   out);
 }
 
 int

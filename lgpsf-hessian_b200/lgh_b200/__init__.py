@@ -309,7 +309,7 @@ SIGNATURES = {
     "lgh_shard_destroy": (None, [P]),
     "lgh_sketch_rows": (ctypes.c_int, [ctypes.c_uint64, I64, I64, I64,
                                        ctypes.c_int, P, I64]),
-    "lgh_mat_create_rows": (ctypes.c_int, [I64, P, P, P, P,
+    "lgh_mat_create_rows": (ctypes.c_int, [I64, P, I64, I64, P, P, P,
                                            ctypes.POINTER(P)]),
     "lgh_mat_rows_info": (ctypes.c_int, [P, P, P, P]),
     "lgh_mat_rows_traffic": (ctypes.c_int, [P, P, P, P]),
@@ -457,20 +457,24 @@ class DeviceBlock:
 
 class Mat:
     """Device CSR operator (the reference's Mat for B and Z).  With rows =
-    (N, comm): this rank's row slab of an N x N operator (csr holds the
-    rank's rows with global column indices), sharded over the row-slab
-    communicator comm (a RowsComm)."""
+    (N, comm) or (N, comm, row0): this rank's row slab of an N x N operator
+    (csr holds the rank's rows, from global row row0, with global column
+    indices; row0 defaults to lgh_shard_range's split), sharded over the
+    row-slab communicator comm (a RowsComm)."""
 
     def __init__(self, csr=None, dense=None, rows=None):
         L = load()
         self.h = P()
         if rows is not None:
-            N, comm = rows
+            N, comm = rows[0], rows[1]
             rp = np.ascontiguousarray(csr["rowptr"], dtype=np.int64)
             ci = np.ascontiguousarray(csr["colidx"], dtype=np.int32)
             va = np.ascontiguousarray(csr["vals"], dtype=np.float64)
+            row0 = rows[2] if len(rows) > 2 else \
+                shard_range(N, comm.size, comm.rank)[0]
             self._comm = comm
             _chk(L.lgh_mat_create_rows(int(N), ctypes.addressof(comm),
+                                       int(row0), len(rp) - 1,
                                        rp.ctypes.data, ci.ctypes.data,
                                        va.ctypes.data, ctypes.byref(self.h)),
                  "lgh_mat_create_rows")

@@ -64,9 +64,17 @@ def c1():
     return P.grid_problem("c1")
 
 
-def _slab(cfg, size, r):
+def petsc_split(N, size, r):
+    """PETSc's default layout: N // size rows each, the remainder on the
+    lowest ranks."""
+    q, m = divmod(N, size)
+    a = r * q + min(r, m)
+    return a, a + q + (1 if r < m else 0)
+
+
+def _slab(cfg, size, r, split=None):
     N = cfg["N"]
-    a, b = L.shard_range(N, size, r)
+    a, b = (split or L.shard_range)(N, size, r)
     return a, b, L.rows_slab(cfg["B"], a, b), L.rows_slab(cfg["Z"], a, b)
 
 
@@ -141,14 +149,14 @@ def _one_rank(cfg, gopts, exec=None, extend=0):
     return _glr_outputs(g, 0, N, N)
 
 
-def _sharded(cfg, size, gopts, exec=None, extend=0):
+def _sharded(cfg, size, gopts, exec=None, extend=0, split=None):
     N = cfg["N"]
 
     def rank(r, comm):
-        a, b, Bs, Zs = _slab(cfg, size, r)
-        pr = L.Prior(Z=L.Mat(Zs, rows=(N, comm)), mass=cfg["mass"][a:b],
+        a, b, Bs, Zs = _slab(cfg, size, r, split)
+        pr = L.Prior(Z=L.Mat(Zs, rows=(N, comm, a)), mass=cfg["mass"][a:b],
                      opts=L.prior_opts(ksp_rtol=RTOL_Z))
-        Bm = L.Mat(Bs, rows=(N, comm))
+        Bm = L.Mat(Bs, rows=(N, comm, a))
         g = L.Glr(Bm, pr, gopts, exec=exec)
         if extend:
             g.extend(extend)
@@ -190,6 +198,35 @@ def test_rows_build_matches_one_rank(cuda_device, c1, size):
     assert abs(rg - rw) <= 1e-3 * rw + 1e-10 * np.abs(want["lam"]).max()
     for ex, nbytes, _ in got["traffic"]:
         assert ex > 0 and nbytes > 0
+
+
+def test_rows_petsc_layout(cuda_device, c1):
+    """Any contiguous split works, e.g. PETSc's MPIAIJ default (4096 rows on
+    3 ranks: 1366, 1365, 1365, where the even split gives 1365, 1365,
+    1366)."""
+    assert petsc_split(c1["N"], 3, 0) != L.shard_range(c1["N"], 3, 0)
+    gopts = L.glr_opts(ell=c1["ell"], seed=11, trunc_rel=0.0)
+    want = _one_rank(c1, gopts)
+    got = _sharded(c1, 3, gopts, split=petsc_split)
+    _close(got, want)
+
+
+def test_rows_bad_split_fails_on_every_rank(cuda_device, c1):
+    """Rank 1 claims rows that leave a gap: every rank's creation fails
+    (the ranks agree on the split before any exchange)."""
+    N = c1["N"]
+
+    def rank(r, comm):
+        a, b = L.shard_range(N, 2, r)
+        if r == 1:
+            a += 8
+        try:
+            L.Mat(L.rows_slab(c1["B"], a, b), rows=(N, comm, a))
+            return 0
+        except L.LghError as e:
+            return e.code
+
+    assert _ranks(2, rank) == [62, 62]
 
 
 def test_rows_extend_matches_one_rank(cuda_device, c1):
