@@ -10,7 +10,8 @@ operators (the reference's MPI slabs give the same model, up to the
 solves' tolerance, glr-woodbury-formulas.tex:76-98):
 
   - the sharded products equal the global CSR product rows;
-  - sharded Z-solves (PCG with the rank-local block-Jacobi V-cycle) match
+  - sharded Z-solves (PCG, the block V-cycle plus the global coarse
+    correction; or Jacobi) match
     the one-rank solves to the solve tolerance;
   - the sharded build keeps the same spectrum (1e-8 of lambda_max), the
     same logdet (1e-9) and the same solve / sample / apply (1e-7), in FP64
