@@ -719,10 +719,13 @@ int lgh_test_zsolve (lgh_prior_t *prior, int w, const double *X, double *Y,
 /* one Chebyshev-Jacobi smoothing step of a square CSR Mat (n x w row-major
  * host blocks) with the smoother's kernel: X in place, Rout = Ro - A d_new,
  * Dout = d_new (flags & 4), d_new = a Do + b D^{-1} Ro (flags & 1: a Do
- * left out; flags & 2: X taken as zero).                                  */
+ * left out; flags & 2: X taken as zero; flags & 8: only Rout written;
+ * flags & 16: Do is the residual given to a flags & 8 first step with
+ * coefficient bp, whose d and x this step forms).                        */
 int lgh_test_cheb_step (lgh_Mat A, int w, double a, double b, int flags,
                         int fp32, double *X, const double *Ro,
-                        const double *Do, double *Rout, double *Dout);
+                        const double *Do, double *Rout, double *Dout,
+                        double bp);
 int lgh_test_gram (int64_t n, int w, const double *X, double *G);
 int lgh_test_gemm_nn (int64_t n, int k, int m, const double *X,
                       const double *M, double *Y);

@@ -42,7 +42,7 @@ down (T *h, const DBuf<T> &d, size_t n)
 template <typename T>
 static int
 test_cheb (lgh_Mat A, int w, double a, double b, int flags, double *X, const double *Ro, const double *Do, double *Rout,
-           double *Dout)
+           double *Dout, double bp)
 {
   const int64_t n = A->csr.n;
   const int ld = round_ld (w);
@@ -63,7 +63,7 @@ test_cheb (lgh_Mat A, int w, double a, double b, int flags, double *X, const dou
   LGH_CUDA (cudaMemset (drn.p, 0, cnt * sizeof (T)));
   LGH_CUDA (cudaMemset (ddn.p, 0, cnt * sizeof (T)));
   LGH_TRY (launch_cheb_step<T> (A->csr, dx.p, dro.p, drn.p, ddo.p, ddn.p, ld, a, b,
-                                flags, stream ()));
+                                flags, stream (), bp));
   LGH_CUDA (cudaStreamSynchronize (stream ()));
   LGH_TRY (down (hx.data (), dx, cnt));
   LGH_TRY (down (hr.data (), drn, cnt));
@@ -182,7 +182,7 @@ lgh_test_spmm (lgh_Mat A, int w, const double *X, double *Y, int fp32)
 int
 lgh_test_cheb_step (lgh_Mat A, int w, double a, double b, int flags,
                     int fp32, double *X, const double *Ro,
-                    const double *Do, double *Rout, double *Dout)
+                    const double *Do, double *Rout, double *Dout, double bp)
 {
   LGH_TRY (ensure_init ());
   LGH_CHECK (A && A->kind == 0 && X && Ro && Rout, LGH_ERR_ARG_NULL,
@@ -190,8 +190,8 @@ lgh_test_cheb_step (lgh_Mat A, int w, double a, double b, int flags,
   LGH_CHECK (A->csr.ncols == 0 || A->csr.ncols == A->csr.n, LGH_ERR_ARG_WRONG,
              "lgh_test_cheb_step: square CSR Mat");
   LGH_CHECK (w >= 1, LGH_ERR_ARG_OUTOFRANGE, "lgh_test_cheb_step: w");
-  return fp32 ? test_cheb<float> (A, w, a, b, flags, X, Ro, Do, Rout, Dout)
-              : test_cheb<double> (A, w, a, b, flags, X, Ro, Do, Rout, Dout);
+  return fp32 ? test_cheb<float> (A, w, a, b, flags, X, Ro, Do, Rout, Dout, bp)
+              : test_cheb<double> (A, w, a, b, flags, X, Ro, Do, Rout, Dout, bp);
 }
 
 /* Y = Z^{-1} X through the prior's blocked solve, n x w row-major */

@@ -50,16 +50,25 @@ int mg_vcycle (Hierarchy *h, const T *B, T *X, int ld, int w, cudaStream_t s,
 /* a Chebyshev step on a CSR operator with the Jacobi PC (zsolve.cu):
  * d_new = a d + b D^{-1} r; x += d_new; r_new = r - A d_new.  flags:
  * CHEB_FIRST (no d yet: a ignored, D not read), CHEB_ZERO_X (x is zero:
- * X not read, only written), CHEB_STORE_D (write d_new for a next step) */
-enum { CHEB_FIRST = 1, CHEB_ZERO_X = 2, CHEB_STORE_D = 4 };
+ * X not read, only written), CHEB_STORE_D (write d_new for a next step),
+ * CHEB_R_ONLY (write r_new alone: neither x nor d), CHEB_PREV_R (the
+ * previous step was a first step with coefficient bp run with
+ * CHEB_R_ONLY: Do holds its input residual r_prev, and its d = bp D^{-1}
+ * r_prev and its x are formed here with the same roundings, so the pair
+ * gives the same bits as two ordinary steps) */
+enum { CHEB_FIRST = 1, CHEB_ZERO_X = 2, CHEB_STORE_D = 4, CHEB_R_ONLY = 8,
+       CHEB_PREV_R = 16 };
 template <typename T>
 int launch_cheb_step (const Csr &A, T *X, const T *Ro, T *Rn, const T *Do,
                       T *Dn, int ld, double a, double b, int flags,
-                      cudaStream_t s);
-/* the same step's x update alone, for a last step whose r_new is unused */
+                      cudaStream_t s, double bp = 0.);
+/* the same step's x update alone, for a last step whose r_new is unused;
+ * bp != 0: D holds the residual of a CHEB_R_ONLY first step with
+ * coefficient bp (as CHEB_PREV_R above) */
 template <typename T>
 int launch_cheb_tail (const Csr &A, T *X, const T *R, const T *D, int ld,
-                      double a, double b, int first, cudaStream_t s);
+                      double a, double b, int first, cudaStream_t s,
+                      double bp = 0.);
 
 int csr_finish (Csr &A);
 void csr_free (Csr &A);

@@ -772,6 +772,38 @@ mg_smooth (const MgLevel &lv, T *X, const T *B, T *R, T *Ra, T *D0, T *D1,
   const T *Ro = pre ? B : R;
   T *Rn = pre ? R : Ra;
   T *Do = D0, *Dn = D1;
+  if (lv.nu == 2) {
+    /* the two-step polynomial in 6 block passes instead of 9: the first
+     * step stores its residual alone, the second forms the first step's d
+     * and x from that step's input residual (the same roundings, so the
+     * same bits as two ordinary steps) */
+    const double b1 = 1.0 / theta;
+    const double rho = 1.0 / (2.0 * sigma1 - rho_old);
+    const double a2 = rho * rho_old, b2 = 2.0 * rho / delta;
+    const int f1 = CHEB_FIRST | CHEB_R_ONLY | (pre ? CHEB_ZERO_X : 0);
+    if (tr) LGH_TRY (tr->begin (K_MG_SMOOTH, sbase + 2. * sblk, s));
+    LGH_TRY (launch_cheb_step<T> (lv.A, X, Ro, Rn, nullptr, nullptr, ld, 0.,
+                                  b1, f1, s));
+    if (tr) LGH_TRY (tr->end (s));
+    T *R2 = (Rn == R) ? Ra : R;
+    if (pre) {
+      /* reads r1 (gathered), r0 = B (gathered); writes x, r2 */
+      if (tr) LGH_TRY (tr->begin (K_MG_SMOOTH, sbase + 4. * sblk
+                                  + (double) lv.n * sizeof (T), s));
+      LGH_TRY (launch_cheb_step<T> (lv.A, X, Rn, R2, Ro, nullptr, ld, a2, b2,
+                                    CHEB_PREV_R | CHEB_ZERO_X, s, b1));
+      if (tr) LGH_TRY (tr->end (s));
+      if (Rout) *Rout = R2;
+    } else {
+      /* reads x, r0, r1; writes x (no Z product) */
+      if (tr) LGH_TRY (tr->begin (K_MG_TAIL, 4. * sblk
+                                  + (double) lv.n * sizeof (T), s));
+      LGH_TRY (launch_cheb_tail<T> (lv.A, X, Rn, Ro, ld, a2, b2, 0, s, b1));
+      if (tr) LGH_TRY (tr->end (s));
+      if (Rout) *Rout = nullptr;
+    }
+    return 0;
+  }
   for (int k = 1; k <= lv.nu; k++) {
     double a, b;
     if (k == 1) { a = 0.; b = 1.0 / theta; }

@@ -311,14 +311,20 @@ k_pcg_upd (ZK z, const T *__restrict__ dinv, T *__restrict__ X,
 
 /* ---- Chebyshev: d_new = a d + b D^{-1} r (on the fly at neighbours),
  *      x += d_new, r_new = r - Z d_new (zsolve_impl.h:108-141) ----------- */
-template <typename T, int CH>
+template <typename T, int CH, bool PR = false>
 __global__ void __launch_bounds__ (ZS_THREADS, (CH * (16 / sizeof (T)) <= 8 ? 4 : 2))
 k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ vdv,
         const T *__restrict__ dinv, T *__restrict__ X,
         const T *__restrict__ Rold, T *__restrict__ Rnew,
         const T *__restrict__ Dold, T *__restrict__ Dnew, int ld, int nvec,
-        int glog, T a, T b, int flags)
+        int glog, T a, T b, int flags, T bp)
 {
+  /* PR: the previous step was a first step (d = bp D^{-1} r_prev) that
+   * stored only its residual; Dold then holds r_prev, and the previous d
+   * and x are formed here with that step's roundings: d_prev = (bp
+   * dinv_j) r_prev_j at every neighbour and at the row, x_prev = d_prev
+   * (from x = 0) or x + d_prev.  CHEB_R_ONLY: store the new residual
+   * alone (the next step forms d and x the same way). */
   /* r_new = r - Z d_new with d_new = a d + b D^{-1} r formed at each
    * neighbour: sum_j (b vd_ij r_j + a v_ij d_j), vd_ij = v_ij / z_jj.
    * Software pipeline over the group's rows: the next row's bounds and
@@ -328,13 +334,13 @@ k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ vdv,
    * own r and d after them (the same round trip), which keeps the
    * two-pack FP64 form within 64 registers: 4 CTAs of 8 warps per SM. */
   ZS_GROUP_SETUP ();
-  const bool first = flags & CHEB_FIRST, zx = flags & CHEB_ZERO_X;
-  const bool wd = flags & CHEB_STORE_D;
+  const bool first = !PR && (flags & CHEB_FIRST), zx = flags & CHEB_ZERO_X;
+  const bool wd = flags & CHEB_STORE_D, ronly = flags & CHEB_R_ONLY;
   const int64_t stride = (int64_t) gridDim.x * ngroups;
   int64_t i = (int64_t) blockIdx.x * ngroups + group;
   int64_t k0 = 0, k1 = 0;
   int mc = 0;
-  T mv = T (0), mw = T (0);
+  T mv = T (0), mw = T (0), md = T (0);
   if (i < z.n) {
     k0 = z.rowptr[i];
     k1 = z.rowptr[i + 1];
@@ -342,6 +348,7 @@ k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ vdv,
       mc = z.col[k0 + lane];
       mv = vals[k0 + lane];
       mw = vdv[k0 + lane];
+      if (PR) md = dinv[mc];
     }
   }
   for (; i < z.n; i += stride) {
@@ -360,23 +367,29 @@ k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ vdv,
       const int cnt = (int) ((k1 - kb) < G ? (k1 - kb) : G);
       if (kb != k0) {   /* rows longer than G: later chunks load inline */
         mc = 0;
-        mv = mw = T (0);
+        mv = mw = md = T (0);
         if (lane < cnt) {
           mc = z.col[kb + lane];
           mv = vals[kb + lane];
           mw = vdv[kb + lane];
+          if (PR) md = dinv[mc];
         }
       }
       for (int t = 0; t < cnt; t++) {
         const int c = __shfl_sync (gmask, mc, t, G);
         const T av = a * __shfl_sync (gmask, mv, t, G);
         const T bw = b * __shfl_sync (gmask, mw, t, G);
+        const T bpj = PR ? bp * __shfl_sync (gmask, md, t, G) : T (0);
 #pragma unroll
         for (int h = 0; h < CH; h++) {
           const int vi = lane + h * G;
           if (vi < nvec) {
             Pack<T> rj = ldp (Rold + (int64_t) c * ld + vi * W);
             Pack<T> dj = first ? pzero<T> () : ldp (Dold + (int64_t) c * ld + vi * W);
+            if (PR) {
+#pragma unroll
+              for (int e = 0; e < W; e++) dj.v[e] = fma (bpj, dj.v[e], T (0));
+            }
 #pragma unroll
             for (int e = 0; e < W; e++)
               acc[h][e] = fma (bw, rj.v[e], fma (av, dj.v[e], acc[h][e]));
@@ -386,13 +399,15 @@ k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ vdv,
     }
     /* the next row's first chunk, behind this row's gathers */
     int mcn = 0;
-    T mvn = T (0), mwn = T (0);
+    T mvn = T (0), mwn = T (0), mdn = T (0);
     if (inx < z.n && lane < k1n - k0n) {
       mcn = z.col[k0n + lane];
       mvn = vals[k0n + lane];
       mwn = vdv[k0n + lane];
+      if (PR) mdn = dinv[mcn];
     }
     const T bdi = b * dinv[i];
+    const T bpi = PR ? bp * dinv[i] : T (0);
 #pragma unroll
     for (int h = 0; h < CH; h++) {
       const int vi = lane + h * G;
@@ -400,14 +415,21 @@ k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ vdv,
         const int64_t o = i * ld + vi * W;
         Pack<T> ri = ldp (Rold + o);
         Pack<T> di = first ? pzero<T> () : ldp (Dold + o);
-        Pack<T> dn, rn, x = zx ? pzero<T> () : ldp (X + o);
+        Pack<T> dn, rn, x = (zx || ronly) ? pzero<T> () : ldp (X + o);
+        if (PR) {
+#pragma unroll
+          for (int e = 0; e < W; e++) {
+            di.v[e] = fma (bpi, di.v[e], T (0));   /* d_prev from r_prev */
+            x.v[e] += di.v[e];         /* x_prev */
+          }
+        }
 #pragma unroll
         for (int e = 0; e < W; e++) {
           dn.v[e] = fma (bdi, ri.v[e], a * di.v[e]);
           x.v[e] += dn.v[e];
           rn.v[e] = ri.v[e] - acc[h][e];
         }
-        stp (X + o, x);
+        if (!ronly) stp (X + o, x);
         if (wd) stp (Dnew + o, dn);
         stp (Rnew + o, rn);
       }
@@ -417,6 +439,7 @@ k_cheb (ZK z, const T *__restrict__ vals, const T *__restrict__ vdv,
     mc = mcn;
     mv = mvn;
     mw = mwn;
+    md = mdn;
   }
 }
 
@@ -1450,7 +1473,8 @@ cheb_l2_budget ()
 template <typename T>
 int
 launch_cheb_step (const Csr &A, T *X, const T *Ro, T *Rn, const T *Do, T *Dn,
-                  int ld, double a, double b, int flags, cudaStream_t s)
+                  int ld, double a, double b, int flags, cudaStream_t s,
+                  double bp)
 {
   constexpr int W = Pack<T>::W;
   const int nvec_all = ld / W;
@@ -1473,11 +1497,19 @@ launch_cheb_step (const Csr &A, T *X, const T *Ro, T *Rn, const T *Do, T *Dn,
     row_group_shape (nvec, glog, ch, A.max_row_nnz);
     const int grid = std::min (row_grid (A.n, glog), num_sms () * 8);
     ZS_DISPATCH (ch, {
-      k_cheb<T, CH_><<<fit_grid (k_cheb<T, CH_>, grid, ZS_THREADS, 0),
-                                            ZS_THREADS, 0, s>>> (zk, vals, zvd<T> (A), dinv, X + c0, Ro + c0,
-                                                  Rn + c0, Do ? Do + c0 : nullptr,
-                                                  Dn ? Dn + c0 : nullptr, ld, nvec, glog,
-                                                  (T) a, (T) b, flags);
+      if (flags & CHEB_PREV_R) {
+        auto k = k_cheb<T, CH_, true>;
+        k<<<fit_grid (k, grid, ZS_THREADS, 0), ZS_THREADS, 0, s>>> (
+            zk, vals, zvd<T> (A), dinv, X + c0, Ro + c0, Rn + c0, Do + c0,
+            Dn ? Dn + c0 : nullptr, ld, nvec, glog, (T) a, (T) b, flags,
+            (T) bp);
+      } else {
+        auto k = k_cheb<T, CH_, false>;
+        k<<<fit_grid (k, grid, ZS_THREADS, 0), ZS_THREADS, 0, s>>> (
+            zk, vals, zvd<T> (A), dinv, X + c0, Ro + c0, Rn + c0,
+            Do ? Do + c0 : nullptr, Dn ? Dn + c0 : nullptr, ld, nvec, glog,
+            (T) a, (T) b, flags, T (0));
+      }
     });
     LGH_LAUNCH_CHECK ();
   }
@@ -1490,8 +1522,11 @@ template <typename T>
 __global__ void
 k_cheb_tail (int64_t n, int ld, const T *__restrict__ dinv, T *__restrict__ X,
              const T *__restrict__ R, const T *__restrict__ D, T a, T b,
-             int first)
+             int first, int prevr, T bp)
 {
+  /* prevr: D holds the residual of a first step (coefficient bp) that
+   * stored only its residual; its d and x are formed here with that
+   * step's roundings (d_prev = (bp dinv_i) r_prev, x_prev = x + d_prev) */
   constexpr int W = Pack<T>::W;
   const int nvec = ld / W;
   const int64_t total = n * nvec;
@@ -1502,6 +1537,14 @@ k_cheb_tail (int64_t n, int ld, const T *__restrict__ dinv, T *__restrict__ X,
     const T bdi = b * dinv[i];
     Pack<T> x = ldp (X + o), r = ldp (R + o);
     Pack<T> d = first ? pzero<T> () : ldp (D + o);
+    if (prevr) {
+      const T bpi = bp * dinv[i];
+#pragma unroll
+      for (int k = 0; k < W; k++) {
+        d.v[k] = fma (bpi, d.v[k], T (0));
+        x.v[k] += d.v[k];
+      }
+    }
 #pragma unroll
     for (int k = 0; k < W; k++) x.v[k] += fma (bdi, r.v[k], a * d.v[k]);
     stp (X + o, x);
@@ -1511,31 +1554,32 @@ k_cheb_tail (int64_t n, int ld, const T *__restrict__ dinv, T *__restrict__ X,
 template <typename T>
 int
 launch_cheb_tail (const Csr &A, T *X, const T *R, const T *D, int ld, double a,
-                  double b, int first, cudaStream_t s)
+                  double b, int first, cudaStream_t s, double bp)
 {
   constexpr int W = Pack<T>::W;
   const int64_t total = A.n * (int64_t) (ld / W);
   const int grid = (int) std::max<int64_t> (1, std::min<int64_t> (
       (int64_t) num_sms () * 8, (total + 255) / 256));
   k_cheb_tail<T><<<grid, 256, 0, s>>> (A.n, ld, zdinv<T> (A), X, R, D, (T) a,
-                                       (T) b, first);
+                                       (T) b, first, bp != 0. ? 1 : 0, (T) bp);
   LGH_LAUNCH_CHECK ();
   return 0;
 }
 
 template int launch_cheb_tail<double> (const Csr &, double *, const double *,
                                        const double *, int, double, double,
-                                       int, cudaStream_t);
+                                       int, cudaStream_t, double);
 template int launch_cheb_tail<float> (const Csr &, float *, const float *,
                                       const float *, int, double, double, int,
-                                      cudaStream_t);
+                                      cudaStream_t, double);
 
 template int launch_cheb_step<double> (const Csr &, double *, const double *,
                                        double *, const double *, double *,
-                                       int, double, double, int, cudaStream_t);
+                                       int, double, double, int, cudaStream_t,
+                                       double);
 template int launch_cheb_step<float> (const Csr &, float *, const float *,
                                       float *, const float *, float *, int,
-                                      double, double, int, cudaStream_t);
+                                      double, double, int, cudaStream_t, double);
 
 /* per-column ||D^{-1}(S B - Z X)||, ||D^{-1} S B|| ; optional R output */
 template <typename TO>

@@ -333,7 +333,8 @@ SIGNATURES = {
     "lgh_test_zsolve": (ctypes.c_int, [P, ctypes.c_int, P, P, ctypes.c_int]),
     "lgh_test_cheb_step": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_int,
-                                          ctypes.c_int, P, P, P, P, P]),
+                                          ctypes.c_int, P, P, P, P, P,
+                                          ctypes.c_double]),
     "lgh_test_gram": (ctypes.c_int, [I64, ctypes.c_int, P, P]),
     "lgh_gram_noalloc": (ctypes.c_int, [I64, ctypes.c_int, P, I64, P, I64]),
     "lgh_test_gemm_nn": (ctypes.c_int, [I64, ctypes.c_int, ctypes.c_int, P,
@@ -1056,9 +1057,10 @@ def test_zsolve(prior, X, fp32=False):
 
 
 CHEB_FIRST, CHEB_ZERO_X, CHEB_STORE_D = 1, 2, 4
+CHEB_R_ONLY, CHEB_PREV_R = 8, 16
 
 
-def test_cheb_step(A, X, R, D, a, b, flags, fp32=False):
+def test_cheb_step(A, X, R, D, a, b, flags, fp32=False, bp=0.0):
     """One Chebyshev-Jacobi smoothing step (lgh_test_cheb_step); returns
     the new (X, R, D)."""
     X = np.array(X, dtype=np.float64, order="C")
@@ -1069,7 +1071,7 @@ def test_cheb_step(A, X, R, D, a, b, flags, fp32=False):
     _chk(load().lgh_test_cheb_step(A.h, X.shape[1], a, b, flags,
                                    1 if fp32 else 0, X.ctypes.data,
                                    R.ctypes.data, D.ctypes.data,
-                                   Rn.ctypes.data, Dn.ctypes.data),
+                                   Rn.ctypes.data, Dn.ctypes.data, bp),
          "lgh_test_cheb_step")
     return X, Rn, Dn
 

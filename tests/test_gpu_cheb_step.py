@@ -6,7 +6,8 @@ lengths, empty rows and rows without a diagonal entry (Jacobi scale 0).
 
 One step: d_new = a d + b D^{-1} r (flags & 1: the a d term left out),
 x += d_new (flags & 2: x taken as zero), r_new = r - A d_new, and d_new
-stored (flags & 4)."""
+stored (flags & 4).  And the two-step form the V-cycle runs at its default
+degree (flags 8 and 16), bit for bit against two ordinary steps."""
 
 import numpy as np
 import pytest
@@ -100,3 +101,39 @@ def test_cheb_step_column_slices_same_bits(ops, monkeypatch):
     for a, b in zip(out["0"], out["0.05"]):
         for u, v in zip(a, b):
             assert np.array_equal(u, v)
+
+
+@pytest.mark.parametrize("name", ["z2d", "z3d", "ragged"])
+@pytest.mark.parametrize("fp32", [False, True])
+def test_two_step_pair_same_bits(ops, name, fp32):
+    """The smoother's two-step form (the V-cycle's default degree): a first
+    step that stores only its residual (flags 8), then a step that forms
+    the first step's d and x from that step's input residual (flags 16,
+    coefficient bp), gives the same bits as two ordinary steps, from x = 0
+    (pre-smoothing) and from a given x (post-smoothing)."""
+    A, M = ops[name]
+    n = A["n"]
+    rng = np.random.default_rng(23)
+    b1, a2, b2 = 0.93, 0.41, 1.27
+    for w in (1, 3, 16, 60, 220):
+        X = rng.standard_normal((n, w))
+        R0 = rng.standard_normal((n, w))
+        if fp32:
+            X, R0 = (v.astype(np.float32).astype(np.float64) for v in (X, R0))
+        zero = np.zeros_like(R0)
+        for zx in (L.CHEB_ZERO_X, 0):
+            # two ordinary steps
+            x1, r1, d1 = L.test_cheb_step(M, X, R0, zero, 0.0, b1,
+                                          L.CHEB_FIRST | zx | L.CHEB_STORE_D,
+                                          fp32)
+            x2, r2, _ = L.test_cheb_step(M, x1, r1, d1, a2, b2, 0, fp32)
+            # the pair: residual only, then the step that forms d1 and x1
+            xs, s1, _ = L.test_cheb_step(M, X, R0, zero, 0.0, b1,
+                                         L.CHEB_FIRST | zx | L.CHEB_R_ONLY,
+                                         fp32)
+            assert np.array_equal(xs, X)            # x left untouched
+            assert np.array_equal(s1, r1), (w, zx)
+            y2, s2, _ = L.test_cheb_step(M, X, s1, R0, a2, b2,
+                                         L.CHEB_PREV_R | zx, fp32, bp=b1)
+            assert np.array_equal(y2, x2), (w, zx)
+            assert np.array_equal(s2, r2), (w, zx)
