@@ -352,10 +352,17 @@ def run_ours(args):
     cs = np.array([SHIFT])
     Lb = L.load()
 
+    # the previous job's object is released when the next job starts (in
+    # the timed region), as a caller that builds one object per job does;
+    # its blocks then come back from the library's allocation cache
+    live = {}
+
     def job(timers=None):
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         ev[0].record()
+        live.pop("g", None)
         g = L.Glr(B, pr, opts, exec=ex)
+        live["g"] = g
         ev[1].record()
         L._chk(Lb.lgh_glr_solve_batch(g.h, 1, cs.ctypes.data_as(L.c_dbl_p),
                                       NRHS, rhs.ptr(), N, xout.ptr(), N),
@@ -364,7 +371,7 @@ def run_ours(args):
         ld = g.logdet(SHIFT)
         ev[3].record()
         if timers is not None:
-            timers.append((ev, g))
+            timers.append(ev)
         return g, ld
 
     def barrier():
@@ -399,10 +406,9 @@ def run_ours(args):
     clk = clocks.stop()
     elapsed = max_over_ranks(t_start.elapsed_time(t_end) / 1e3, world,
                              "cuda")
-    build_s = [ev[0].elapsed_time(ev[1]) / 1e3 for ev, _ in timers]
-    solve_s = [ev[1].elapsed_time(ev[2]) / 1e3 for ev, _ in timers]
-    g_last = timers[-1][1]
-    del timers[:-1]
+    build_s = [ev[0].elapsed_time(ev[1]) / 1e3 for ev in timers]
+    solve_s = [ev[1].elapsed_time(ev[2]) / 1e3 for ev in timers]
+    g_last = live["g"]
 
     # per-kernel roofline: a separate, untimed pass of the same job with
     # the library's per-launch CUDA-event registry on (the registry adds an
@@ -471,11 +477,18 @@ def run_ours(args):
     if peak is None:
         peak, peak_note = 6650.0, "fallback 6.65 TB/s"
     achieved = (kbytes / kn) / (kms / kn / 1e3) / 1e9 if kn else None
+    # DRAM bytes per launch: the ncu captures give DRAM / algorithmic bytes
+    # for the kernel's launch kinds at C2 (profiles/traffic.json); scaled by
+    # this run's algorithmic bytes per launch, whose launch widths differ
     traffic = None
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            traffic = json.load(f).get(name)
-    except (OSError, ValueError):
+            ent = json.load(f).get(name)
+        if isinstance(ent, dict) and kn:
+            traffic = ent["dram_per_algorithmic"] * kbytes / kn
+        elif isinstance(ent, (int, float)):
+            traffic = ent
+    except (OSError, ValueError, KeyError):
         pass
     tot_ms = sum(v[0] for v in ktimes.values()) or 1.0
     kernels = {k: {"ms": round(v[0], 3), "launches": v[1],
@@ -523,6 +536,7 @@ def run_ours(args):
         # the other configurations, one sub-object each (not the headline)
         del g_last
         timers.clear()
+        live.clear()
         line["configs"] = {}
         for name, fn in (("c3", run_c3), ("c4", run_c4), ("c5", run_c5)):
             try:
@@ -594,6 +608,7 @@ def run_mixed_job(args, B, pr, opts, N, g64, rhs, xout, L, torch):
     g = None
     for _ in range(args.steps):
         evs[0].record()
+        g = None             # the previous job's object goes first
         g = L.Glr(B, pr, opts, exec=ex)
         evs[1].record()
         L._chk(Lb.lgh_glr_solve_batch(g.h, 1, cs.ctypes.data_as(L.c_dbl_p),
