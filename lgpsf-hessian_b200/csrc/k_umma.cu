@@ -25,7 +25,9 @@
  *     tcgen05.commit that frees the stage when those MMAs are done;
  *   - after the last commit every warp reads its 32 TMEM lanes (rows)
  *     with tcgen05.ld and writes the caller's column-major output, adding
- *     fc y0: for each column the 32 lanes store 32 consecutive doubles.
+ *     fc y0 (staged through the freed stage buffer, 32 columns at a time,
+ *     with coalesced row loads): for each column the 32 lanes store 32
+ *     consecutive doubles.
  * Every mbarrier wait is bounded; a wait that runs out sets *err, the CTA
  * still waits (bounded) for its own MMAs through one final commit, frees
  * its TMEM and returns, and the host reports the error.
@@ -235,7 +237,20 @@ k_shift_combine_umma (const __grid_constant__ CUtensorMap mAh,
     const int64_t i = row0 + warp * 32 + lane;
     double *const o = *out;
     const int64_t ld = *ldo;
+    /* the stage buffer is free once the last MMA is done: each 32-column
+     * chunk's y0 values (128 rows, row stride 33 doubles against bank
+     * conflicts) are staged there with coalesced row loads, lane = column */
+    double *const sy = (double *) gbase;
     for (int q0 = 0; q0 < TN; q0 += 32) {
+      {
+        const int Jl = col0 + q0 + lane;
+        const int jl = Jl < ncol ? Jl - (Jl / m) * m : 0;
+        for (int r = warp; r < UM; r += 4) {
+          const int64_t ii = row0 + r;
+          sy[r * 33 + lane] = (ii < n && Jl < ncol) ? Y0[ii * ldy0 + jl] : 0.;
+        }
+      }
+      __syncthreads ();
       uint32_t v[32];
       const uint32_t ta = tmem + ((uint32_t) (warp * 32) << 16) + (uint32_t) q0;
       asm volatile ("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
@@ -253,16 +268,18 @@ k_shift_combine_umma (const __grid_constant__ CUtensorMap mAh,
                     : "r"(ta));
       asm volatile ("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (i < n) {
+        const double *yr = sy + (warp * 32 + lane) * 33;
 #pragma unroll
         for (int q = 0; q < 32; q++) {
           const int J = col0 + q0 + q;
           if (J < ncol) {
-            const int si = J / m, j = J - si * m;
+            const int si = J / m;
             o[i + (int64_t) J * ld] = (double) __uint_as_float (v[q])
-                                      + fc[si] * Y0[i * ldy0 + j];
+                                      + fc[si] * yr[q];
           }
         }
       }
+      __syncthreads ();
     }
   }
   asm volatile ("tcgen05.fence::before_thread_sync;" ::: "memory");
