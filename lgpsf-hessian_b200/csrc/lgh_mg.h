@@ -18,6 +18,14 @@ struct MgLevel
   double smax = 0., slo = 0., shi = 0.;
   int nu = 2;
   int own = 1;
+  /* the first smoothing step of the two-step form as a plain residual
+   * product r1 = r0 - F1 r0: A's pattern (F1 shares A's arrays) with the
+   * values fl(b1 vd_ij) in FP64 and fl((float) b1 vd32_ij) in FP32, b1 =
+   * 1 / theta, the very products the Chebyshev step forms (owned: f1v,
+   * f1v32; null where the level does not smooth) */
+  Csr F1;
+  double *f1v = nullptr;
+  float *f1v32 = nullptr;
 };
 
 struct MgWork

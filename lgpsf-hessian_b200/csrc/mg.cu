@@ -591,7 +591,50 @@ Hierarchy::~Hierarchy ()
     if (l.own) csr_free (l.A);
     csr_free (l.P);
     csr_free (l.R);
+    dfree (l.f1v);
+    dfree (l.f1v32);
   }
+}
+
+/* the first smoothing step's values: fl(b1 vd) and fl((float) b1 vd32) */
+__global__ void
+k_first_step_vals (int64_t nnz, double b1, const double *__restrict__ vd,
+                   const float *__restrict__ vd32, double *__restrict__ out,
+                   float *__restrict__ out32)
+{
+  const float b1f = (float) b1;
+  for (int64_t k = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; k < nnz;
+       k += (int64_t) gridDim.x * blockDim.x) {
+    out[k] = b1 * vd[k];
+    out32[k] = b1f * vd32[k];
+  }
+}
+
+static int
+first_step_operator (MgLevel &lv)
+{
+  const Csr &A = lv.A;
+  if (!A.vd || !A.vd32 || A.nnz == 0) return 0;
+  const double theta = 0.5 * (lv.shi + lv.slo);
+  const double b1 = 1.0 / theta;      /* mg_smooth's first coefficient */
+  int rc = dalloc ((void **) &lv.f1v, (size_t) A.nnz * sizeof (double) + 16);
+  if (!rc) rc = dalloc ((void **) &lv.f1v32, (size_t) A.nnz * sizeof (float) + 16);
+  if (rc) {
+    dfree (lv.f1v);
+    dfree (lv.f1v32);
+    lv.f1v = nullptr;
+    lv.f1v32 = nullptr;
+    return rc;
+  }
+  const int grid = (int) std::max<int64_t> (1, std::min<int64_t> (
+      (A.nnz + 255) / 256, (int64_t) num_sms () * 8));
+  k_first_step_vals<<<grid, 256, 0, stream ()>>> (A.nnz, b1, A.vd, A.vd32,
+                                                  lv.f1v, lv.f1v32);
+  LGH_LAUNCH_CHECK ();
+  lv.F1 = A;                          /* A's pattern; only the values differ */
+  lv.F1.vals = lv.f1v;
+  lv.F1.vals32 = lv.f1v32;
+  return 0;
 }
 
 void
@@ -644,6 +687,10 @@ mg_build (const Csr &Z, int tile, double smoother_top, int nu, Hierarchy **out)
     if (l == 0) lmax_own = lv.smax;
     lv.slo = 0.1 * lv.smax;
     lv.shi = smoother_top * lv.smax;
+    if (lv.nu == 2 && !(A.n <= coarse_max || l == 11)) {
+      rc = first_step_operator (lv);
+      if (rc) { delete h; return rc; }
+    }
     lap (1);
     if (A.n <= coarse_max || l == 11) {
       /* coarsest: dense inverse on the device, A^{-1} = L^{-T} L^{-1} */
@@ -781,10 +828,19 @@ mg_smooth (const MgLevel &lv, T *X, const T *B, T *R, T *Ra, T *D0, T *D1,
     const double rho = 1.0 / (2.0 * sigma1 - rho_old);
     const double a2 = rho * rho_old, b2 = 2.0 * rho / delta;
     const int f1 = CHEB_FIRST | CHEB_R_ONLY | (pre ? CHEB_ZERO_X : 0);
-    if (tr) LGH_TRY (tr->begin (K_MG_SMOOTH, sbase + 2. * sblk, s));
-    LGH_TRY (launch_cheb_step<T> (lv.A, X, Ro, Rn, nullptr, nullptr, ld, 0.,
-                                  b1, f1, s));
-    if (tr) LGH_TRY (tr->end (s));
+    if (lv.f1v) {
+      /* r1 = r0 - (b1 Z D^{-1}) r0 with the products fl(b1 vd_ij) formed
+       * once at set-up: the same products and order as the Chebyshev
+       * kernel's first step, without its direction and x streams */
+      if (tr) LGH_TRY (tr->begin (K_MG_FIRST, sbase + 2. * sblk, s));
+      LGH_TRY (launch_spmm_mode<T> (lv.F1, Ro, ld, Rn, ld, ld, 2, Ro, ld, s));
+      if (tr) LGH_TRY (tr->end (s));
+    } else {
+      if (tr) LGH_TRY (tr->begin (K_MG_SMOOTH, sbase + 2. * sblk, s));
+      LGH_TRY (launch_cheb_step<T> (lv.A, X, Ro, Rn, nullptr, nullptr, ld, 0.,
+                                    b1, f1, s));
+      if (tr) LGH_TRY (tr->end (s));
+    }
     T *R2 = (Rn == R) ? Ra : R;
     if (pre) {
       /* reads r1 (gathered), r0 = B (gathered); writes x, r2 */
