@@ -11,19 +11,35 @@
  * nnz (s_v + 4) + 8 (N + 1) + 2 N w s_x.
  */
 
+#include <type_traits>
+
 #include "lgh_device.cuh"
 #include "lgh_internal.h"
 
 namespace lgh
 {
 
-/* MODE 0: Y = A X;  1: Y += A X;  2: Y = B - A X */
+/* the post-smoothing epilogue of MODE 3 (the coefficients of a two-step
+ * Chebyshev-Jacobi sequence; dinv the inverse diagonal) */
+template <typename T>
+struct SpPost
+{
+  const T *dinv;
+  T a, b, bp;
+};
+
+/* MODE 0: Y = A X;  1: Y += A X;  2: Y = B - A X;
+ * 3: the last two steps of a post-smoothing sequence in one pass, with
+ *    X = B = r0 and Y = x (read and written), A = b1 Z D^{-1}:
+ *    r1 = r0 - A r0, d0 = (bp dinv_i) r0, x += d0,
+ *    x += (b dinv_i) r1 + a d0 (the roundings of the separate first step
+ *    and elementwise tail) */
 template <typename T, typename TV, int CH, int MODE>
 __global__ void __launch_bounds__ (256)
 k_spmm (int64_t n, const int64_t *__restrict__ rowptr,
         const int32_t *__restrict__ colidx, const TV *__restrict__ vals,
         const T *__restrict__ X, int ldx, T *__restrict__ Y, int ldy,
-        int nvec, int glog, const T *__restrict__ Bm, int ldb)
+        int nvec, int glog, const T *__restrict__ Bm, int ldb, SpPost<T> pp)
 {
   constexpr int W = Pack<T>::W;
   const int G = 1 << glog;
@@ -86,12 +102,28 @@ k_spmm (int64_t n, const int64_t *__restrict__ rowptr,
       }
     }
     T *yr = Y + i * ldy;
+    T bdi = T (0), bpi = T (0);
+    if (MODE == 3) {
+      const T di = pp.dinv[i];
+      bdi = pp.b * di;
+      bpi = pp.bp * di;
+    }
 #pragma unroll
     for (int h = 0; h < CH; h++) {
       const int vi = lane + h * G;
       if (vi < nvec) {
         Pack<T> o;
-        if (MODE == 1) {
+        if (MODE == 3) {
+          Pack<T> r0 = ldp (Bm + i * ldb + vi * W);
+          o = ldp (yr + vi * W);
+#pragma unroll
+          for (int e = 0; e < W; e++) {
+            const T r1 = r0.v[e] - acc[h][e];
+            const T d0 = fma (bpi, r0.v[e], T (0));
+            o.v[e] += d0;
+            o.v[e] += fma (bdi, r1, pp.a * d0);
+          }
+        } else if (MODE == 1) {
           Pack<T> y = ldp (yr + vi * W);
 #pragma unroll
           for (int e = 0; e < W; e++) o.v[e] = y.v[e] + acc[h][e];
@@ -180,13 +212,14 @@ template <typename T, typename TV>
 static int
 spmm_dispatch (const Csr &A, const TV *vals, const T *X, int ldx, T *Y,
                int ldy, int w, cudaStream_t s, int mode = 0,
-               const T *Bm = nullptr, int ldb = 0)
+               const T *Bm = nullptr, int ldb = 0,
+               SpPost<T> pp = SpPost<T>{ nullptr, T (0), T (0), T (0) })
 {
   constexpr int W = Pack<T>::W;
   const int MAXCH = 10;
   const bool vec_ok = (ldx % W == 0) && (ldy % W == 0)
                       && ((uintptr_t) X % 16 == 0) && ((uintptr_t) Y % 16 == 0)
-                      && (mode != 2 || (ldb % W == 0 && (uintptr_t) Bm % 16 == 0));
+                      && (mode < 2 || (ldb % W == 0 && (uintptr_t) Bm % 16 == 0));
   if (!vec_ok) {
     if (mode != 0)
       return set_error (LGH_ERR_ARG_WRONG, "spmm: accumulate/residual forms "
@@ -204,22 +237,21 @@ spmm_dispatch (const Csr &A, const TV *vals, const T *X, int ldx, T *Y,
     const int wc = (w - c0) < 32 * MAXCH * W ? (w - c0) : 32 * MAXCH * W;
     const int nvec = (wc + W - 1) / W;
     int glog, ch;
-    row_group_shape (nvec, glog, ch, mode == 2 ? A.max_row_nnz : 0);
+    row_group_shape (nvec, glog, ch, mode >= 2 ? A.max_row_nnz : 0);
     const int grid = row_grid (A.n, glog);
     const T *Xc = X + c0;
     T *Yc = Y + c0;
     const T *Bc = Bm ? Bm + c0 : nullptr;
+#define LGH_SPMM_MODE(C, M)                                                  \
+  k_spmm<T, TV, C, M><<<fit_grid (k_spmm<T, TV, C, M>, grid, 256, 0), 256,   \
+                        0, s>>> (A.n, A.rowptr, A.colidx, vals, Xc, ldx, Yc, \
+                                 ldy, nvec, glog, Bc, ldb, pp)
 #define LGH_SPMM_CASE(C)                                                     \
   case C:                                                                    \
-    if (mode == 0)                                                           \
-      k_spmm<T, TV, C, 0><<<fit_grid (k_spmm<T, TV, C, 0>, grid, 256, 0), 256, 0, s>>> (A.n, A.rowptr, A.colidx,     \
-          vals, Xc, ldx, Yc, ldy, nvec, glog, Bc, ldb);                      \
-    else if (mode == 1)                                                      \
-      k_spmm<T, TV, C, 1><<<fit_grid (k_spmm<T, TV, C, 1>, grid, 256, 0), 256, 0, s>>> (A.n, A.rowptr, A.colidx,     \
-          vals, Xc, ldx, Yc, ldy, nvec, glog, Bc, ldb);                      \
-    else                                                                     \
-      k_spmm<T, TV, C, 2><<<fit_grid (k_spmm<T, TV, C, 2>, grid, 256, 0), 256, 0, s>>> (A.n, A.rowptr, A.colidx,     \
-          vals, Xc, ldx, Yc, ldy, nvec, glog, Bc, ldb);                      \
+    if (mode == 0) LGH_SPMM_MODE (C, 0);                                     \
+    else if (mode == 1) LGH_SPMM_MODE (C, 1);                                \
+    else if (mode == 2) LGH_SPMM_MODE (C, 2);                                \
+    else LGH_SPMM_MODE (C, 3);                                               \
     break;
     switch (ch) {
       LGH_SPMM_CASE (1) LGH_SPMM_CASE (2) LGH_SPMM_CASE (3)
@@ -230,6 +262,7 @@ spmm_dispatch (const Csr &A, const TV *vals, const T *X, int ldx, T *Y,
       return set_error (LGH_ERR_SUP, "spmm: unsupported chunking %d", ch);
     }
 #undef LGH_SPMM_CASE
+#undef LGH_SPMM_MODE
     LGH_LAUNCH_CHECK ();
   }
   return 0;
@@ -271,5 +304,36 @@ launch_spmm_mode<float> (const Csr &A, const float *X, int ldx, float *Y,
   return spmm_dispatch<float, float> (A, A.vals32, X, ldx, Y, ldy, w, s, mode,
                                       Bm, ldb);
 }
+
+template <typename T>
+static const T *
+mode_vals (const Csr &A)
+{
+  if constexpr (std::is_same<T, double>::value) return A.vals;
+  else return A.vals32;
+}
+
+/* the post-smoothing finish (MODE 3): F1 = b1 Z D^{-1} (values
+ * fl(b1 vd_ij)), R0 the residual before the first step, X the iterate */
+template <typename T>
+int
+launch_spmm_cheb_post (const Csr &F1, const T *R0, T *X, int ld, int w,
+                       const T *dinv, double a, double b, double bp,
+                       cudaStream_t s)
+{
+  if (mode_vals<T> (F1) == nullptr || dinv == nullptr)
+    return set_error (LGH_ERR_ARG_WRONG, "spmm: post-smoothing needs values "
+                      "and the inverse diagonal");
+  return spmm_dispatch<T, T> (F1, mode_vals<T> (F1), R0, ld, X, ld, w, s, 3,
+                              R0, ld, SpPost<T>{ dinv, (T) a, (T) b, (T) bp });
+}
+
+template int launch_spmm_cheb_post<double> (const Csr &, const double *,
+                                            double *, int, int, const double *,
+                                            double, double, double,
+                                            cudaStream_t);
+template int launch_spmm_cheb_post<float> (const Csr &, const float *, float *,
+                                           int, int, const float *, double,
+                                           double, double, cudaStream_t);
 
 } /* namespace lgh */

@@ -27,7 +27,8 @@ static const char *g_names[K_NKERN] = {
   "k_pcgx_pq", "k_pcgx_upd", "k_pcgx_dots", "k_chebx",
   "k_cheb@vcycle", "k_spmm<resid>@vcycle", "k_spmm@restrict",
   "k_spmm<acc>@prolong", "k_dense_apply@coarse", "k_cheb_tail@vcycle",
-  "k_pcgx_pform", "k_spmm<first>@vcycle"
+  "k_pcgx_pform", "k_spmm<first>@vcycle",
+  "k_spmm<post>@vcycle"
 };
 
 int

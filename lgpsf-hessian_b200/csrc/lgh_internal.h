@@ -187,6 +187,14 @@ template <typename T>
 int launch_spmm_mode (const Csr &A, const T *X, int ldx, T *Y, int ldy, int w,
                       int mode, const T *Bm, int ldb, cudaStream_t s);
 
+/* the last two steps of a two-step post-smoothing sequence in one pass:
+ * with F1 = b1 Z D^{-1} (values fl(b1 vd_ij)) and R0 the residual,
+ * r1 = R0 - F1 R0, d0 = (bp dinv) R0, X += d0, X += (b dinv) r1 + a d0 */
+template <typename T>
+int launch_spmm_cheb_post (const Csr &F1, const T *R0, T *X, int ld, int w,
+                           const T *dinv, double a, double b, double bp,
+                           cudaStream_t s);
+
 /* Y = (TO) X over count elements of two blocks with the same layout */
 template <typename TI, typename TO>
 int cvt_flat (int64_t count, const TI *X, TO *Y, cudaStream_t s);

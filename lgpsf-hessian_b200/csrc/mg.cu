@@ -797,6 +797,14 @@ mg_work (Hierarchy *h, int ld, MgWork **w0, std::vector<MgWork> *own)
   return 0;
 }
 
+template <typename T>
+static const T *
+zdinv_of (const Csr &A)
+{
+  if constexpr (std::is_same<T, double>::value) return A.dinv;
+  else return A.dinv32;
+}
+
 /* Chebyshev-Jacobi smoothing in correction form on level l: R holds
  * B - A X on entry; nu terms; returns the buffer holding the residual */
 template <typename T>
@@ -828,6 +836,18 @@ mg_smooth (const MgLevel &lv, T *X, const T *B, T *R, T *Ra, T *D0, T *D1,
     const double rho = 1.0 / (2.0 * sigma1 - rho_old);
     const double a2 = rho * rho_old, b2 = 2.0 * rho / delta;
     const int f1 = CHEB_FIRST | CHEB_R_ONLY | (pre ? CHEB_ZERO_X : 0);
+    if (lv.f1v && !pre) {
+      /* post: both steps in one pass over r0 (gathered) and x; reads x
+       * and r0, writes x (r1 stays in registers) */
+      if (tr) LGH_TRY (tr->begin (K_MG_POST, sbase + 3. * sblk
+                                  + (double) lv.n * sizeof (T), s));
+      LGH_TRY (launch_spmm_cheb_post<T> (lv.F1, Ro, X, ld, ld,
+                                         zdinv_of<T> (lv.A), a2,
+                                         b2, b1, s));
+      if (tr) LGH_TRY (tr->end (s));
+      if (Rout) *Rout = nullptr;
+      return 0;
+    }
     if (lv.f1v) {
       /* r1 = r0 - (b1 Z D^{-1}) r0 with the products fl(b1 vd_ij) formed
        * once at set-up: the same products and order as the Chebyshev
