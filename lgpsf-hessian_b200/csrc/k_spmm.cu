@@ -305,6 +305,168 @@ launch_spmm_mode<float> (const Csr &A, const float *X, int ldx, float *Y,
                                       Bm, ldb);
 }
 
+/* The coarse correction and the whole post-smoothing of a two-step
+ * Chebyshev-Jacobi sequence in one pass over the fine rows:
+ *   xf = x + P xc          (the prolongation, its order and rounding)
+ *   r1 = r - F1 r          (F1 = b1 Z D^{-1}, r the post residual)
+ *   d0 = (bp dinv_i) r,  xf += d0,  xf += (b dinv_i) r1 + a d0.
+ * Each row is owned by a group of G lanes as in k_spmm; the next row's
+ * bounds and first (column, value) chunks of both operators load during
+ * the current row's gathers. */
+template <typename T, int CH>
+__global__ void __launch_bounds__ (256)
+k_post_prolong (int64_t n, const int64_t *__restrict__ frp,
+                const int32_t *__restrict__ fci, const T *__restrict__ fv,
+                const int64_t *__restrict__ prp,
+                const int32_t *__restrict__ pci, const T *__restrict__ pv,
+                const T *__restrict__ Rr, const T *__restrict__ Xc,
+                T *__restrict__ X, int ld, int nvec, int glog, SpPost<T> pp)
+{
+  constexpr int W = Pack<T>::W;
+  const int G = 1 << glog;
+  const int lane = threadIdx.x & (G - 1);
+  const int group = threadIdx.x >> glog;
+  const int ngroups = blockDim.x >> glog;
+  const unsigned gmask = (G == 32) ? 0xffffffffu
+                         : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+  const int64_t stride = (int64_t) gridDim.x * ngroups;
+  int64_t i = (int64_t) blockIdx.x * ngroups + group;
+  int64_t k0 = 0, k1 = 0, q0 = 0, q1 = 0;
+  int mc = 0, pc = 0;
+  T mv = T (0), pw = T (0);
+  if (i < n) {
+    k0 = frp[i];
+    k1 = frp[i + 1];
+    q0 = prp[i];
+    q1 = prp[i + 1];
+    if (lane < k1 - k0) {
+      mc = fci[k0 + lane];
+      mv = fv[k0 + lane];
+    }
+    if (lane < q1 - q0) {
+      pc = pci[q0 + lane];
+      pw = pv[q0 + lane];
+    }
+  }
+  for (; i < n; i += stride) {
+    const int64_t inx = i + stride;
+    int64_t k0n = 0, k1n = 0, q0n = 0, q1n = 0;
+    if (inx < n) {
+      k0n = frp[inx];
+      k1n = frp[inx + 1];
+      q0n = prp[inx];
+      q1n = prp[inx + 1];
+    }
+    /* the prolongation row: (P xc)_i, then xf = x_i + (P xc)_i */
+    T xf[CH][W];
+#pragma unroll
+    for (int h = 0; h < CH; h++)
+#pragma unroll
+      for (int e = 0; e < W; e++) xf[h][e] = T (0);
+    for (int64_t kb = q0; kb < q1; kb += G) {
+      const int cnt = (int) ((q1 - kb) < G ? (q1 - kb) : G);
+      if (kb != q0) {
+        pc = 0;
+        pw = T (0);
+        if (lane < cnt) {
+          pc = pci[kb + lane];
+          pw = pv[kb + lane];
+        }
+      }
+      for (int t = 0; t < cnt; t++) {
+        const int c = __shfl_sync (gmask, pc, t, G);
+        const T v = __shfl_sync (gmask, pw, t, G);
+        const T *xr = Xc + (int64_t) c * ld;
+#pragma unroll
+        for (int h = 0; h < CH; h++) {
+          const int vi = lane + h * G;
+          if (vi < nvec) {
+            Pack<T> x = ldp_nc (xr + vi * W);
+#pragma unroll
+            for (int e = 0; e < W; e++) xf[h][e] = fma (v, x.v[e], xf[h][e]);
+          }
+        }
+      }
+    }
+    T *xi = X + i * ld;
+#pragma unroll
+    for (int h = 0; h < CH; h++) {
+      const int vi = lane + h * G;
+      if (vi < nvec) {
+        Pack<T> x = ldp (xi + vi * W);
+#pragma unroll
+        for (int e = 0; e < W; e++) xf[h][e] = x.v[e] + xf[h][e];
+      }
+    }
+    /* the first step's product F1 r */
+    T acc[CH][W];
+#pragma unroll
+    for (int h = 0; h < CH; h++)
+#pragma unroll
+      for (int e = 0; e < W; e++) acc[h][e] = T (0);
+    for (int64_t kb = k0; kb < k1; kb += G) {
+      const int cnt = (int) ((k1 - kb) < G ? (k1 - kb) : G);
+      if (kb != k0) {
+        mc = 0;
+        mv = T (0);
+        if (lane < cnt) {
+          mc = fci[kb + lane];
+          mv = fv[kb + lane];
+        }
+      }
+      for (int t = 0; t < cnt; t++) {
+        const int c = __shfl_sync (gmask, mc, t, G);
+        const T v = __shfl_sync (gmask, mv, t, G);
+        const T *rr = Rr + (int64_t) c * ld;
+#pragma unroll
+        for (int h = 0; h < CH; h++) {
+          const int vi = lane + h * G;
+          if (vi < nvec) {
+            Pack<T> r = ldp_nc (rr + vi * W);
+#pragma unroll
+            for (int e = 0; e < W; e++) acc[h][e] = fma (v, r.v[e], acc[h][e]);
+          }
+        }
+      }
+    }
+    /* the next row's first chunks, behind this row's gathers */
+    mc = pc = 0;
+    mv = pw = T (0);
+    if (inx < n) {
+      if (lane < k1n - k0n) {
+        mc = fci[k0n + lane];
+        mv = fv[k0n + lane];
+      }
+      if (lane < q1n - q0n) {
+        pc = pci[q0n + lane];
+        pw = pv[q0n + lane];
+      }
+    }
+    const T di = pp.dinv[i];
+    const T bdi = pp.b * di, bpi = pp.bp * di;
+#pragma unroll
+    for (int h = 0; h < CH; h++) {
+      const int vi = lane + h * G;
+      if (vi < nvec) {
+        Pack<T> r0 = ldp (Rr + i * ld + vi * W);
+        Pack<T> o;
+#pragma unroll
+        for (int e = 0; e < W; e++) {
+          const T r1 = r0.v[e] - acc[h][e];
+          const T d0 = fma (bpi, r0.v[e], T (0));
+          o.v[e] = xf[h][e] + d0;
+          o.v[e] += fma (bdi, r1, pp.a * d0);
+        }
+        stp (xi + vi * W, o);
+      }
+    }
+    k0 = k0n;
+    k1 = k1n;
+    q0 = q0n;
+    q1 = q1n;
+  }
+}
+
 template <typename T>
 static const T *
 mode_vals (const Csr &A)
@@ -335,5 +497,57 @@ template int launch_spmm_cheb_post<double> (const Csr &, const double *,
 template int launch_spmm_cheb_post<float> (const Csr &, const float *, float *,
                                            int, int, const float *, double,
                                            double, double, cudaStream_t);
+
+/* the coarse correction and post-smoothing in one pass (k_post_prolong):
+ * F1 = b1 Z D^{-1}, R the post residual, P the prolongation, Xc the
+ * coarse correction (ld columns each) */
+template <typename T>
+int
+launch_post_prolong (const Csr &F1, const Csr &P, const T *R, const T *Xc,
+                     T *X, int ld, int w, const T *dinv, double a, double b,
+                     double bp, cudaStream_t s)
+{
+  constexpr int W = Pack<T>::W;
+  if (mode_vals<T> (F1) == nullptr || mode_vals<T> (P) == nullptr
+      || dinv == nullptr || P.n != F1.n)
+    return set_error (LGH_ERR_ARG_WRONG, "post-prolong: operators");
+  if (ld % W || (uintptr_t) R % 16 || (uintptr_t) Xc % 16 || (uintptr_t) X % 16
+      || w > 32 * 10 * W)
+    return set_error (LGH_ERR_ARG_WRONG, "post-prolong: needs 16-byte aligned "
+                      "row-major blocks of at most %d columns", 32 * 10 * W);
+  const int nvec = (w + W - 1) / W;
+  int glog, ch;
+  row_group_shape (nvec, glog, ch, F1.max_row_nnz);
+  const int grid = row_grid (F1.n, glog);
+  const SpPost<T> pp{ dinv, (T) a, (T) b, (T) bp };
+#define LGH_PP_CASE(C)                                                       \
+  case C:                                                                    \
+    k_post_prolong<T, C><<<fit_grid (k_post_prolong<T, C>, grid, 256, 0),    \
+                           256, 0, s>>> (F1.n, F1.rowptr, F1.colidx,         \
+                                         mode_vals<T> (F1), P.rowptr,        \
+                                         P.colidx, mode_vals<T> (P), R, Xc,  \
+                                         X, ld, nvec, glog, pp);             \
+    break;
+  switch (ch) {
+    LGH_PP_CASE (1) LGH_PP_CASE (2) LGH_PP_CASE (3) LGH_PP_CASE (4)
+    LGH_PP_CASE (5) LGH_PP_CASE (6) LGH_PP_CASE (7) LGH_PP_CASE (8)
+    LGH_PP_CASE (9) LGH_PP_CASE (10)
+  default:
+    return set_error (LGH_ERR_SUP, "post-prolong: unsupported chunking %d", ch);
+  }
+#undef LGH_PP_CASE
+  LGH_LAUNCH_CHECK ();
+  return 0;
+}
+
+template int launch_post_prolong<double> (const Csr &, const Csr &,
+                                          const double *, const double *,
+                                          double *, int, int, const double *,
+                                          double, double, double,
+                                          cudaStream_t);
+template int launch_post_prolong<float> (const Csr &, const Csr &,
+                                         const float *, const float *, float *,
+                                         int, int, const float *, double,
+                                         double, double, cudaStream_t);
 
 } /* namespace lgh */

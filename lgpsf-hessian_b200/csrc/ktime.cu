@@ -28,7 +28,8 @@ static const char *g_names[K_NKERN] = {
   "k_cheb@vcycle", "k_spmm<resid>@vcycle", "k_spmm@restrict",
   "k_spmm<acc>@prolong", "k_dense_apply@coarse", "k_cheb_tail@vcycle",
   "k_pcgx_pform", "k_spmm<first>@vcycle",
-  "k_spmm<post>@vcycle"
+  "k_spmm<post>@vcycle",
+  "k_post_prolong@vcycle"
 };
 
 int

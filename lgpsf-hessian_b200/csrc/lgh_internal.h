@@ -195,6 +195,14 @@ int launch_spmm_cheb_post (const Csr &F1, const T *R0, T *X, int ld, int w,
                            const T *dinv, double a, double b, double bp,
                            cudaStream_t s);
 
+/* the coarse correction and the whole two-step post-smoothing in one
+ * pass: X += P Xc (the prolongation), then the two steps of
+ * launch_spmm_cheb_post from the post residual R */
+template <typename T>
+int launch_post_prolong (const Csr &F1, const Csr &P, const T *R, const T *Xc,
+                         T *X, int ld, int w, const T *dinv, double a,
+                         double b, double bp, cudaStream_t s);
+
 /* Y = (TO) X over count elements of two blocks with the same layout */
 template <typename TI, typename TO>
 int cvt_flat (int64_t count, const TI *X, TO *Y, cudaStream_t s);

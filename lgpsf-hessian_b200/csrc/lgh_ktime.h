@@ -15,7 +15,7 @@ enum KId
   K_PCG_PQ = 0, K_PCG_UPD, K_CHEB, K_SPMM, K_PCG_INIT,
   K_PCGX_PQ, K_PCGX_UPD, K_PCGX_DOTS, K_CHEBX,
   K_MG_SMOOTH, K_MG_RESID, K_MG_RESTRICT, K_MG_PROLONG, K_MG_COARSE,
-  K_MG_TAIL, K_PCGX_PFORM, K_MG_FIRST, K_MG_POST,
+  K_MG_TAIL, K_PCGX_PFORM, K_MG_FIRST, K_MG_POST, K_MG_POSTP,
   K_NKERN
 };
 

@@ -26,6 +26,10 @@ struct MgLevel
   Csr F1;
   double *f1v = nullptr;
   float *f1v32 = nullptr;
+  /* A P (n_l x n_{l+1}): the post residual after the coarse correction is
+   * r2 - (A P) xc, from the pre-smoothing residual r2, without the fine
+   * product A (x + P xc) (owned; empty on the coarsest level) */
+  Csr AP;
 };
 
 struct MgWork

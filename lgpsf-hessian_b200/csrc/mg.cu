@@ -593,6 +593,7 @@ Hierarchy::~Hierarchy ()
     csr_free (l.R);
     dfree (l.f1v);
     dfree (l.f1v32);
+    csr_free (l.AP);
   }
 }
 
@@ -755,6 +756,7 @@ mg_build (const Csr &Z, int tile, double smoother_top, int nu, Hierarchy **out)
     lap (3);
     rc = csr_upload (P, lv.P);
     if (!rc) rc = csr_upload (R, lv.R);
+    if (!rc && lv.f1v) rc = csr_upload (AP, lv.AP);
     if (rc) { delete h; return rc; }
     h->lev.push_back (lv);
     A = std::move (Ac);
@@ -803,6 +805,21 @@ zdinv_of (const Csr &A)
 {
   if constexpr (std::is_same<T, double>::value) return A.dinv;
   else return A.dinv32;
+}
+
+/* the two-step Chebyshev-Jacobi coefficients on [slo, shi]: the first
+ * step d = b1 D^{-1} r, the second d = a2 d + b2 D^{-1} r */
+static void
+cheb2_coeffs (const MgLevel &lv, double *b1, double *a2, double *b2)
+{
+  const double theta = 0.5 * (lv.shi + lv.slo);
+  const double delta = 0.5 * (lv.shi - lv.slo);
+  const double sigma1 = theta / delta;
+  const double rho_old = 1.0 / sigma1;
+  const double rho = 1.0 / (2.0 * sigma1 - rho_old);
+  *b1 = 1.0 / theta;
+  *a2 = rho * rho_old;
+  *b2 = 2.0 * rho / delta;
 }
 
 /* Chebyshev-Jacobi smoothing in correction form on level l: R holds
@@ -944,6 +961,26 @@ vcycle_level (Hierarchy *h, MgWork *W, size_t l, const T *B, T *X, int ld,
   LGH_TRY (launch_spmm<T> (lv.R, Rc, ld, Bc, ld, ld, s));
   if (tr) LGH_TRY (tr->end (s));
   LGH_TRY (vcycle_level<T> (h, W, l + 1, Bc, Xc, ld, w, s, trace));
+  constexpr int PW = Pack<T>::W;
+  if (lv.nu == 2 && lv.f1v && lv.AP.n == n && Rc && ld <= 32 * 10 * PW) {
+    /* r = r2 - (A P) xc: the residual of x + P xc from the pre-smoothing
+     * residual r2 (the same value in exact arithmetic as B - A (x + P xc));
+     * then the prolongation and both post-smoothing steps in one pass */
+    T *Rp = (Rc == R) ? Ra : R;
+    double b1, a2, b2;
+    cheb2_coeffs (lv, &b1, &a2, &b2);
+    if (tr) LGH_TRY (tr->begin (K_MG_RESID, 2. * blk + cblk
+                                + (4. + sizeof (T)) * lv.AP.nnz, s));
+    LGH_TRY (launch_spmm_mode<T> (lv.AP, Xc, ld, Rp, ld, ld, 2, Rc, ld, s));
+    if (tr) LGH_TRY (tr->end (s));
+    if (tr) LGH_TRY (tr->begin (K_MG_POSTP, 3. * blk + cblk + (double) n * sizeof (T)
+                                + (4. + sizeof (T)) * (lv.F1.nnz + lv.P.nnz)
+                                + 16. * (n + 1), s));
+    LGH_TRY (launch_post_prolong<T> (lv.F1, lv.P, Rp, Xc, X, ld, ld,
+                                     zdinv_of<T> (lv.A), a2, b2, b1, s));
+    if (tr) LGH_TRY (tr->end (s));
+    return 0;
+  }
   if (tr) LGH_TRY (tr->begin (K_MG_PROLONG, 2. * blk + cblk + 12. * lv.P.nnz, s));
   LGH_TRY (launch_spmm_mode<T> (lv.P, Xc, ld, X, ld, ld, 1, nullptr, 0, s));
   if (tr) LGH_TRY (tr->end (s));
