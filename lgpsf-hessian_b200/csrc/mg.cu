@@ -789,10 +789,16 @@ mg_work (Hierarchy *h, int ld, MgWork **w0, std::vector<MgWork> *own)
       LGH_TRY (w.B.alloc (bytes));
       LGH_TRY (w.X.alloc (bytes));
     }
-    LGH_TRY (w.R0.alloc (bytes));
-    LGH_TRY (w.R1.alloc (bytes));
-    LGH_TRY (w.D0.alloc (bytes));
-    LGH_TRY (w.D1.alloc (bytes));
+    /* the coarsest level solves densely from B into X; the two-step
+     * smoother keeps no direction blocks (only other degrees use D0, D1) */
+    if (l + 1 < h->lev.size ()) {
+      LGH_TRY (w.R0.alloc (bytes));
+      LGH_TRY (w.R1.alloc (bytes));
+      if (h->lev[l].nu != 2) {
+        LGH_TRY (w.D0.alloc (bytes));
+        LGH_TRY (w.D1.alloc (bytes));
+      }
+    }
     w.cap = ld;
   }
   *w0 = W.data ();

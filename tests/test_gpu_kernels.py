@@ -202,6 +202,33 @@ def test_zsolve_pcg_c1_vs_oracle(w):
     assert abs(pr.info()["mean_col_iters"] - po.info()["mean_cg_its"]) <= 2
 
 
+@pytest.mark.parametrize("nu", [1, 2, 3])
+def test_zsolve_amg_smoother_degrees(nu):
+    """The V-cycle at smoother degrees 1 to 3, FP64 and FP32.  Degree 2 (the
+    default) runs the two-step form: a residual-only first step, the post
+    residual r2 - (A P) x_c and the prolongation fused into the
+    post-smoothing pass; the other degrees run the plain step sequence with
+    direction blocks.  Each solves to the dense answer, and a higher degree
+    takes no more PCG iterations than a lower one."""
+    cfg = P.grid_problem("c1")
+    Z = L.Mat(cfg["Z"])
+    X = np.random.default_rng(11).standard_normal((cfg["N"], 16))
+    ref = np.linalg.solve(P.csr_to_dense(cfg["Z"]), X)
+    its = {}
+    for k in sorted({1, nu}):
+        pr = L.Prior(Z=Z, mass=cfg["mass"],
+                     opts=L.prior_opts(ksp_rtol=1e-10, nu_force=k))
+        assert pr.info()["mg_levels"] >= 2
+        Y = L.test_zsolve(pr, X)
+        assert max(_rd(Y[:, j], ref[:, j]) for j in range(16)) < 1e-8
+        its[k] = pr.info()["mean_col_iters"]
+        pr32 = L.Prior(Z=Z, mass=cfg["mass"],
+                       opts=L.prior_opts(ksp_rtol=1e-5, nu_force=k))
+        Y32 = L.test_zsolve(pr32, X, fp32=True)
+        assert max(_rd(Y32[:, j], ref[:, j]) for j in range(16)) < 1e-3
+    assert its[nu] <= its[1]
+
+
 def test_zsolve_fp32():
     cfg = P.grid_problem("c1")
     Z = L.Mat(cfg["Z"])
