@@ -148,6 +148,13 @@ pool_release_all ()
 }
 } /* namespace */
 
+size_t
+pool_cached_bytes ()
+{
+  std::lock_guard<std::mutex> lk (g_pool_mu);
+  return g_pool_bytes;
+}
+
 int
 dalloc (void **p, size_t bytes)
 {

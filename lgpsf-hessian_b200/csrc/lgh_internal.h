@@ -77,6 +77,10 @@ double wall ();
 /* device allocation helpers (return LGH_ERR_MEM on failure) */
 int dalloc (void **p, size_t bytes);
 void dfree (void *p);
+/* bytes of freed blocks the allocation cache holds: dalloc reuses them,
+ * or releases them all and retries when the device is out of memory, so
+ * they count as free device memory */
+size_t pool_cached_bytes ();
 
 template <typename T>
 struct DBuf

@@ -320,7 +320,10 @@ srv_finish (lgh_server_t *sv, SReq *r, int rc)
   sv->ccv.notify_all ();
 }
 
-/* room on the device for a request's staging above the reserve */
+/* room on the device for a request's staging above the reserve; the
+ * allocation cache's free blocks count as free (blocks that objects built
+ * before this loop released stay cached, and the driver does not see
+ * them as free) */
 static bool
 srv_room (lgh_server_t *sv, const SReq *r)
 {
@@ -329,9 +332,10 @@ srv_room (lgh_server_t *sv, const SReq *r)
     cudaGetLastError ();
     return true;
   }
+  const double avail = (double) fb + (double) pool_cached_bytes ();
   const double need = (double) sv->g->n * r->m * 16.
                       + (double) std::max (sv->g->kept, 1) * r->m * 8.;
-  return (double) fb - need >= sv->reserve * (double) tb;
+  return avail - need >= sv->reserve * (double) tb;
 }
 
 /* a request's input columns to the device through the pinned halves */
