@@ -208,7 +208,7 @@ struct Harvest
   double *out_b[MAXS];       /* request output columns */
 };
 
-/* a run of one request's columns admitted into slots this round */
+/* a run of one request's columns admitted into slots in one admission pass */
 struct Adm
 {
   SReq *r;
