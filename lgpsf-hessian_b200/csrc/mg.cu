@@ -93,29 +93,62 @@ hdot (const std::vector<double> &a, const std::vector<double> &b)
   return s;
 }
 
+/* T = A^T with each row of T in ascending source row order.  Row chunks
+ * of A count their entries per column, the counts give every chunk its
+ * start in each row of T (chunks in row order), and the chunks scatter
+ * in parallel: the result is the serial transpose's, bit for bit. */
 static HCsr
 hcsr_transpose (const HCsr &A)
 {
   HCsr T;
   T.n = A.m;
   T.m = A.n;
+  const int64_t nnz = A.rp[A.n];
   T.rp.assign (T.n + 1, 0);
-  for (int64_t k = 0; k < A.rp[A.n]; k++) T.rp[A.ci[k] + 1]++;
-  for (int64_t i = 0; i < T.n; i++) T.rp[i + 1] += T.rp[i];
-  T.ci.resize (A.rp[A.n]);
-  T.v.resize (A.rp[A.n]);
-  std::vector<int64_t> pos (T.rp.begin (), T.rp.end () - 1);
-  for (int64_t i = 0; i < A.n; i++)
-    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++) {
-      const int64_t p = pos[A.ci[k]]++;
-      T.ci[p] = (int32_t) i;
-      T.v[p] = A.v[k];
+  T.ci.resize (nnz);
+  T.v.resize (nnz);
+  const int nt = std::max (1, std::min (omp_get_max_threads (), 64));
+  /* one chunk per thread, unless the count arrays would outweigh A */
+  int nch = (int) std::min<int64_t> (std::max<int64_t> (A.n, 1), nt);
+  while (nch > 1 && (int64_t) nch * T.n > 4 * nnz + 4096) nch /= 2;
+  std::vector<int64_t> pos ((size_t) nch * T.n, 0);
+#pragma omp parallel for schedule(static) num_threads(nt)
+  for (int c = 0; c < nch; c++) {
+    int64_t *cnt = pos.data () + (size_t) c * T.n;
+    const int64_t r0 = A.n * c / nch, r1 = A.n * (c + 1) / nch;
+    for (int64_t k = A.rp[r0]; k < A.rp[r1]; k++) cnt[A.ci[k]]++;
+  }
+  /* row starts of T, then each chunk's start within every row */
+#pragma omp parallel for schedule(static) num_threads(nt)
+  for (int64_t j = 0; j < T.n; j++) {
+    int64_t s = 0;
+    for (int c = 0; c < nch; c++) s += pos[(size_t) c * T.n + j];
+    T.rp[j + 1] = s;
+  }
+  for (int64_t j = 0; j < T.n; j++) T.rp[j + 1] += T.rp[j];
+#pragma omp parallel for schedule(static) num_threads(nt)
+  for (int64_t j = 0; j < T.n; j++) {
+    int64_t s = T.rp[j];
+    for (int c = 0; c < nch; c++) {
+      const int64_t k = pos[(size_t) c * T.n + j];
+      pos[(size_t) c * T.n + j] = s;
+      s += k;
     }
+  }
+#pragma omp parallel for schedule(static) num_threads(nt)
+  for (int c = 0; c < nch; c++) {
+    int64_t *at = pos.data () + (size_t) c * T.n;
+    const int64_t r0 = A.n * c / nch, r1 = A.n * (c + 1) / nch;
+    for (int64_t i = r0; i < r1; i++)
+      for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++) {
+        const int64_t p = at[A.ci[k]]++;
+        T.ci[p] = (int32_t) i;
+        T.v[p] = A.v[k];
+      }
+  }
   return T;
 }
 
-/* C = A B (Gustavson, dense accumulator), columns sorted per row; row
- * chunks in parallel, each with its own accumulator, then concatenated */
 /* rows of a product assembled chunk by chunk: each chunk's rows go into
  * vectors of its own (moved out once, so threads never write shared
  * headers), then the chunks are concatenated in parallel at their
@@ -156,48 +189,76 @@ hcsr_concat (std::vector<HChunk> &ch, int64_t n, HCsr &C)
 static HCsr
 hcsr_gemm (const HCsr &A, const HCsr &B)
 {
+  /* C = A B (Gustavson, dense accumulator), columns sorted per row: a
+   * counting pass sizes every row, then the rows are formed in place, in
+   * parallel; each row sums its terms in A's then B's entry order, so the
+   * product does not depend on the thread count */
   HCsr C;
   C.n = A.n;
   C.m = B.m;
   const int nt = std::max (1, std::min (omp_get_max_threads (), 64));
-  const int nchunk = (int) std::min<int64_t> (std::max<int64_t> (A.n, 1), 4 * nt);
-  std::vector<HChunk> ch (nchunk);
+  /* about 8 scheduling chunks per thread, at least 64 rows each */
+  const int64_t rows_per = std::max<int64_t> (64, A.n / (8 * nt));
+  C.rp.assign (C.n + 1, 0);
+#pragma omp parallel num_threads(nt)
+  {
+    std::vector<int64_t> mark (B.m, -1);
+#pragma omp for schedule(dynamic, rows_per)
+    for (int64_t i = 0; i < A.n; i++) {
+      int64_t cnt = 0;
+      for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++) {
+        const int64_t j = A.ci[k];
+        for (int64_t q = B.rp[j]; q < B.rp[j + 1]; q++) {
+          const int32_t col = B.ci[q];
+          if (mark[col] != i) {
+            mark[col] = i;
+            cnt++;
+          }
+        }
+      }
+      C.rp[i + 1] = cnt;
+    }
+  }
+  for (int64_t i = 0; i < C.n; i++) C.rp[i + 1] += C.rp[i];
+  C.ci.resize (C.rp[C.n]);
+  C.v.resize (C.rp[C.n]);
 #pragma omp parallel num_threads(nt)
   {
     std::vector<double> acc (B.m, 0.);
     std::vector<int64_t> mark (B.m, -1);
-    std::vector<int32_t> cols;
-#pragma omp for schedule(dynamic, 1)
-    for (int c = 0; c < nchunk; c++) {
-      const int64_t r0 = A.n * c / nchunk, r1 = A.n * (c + 1) / nchunk;
-      HChunk loc;
-      loc.cnt.reserve (r1 - r0);
-      for (int64_t i = r0; i < r1; i++) {
-        cols.clear ();
-        for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++) {
-          const int64_t j = A.ci[k];
-          const double a = A.v[k];
-          for (int64_t q = B.rp[j]; q < B.rp[j + 1]; q++) {
-            const int32_t col = B.ci[q];
-            if (mark[col] != i) {
-              mark[col] = i;
-              acc[col] = 0.;
-              cols.push_back (col);
-            }
-            acc[col] += a * B.v[q];
+#pragma omp for schedule(dynamic, rows_per)
+    for (int64_t i = 0; i < A.n; i++) {
+      int32_t *cols = C.ci.data () + C.rp[i];
+      size_t nc = 0;
+      for (int64_t k = A.rp[i]; k < A.rp[i + 1]; k++) {
+        const int64_t j = A.ci[k];
+        const double a = A.v[k];
+        for (int64_t q = B.rp[j]; q < B.rp[j + 1]; q++) {
+          const int32_t col = B.ci[q];
+          if (mark[col] != i) {
+            mark[col] = i;
+            acc[col] = 0.;
+            cols[nc++] = col;
           }
+          acc[col] += a * B.v[q];
         }
-        std::sort (cols.begin (), cols.end ());
-        for (int32_t col : cols) {
-          loc.ci.push_back (col);
-          loc.v.push_back (acc[col]);
-        }
-        loc.cnt.push_back ((int64_t) cols.size ());
       }
-      ch[c] = std::move (loc);
+      /* ascending columns: rows of these products hold a few dozen
+       * entries at most, where an insertion sort beats std::sort */
+      if (nc > 48) {
+        std::sort (cols, cols + nc);
+      } else {
+        for (size_t t = 1; t < nc; t++) {
+          const int32_t x = cols[t];
+          size_t u = t;
+          for (; u > 0 && cols[u - 1] > x; u--) cols[u] = cols[u - 1];
+          cols[u] = x;
+        }
+      }
+      double *v = C.v.data () + C.rp[i];
+      for (size_t t = 0; t < nc; t++) v[t] = acc[cols[t]];
     }
   }
-  hcsr_concat (ch, C.n, C);
   return C;
 }
 
@@ -745,12 +806,23 @@ mg_build (const Csr &Z, int tile, double smoother_top, int nu, Hierarchy **out)
     HCsr R = hcsr_transpose (P);
     HCsr AP = hcsr_gemm (A, P);
     HCsr Ac = hcsr_gemm (R, AP);
-    /* symmetrise the Galerkin product against rounding */
+    /* symmetrise the Galerkin product against rounding: every entry (i, j)
+     * with its mirror (j, i), found in row j's sorted columns (the pattern
+     * of P^T A P is symmetric); the new values go to a copy so that each
+     * pair reads the unsymmetrised ones */
     {
-      HCsr AcT = hcsr_transpose (Ac);
+      std::vector<double> vs (Ac.v.size ());
+#pragma omp parallel for schedule(dynamic, 256)
       for (int64_t i = 0; i < Ac.n; i++)
-        for (int64_t k = Ac.rp[i], kt = AcT.rp[i]; k < Ac.rp[i + 1]; k++, kt++)
-          Ac.v[k] = 0.5 * (Ac.v[k] + AcT.v[kt]);
+        for (int64_t k = Ac.rp[i]; k < Ac.rp[i + 1]; k++) {
+          const int64_t j = Ac.ci[k];
+          const int32_t *b = Ac.ci.data () + Ac.rp[j];
+          const int32_t *e = Ac.ci.data () + Ac.rp[j + 1];
+          const int32_t *f = std::lower_bound (b, e, (int32_t) i);
+          const double mirror = (f != e && *f == i) ? Ac.v[Ac.rp[j] + (f - b)] : 0.;
+          vs[k] = 0.5 * (Ac.v[k] + mirror);
+        }
+      Ac.v.swap (vs);
     }
     Ac.m = Ac.n;
     lap (3);
