@@ -43,12 +43,30 @@ namespace lgh
 
 /* ---- host CSR helpers -------------------------------------------------- */
 
+/* an allocator whose resize leaves new elements uninitialised: every
+ * column and value array of the host set-up is sized and then written in
+ * full by a parallel loop (or a copy), so its pages are first touched by
+ * the threads that fill them instead of by a serial zero fill */
+template <typename T>
+struct NoInitAlloc : std::allocator<T>
+{
+  template <typename U> struct rebind { using other = NoInitAlloc<U>; };
+  NoInitAlloc () = default;
+  template <typename U> NoInitAlloc (const NoInitAlloc<U> &) noexcept {}
+  template <typename U> void construct (U *p) noexcept { ::new ((void *) p) U; }
+  template <typename U, typename... Args>
+  void construct (U *p, Args &&...args)
+  {
+    ::new ((void *) p) U (std::forward<Args> (args)...);
+  }
+};
+
 struct HCsr
 {
   int64_t n = 0, m = 0; /* rows, cols */
   std::vector<int64_t> rp;
-  std::vector<int32_t> ci;
-  std::vector<double> v;
+  std::vector<int32_t, NoInitAlloc<int32_t>> ci;
+  std::vector<double, NoInitAlloc<double>> v;
 };
 
 static double
@@ -811,7 +829,7 @@ mg_build (const Csr &Z, int tile, double smoother_top, int nu, Hierarchy **out)
      * of P^T A P is symmetric); the new values go to a copy so that each
      * pair reads the unsymmetrised ones */
     {
-      std::vector<double> vs (Ac.v.size ());
+      decltype (Ac.v) vs (Ac.v.size ());
 #pragma omp parallel for schedule(dynamic, 256)
       for (int64_t i = 0; i < Ac.n; i++)
         for (int64_t k = Ac.rp[i]; k < Ac.rp[i + 1]; k++) {
