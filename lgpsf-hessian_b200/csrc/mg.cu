@@ -402,6 +402,7 @@ sa_coarsen (const HCsr &A, double theta, double lmax, HCsr &P, int64_t &nc)
   std::vector<double> sz (nc, 0.);
   for (int64_t i = 0; i < n; i++) sz[agg[i]] += 1.;
   std::vector<double> p0 (n);
+#pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < n; i++) p0[i] = 1. / sqrt (sz[agg[i]]);
   /* omega = 4/3 / lambda_max(D^{-1}A) (the level's own estimate) */
   const double omega = (4.0 / 3.0) / lmax;
