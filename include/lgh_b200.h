@@ -733,6 +733,21 @@ int lgh_test_potrf (int n, const double *G, int jitter_mode, double *L,
                     double *Linv, int *info);
 int lgh_test_syev (int n, const double *A, double *w, double *V,
                    int *sweeps);
+/* The multigrid set-up's first coarsening of a square CSR (host arrays),
+ * run on the host alone with no device call: the smoothed-aggregation
+ * prolongator P (n x nc) and the symmetrised Galerkin operator
+ * Ac = P^T A P (nc x nc), with `threads` OpenMP threads (0: the default).
+ * *nc, *p_nnz and *c_nnz always get the sizes; P and Ac are written when
+ * p_rowptr / c_rowptr are non-null (n + 1 and nc + 1 row pointers,
+ * capacities p_cap / c_cap entries), so a first call with null arrays
+ * sizes the second.                                                      */
+int lgh_test_mg_galerkin (int64_t n, const int64_t *rowptr,
+                          const int32_t *colidx, const double *vals,
+                          int threads, int64_t *nc, int64_t *p_rowptr,
+                          int32_t *p_colidx, double *p_vals, int64_t p_cap,
+                          int64_t *p_nnz, int64_t *c_rowptr,
+                          int32_t *c_colidx, double *c_vals, int64_t c_cap,
+                          int64_t *c_nnz);
 
 #ifdef __cplusplus
 }

@@ -294,4 +294,18 @@ lgh_test_syev (int n, const double *A, double *w, double *V, int *sweeps)
   return down (V, dv, (size_t) n * n);
 }
 
+/* the host multigrid set-up's first coarsening (no device call) */
+int
+lgh_test_mg_galerkin (int64_t n, const int64_t *rowptr, const int32_t *colidx,
+                      const double *vals, int threads, int64_t *nc,
+                      int64_t *p_rowptr, int32_t *p_colidx, double *p_vals,
+                      int64_t p_cap, int64_t *p_nnz, int64_t *c_rowptr,
+                      int32_t *c_colidx, double *c_vals, int64_t c_cap,
+                      int64_t *c_nnz)
+{
+  return mg_host_galerkin (n, rowptr, colidx, vals, threads, nc, p_rowptr,
+                           p_colidx, p_vals, p_cap, p_nnz, c_rowptr, c_colidx,
+                           c_vals, c_cap, c_nnz);
+}
+
 } /* extern "C" */

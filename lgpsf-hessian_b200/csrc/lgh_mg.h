@@ -50,6 +50,15 @@ struct Hierarchy
 
 struct KTrace;
 
+/* the host set-up's first coarsening of a square host CSR, on the host
+ * alone (test hook; see mg.cu) */
+int mg_host_galerkin (int64_t n, const int64_t *rowptr, const int32_t *colidx,
+                      const double *vals, int threads, int64_t *nc_out,
+                      int64_t *p_rowptr, int32_t *p_colidx, double *p_vals,
+                      int64_t p_cap, int64_t *p_nnz, int64_t *c_rowptr,
+                      int32_t *c_colidx, double *c_vals, int64_t c_cap,
+                      int64_t *c_nnz);
+
 /* X = V(B): one block V-cycle from the finest level (X overwritten);
  * tr (nullable) records the fine level's kernels for the timing registry;
  * work (nullable) gives the level buffers of a caller that runs V-cycles

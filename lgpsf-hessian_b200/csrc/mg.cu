@@ -725,6 +725,96 @@ mg_destroy (Hierarchy *h)
 }
 
 /* smoothed-aggregation hierarchy of Z (level 0 borrows Z's device arrays) */
+/* the Galerkin step of one level: R = P^T, A P (kept for the post
+ * residual) and Ac = P^T (A P), symmetrised against rounding: every entry
+ * (i, j) averaged with its mirror (j, i), found in row j's sorted columns
+ * (the pattern of P^T A P is symmetric); the averages go to a copy so that
+ * each pair reads the unsymmetrised values */
+static void
+galerkin (const HCsr &A, const HCsr &P, HCsr &R, HCsr &AP, HCsr &Ac)
+{
+  R = hcsr_transpose (P);
+  AP = hcsr_gemm (A, P);
+  Ac = hcsr_gemm (R, AP);
+  decltype (Ac.v) vs (Ac.v.size ());
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < Ac.n; i++)
+    for (int64_t k = Ac.rp[i]; k < Ac.rp[i + 1]; k++) {
+      const int64_t j = Ac.ci[k];
+      const int32_t *b = Ac.ci.data () + Ac.rp[j];
+      const int32_t *e = Ac.ci.data () + Ac.rp[j + 1];
+      const int32_t *f = std::lower_bound (b, e, (int32_t) i);
+      const double mirror = (f != e && *f == i) ? Ac.v[Ac.rp[j] + (f - b)] : 0.;
+      vs[k] = 0.5 * (Ac.v[k] + mirror);
+    }
+  Ac.v.swap (vs);
+  Ac.m = Ac.n;
+}
+
+/* The first coarsening of a square host CSR on the host alone (no device
+ * call): the level's lambda_max from the host CG-Lanczos, the smoothed
+ * aggregation prolongator and the Galerkin step, with `threads` OpenMP
+ * threads (0: the current default).  The set-up proper estimates
+ * lambda_max on the device for large levels; this is for checking the host
+ * products and their independence of the thread count. */
+int
+mg_host_galerkin (int64_t n, const int64_t *rowptr, const int32_t *colidx,
+                  const double *vals, int threads, int64_t *nc_out,
+                  int64_t *p_rowptr, int32_t *p_colidx, double *p_vals,
+                  int64_t p_cap, int64_t *p_nnz, int64_t *c_rowptr,
+                  int32_t *c_colidx, double *c_vals, int64_t c_cap,
+                  int64_t *c_nnz)
+{
+  LGH_CHECK (n > 0 && rowptr && colidx && vals && nc_out && p_nnz && c_nnz,
+             LGH_ERR_ARG_NULL, "mg_host_galerkin: null argument");
+  LGH_CHECK (n < INT32_MAX, LGH_ERR_ARG_OUTOFRANGE,
+             "mg_host_galerkin: n too large");
+  LGH_CHECK (rowptr[0] == 0, LGH_ERR_ARG_WRONG,
+             "mg_host_galerkin: rowptr[0] != 0");
+  for (int64_t i = 0; i < n; i++)
+    LGH_CHECK (rowptr[i + 1] >= rowptr[i], LGH_ERR_ARG_WRONG,
+               "mg_host_galerkin: rowptr not monotone at row %lld",
+               (long long) i);
+  const int64_t nnz = rowptr[n];
+  for (int64_t k = 0; k < nnz; k++)
+    LGH_CHECK (colidx[k] >= 0 && colidx[k] < n, LGH_ERR_ARG_WRONG,
+               "mg_host_galerkin: column out of range at entry %lld",
+               (long long) k);
+  HCsr A;
+  A.n = A.m = n;
+  A.rp.assign (rowptr, rowptr + n + 1);
+  A.ci.resize (nnz);
+  A.v.resize (nnz);
+  memcpy (A.ci.data (), colidx, (size_t) nnz * sizeof (int32_t));
+  memcpy (A.v.data (), vals, (size_t) nnz * sizeof (double));
+  const int prev = omp_get_max_threads ();
+  if (threads > 0) omp_set_num_threads (threads);
+  const double lmax = lanczos_lmax (A, 40, 20260813ULL);
+  HCsr P, R, AP, Ac;
+  int64_t nc = 0;
+  sa_coarsen (A, 0.0, lmax, P, nc);
+  galerkin (A, P, R, AP, Ac);
+  omp_set_num_threads (prev);
+  *nc_out = nc;
+  *p_nnz = P.rp[P.n];
+  *c_nnz = Ac.rp[Ac.n];
+  if (p_rowptr) {
+    LGH_CHECK (p_cap >= *p_nnz && p_colidx && p_vals, LGH_ERR_ARG_OUTOFRANGE,
+               "mg_host_galerkin: P needs %lld entries", (long long) *p_nnz);
+    memcpy (p_rowptr, P.rp.data (), (size_t) (n + 1) * sizeof (int64_t));
+    memcpy (p_colidx, P.ci.data (), (size_t) *p_nnz * sizeof (int32_t));
+    memcpy (p_vals, P.v.data (), (size_t) *p_nnz * sizeof (double));
+  }
+  if (c_rowptr) {
+    LGH_CHECK (c_cap >= *c_nnz && c_colidx && c_vals, LGH_ERR_ARG_OUTOFRANGE,
+               "mg_host_galerkin: Ac needs %lld entries", (long long) *c_nnz);
+    memcpy (c_rowptr, Ac.rp.data (), (size_t) (nc + 1) * sizeof (int64_t));
+    memcpy (c_colidx, Ac.ci.data (), (size_t) *c_nnz * sizeof (int32_t));
+    memcpy (c_vals, Ac.v.data (), (size_t) *c_nnz * sizeof (double));
+  }
+  return 0;
+}
+
 int
 mg_build (const Csr &Z, int tile, double smoother_top, int nu, Hierarchy **out)
 {
@@ -822,28 +912,8 @@ mg_build (const Csr &Z, int tile, double smoother_top, int nu, Hierarchy **out)
       return set_error (LGH_ERR_SUP, "mg: aggregation made no progress at n=%lld",
                         (long long) A.n);
     }
-    HCsr R = hcsr_transpose (P);
-    HCsr AP = hcsr_gemm (A, P);
-    HCsr Ac = hcsr_gemm (R, AP);
-    /* symmetrise the Galerkin product against rounding: every entry (i, j)
-     * with its mirror (j, i), found in row j's sorted columns (the pattern
-     * of P^T A P is symmetric); the new values go to a copy so that each
-     * pair reads the unsymmetrised ones */
-    {
-      decltype (Ac.v) vs (Ac.v.size ());
-#pragma omp parallel for schedule(dynamic, 256)
-      for (int64_t i = 0; i < Ac.n; i++)
-        for (int64_t k = Ac.rp[i]; k < Ac.rp[i + 1]; k++) {
-          const int64_t j = Ac.ci[k];
-          const int32_t *b = Ac.ci.data () + Ac.rp[j];
-          const int32_t *e = Ac.ci.data () + Ac.rp[j + 1];
-          const int32_t *f = std::lower_bound (b, e, (int32_t) i);
-          const double mirror = (f != e && *f == i) ? Ac.v[Ac.rp[j] + (f - b)] : 0.;
-          vs[k] = 0.5 * (Ac.v[k] + mirror);
-        }
-      Ac.v.swap (vs);
-    }
-    Ac.m = Ac.n;
+    HCsr R, AP, Ac;
+    galerkin (A, P, R, AP, Ac);
     lap (3);
     rc = csr_upload (P, lv.P);
     if (!rc) rc = csr_upload (R, lv.R);

@@ -342,6 +342,9 @@ SIGNATURES = {
     "lgh_test_potrf": (ctypes.c_int, [ctypes.c_int, P, ctypes.c_int, P, P,
                                       P]),
     "lgh_test_syev": (ctypes.c_int, [ctypes.c_int, P, P, P, P]),
+    "lgh_test_mg_galerkin": (ctypes.c_int, [I64, P, P, P, ctypes.c_int, P,
+                                            P, P, P, I64, P, P, P, P, I64,
+                                            P]),
 }
 
 
@@ -1105,6 +1108,36 @@ def test_potrf(G, jitter_mode=0):
                                Li.ctypes.data, info.ctypes.data),
          "lgh_test_potrf")
     return L, (Li if info[0] == 0 else None), info
+
+
+def test_mg_galerkin(csr, threads=0):
+    """The multigrid set-up's first coarsening of a square CSR dict (n,
+    rowptr, colidx, vals), run on the host alone (lgh_test_mg_galerkin):
+    returns (P, Ac) as CSR dicts, P n x nc, Ac = P^T A P (nc x nc)."""
+    n = int(csr["n"]) if "n" in csr else len(csr["rowptr"]) - 1
+    rp = np.ascontiguousarray(csr["rowptr"], dtype=np.int64)
+    ci = np.ascontiguousarray(csr["colidx"], dtype=np.int32)
+    v = np.ascontiguousarray(csr["vals"], dtype=np.float64)
+    nc, pn, cn = ctypes.c_int64(0), ctypes.c_int64(0), ctypes.c_int64(0)
+    L = load()
+    args = (n, rp.ctypes.data, ci.ctypes.data, v.ctypes.data, threads,
+            ctypes.byref(nc))
+    _chk(L.lgh_test_mg_galerkin(*args, None, None, None, 0, ctypes.byref(pn),
+                                None, None, None, 0, ctypes.byref(cn)),
+         "lgh_test_mg_galerkin")
+    Prp = np.empty(n + 1, dtype=np.int64)
+    Pci = np.empty(pn.value, dtype=np.int32)
+    Pv = np.empty(pn.value)
+    Crp = np.empty(nc.value + 1, dtype=np.int64)
+    Cci = np.empty(cn.value, dtype=np.int32)
+    Cv = np.empty(cn.value)
+    _chk(L.lgh_test_mg_galerkin(*args, Prp.ctypes.data, Pci.ctypes.data,
+                                Pv.ctypes.data, pn.value, ctypes.byref(pn),
+                                Crp.ctypes.data, Cci.ctypes.data,
+                                Cv.ctypes.data, cn.value, ctypes.byref(cn)),
+         "lgh_test_mg_galerkin")
+    return (dict(n=n, m=nc.value, rowptr=Prp, colidx=Pci, vals=Pv),
+            dict(n=nc.value, m=nc.value, rowptr=Crp, colidx=Cci, vals=Cv))
 
 
 def test_syev(A):
